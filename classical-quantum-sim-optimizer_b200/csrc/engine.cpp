@@ -1,0 +1,219 @@
+#include "engine.hpp"
+
+#include <chrono>
+#include <cstring>
+
+namespace dq {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(kMemoryError, std::string("Unable to allocate device memory for ") + what);
+    }
+    fail(kCudaError, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void DevMem::alloc(size_t b, const char* what) {
+    release();
+    if (b == 0) b = 16;
+    cuda_check(cudaMalloc(&p, b), what);
+    bytes = b;
+}
+
+void DevMem::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+Device::Device(int ord) : ordinal(ord) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        fail(kCudaError, std::string("no CUDA device available: ") + (e == cudaSuccess ? "0 devices" : cudaGetErrorString(e)));
+    if (ord < 0 || ord >= count) fail(kValueError, "CUDA device ordinal out of range");
+    cuda_check(cudaSetDevice(ord), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+Device::~Device() {
+    if (stream) {
+        cudaSetDevice(ordinal);
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+}
+
+void Device::activate() const { cuda_check(cudaSetDevice(ordinal), "cudaSetDevice"); }
+
+void Device::sync() { cuda_check(cudaStreamSynchronize(stream), "stream synchronize"); }
+
+void StateBatch::allocate(int n_, uint64_t W_, uint64_t ncb_, bool c64_) {
+    n = n_;
+    W = W_;
+    ncb = ncb_;
+    c64 = c64_;
+    cwords = int(std::max<uint64_t>(1, (ncb + 63) / 64));
+    amps.alloc((size_t(W) << n) * (c64 ? 8 : 16), "the statevector");
+    cbits.alloc(size_t(W) * cwords * 8, "classical bits");
+    seeds.alloc(size_t(W) * 8, "rng seeds");
+    draws.alloc(size_t(W) * 8, "rng counters");
+    outcome.alloc(size_t(W) * 4, "measurement outcomes");
+    scale.alloc(size_t(W) * 8, "measurement scales");
+    partial.alloc(size_t(W) * k::kMaxChunks * 2 * 8, "measurement partial sums");
+    err.alloc(16, "error flag");
+}
+
+k::Batch StateBatch::view(cudaStream_t s, uint64_t W_active) const {
+    k::Batch b;
+    b.stream = s;
+    b.c64 = c64;
+    b.amps = amps.p;
+    b.n = n;
+    b.W = W_active;
+    b.cbits = cbits.as<uint64_t>();
+    b.cwords = cwords;
+    b.rng_seed = seeds.as<uint64_t>();
+    b.draws = draws.as<uint64_t>();
+    b.outcome = outcome.as<int>();
+    b.scale = scale.as<double>();
+    b.partial = partial.as<double>();
+    b.err = err.as<int>();
+    return b;
+}
+
+namespace {
+double2 d2(cplx c) { return make_double2(c.re, c.im); }
+}  // namespace
+
+Executor::Executor(const std::vector<Operation>& ops, size_t begin, size_t end) {
+    for (size_t i = begin; i < end; i++) {
+        std::vector<Condition> conds;
+        lower(ops[i], conds);
+    }
+}
+
+void Executor::lower(const Operation& op, std::vector<Condition>& conds) {
+    if (op.type == Operation::Conditional) {
+        conds.push_back(op.condition);
+        lower(*op.inner, conds);
+        conds.pop_back();
+        return;
+    }
+    if (op.type == Operation::Noop) return;
+    if (conds.size() > 6) fail(kValueError, "Classical conditions nested deeper than 6 levels are not supported");
+    Step s;
+    s.type = op.type;
+    s.host_conds = conds;
+    s.cond.n = int(conds.size());
+    for (size_t i = 0; i < conds.size(); i++) {
+        s.cond.base[i] = conds[i].creg_base;
+        s.cond.size[i] = uint32_t(conds[i].creg_size);
+        s.cond.value[i] = conds[i].creg_value;
+    }
+    for (auto& c : op.controls) s.controls.push_back({int(c.qubit), c.value});
+    switch (op.type) {
+        case Operation::One:
+            s.target = int(op.target);
+            s.u[0] = d2(op.m[0][0]);
+            s.u[1] = d2(op.m[0][1]);
+            s.u[2] = d2(op.m[1][0]);
+            s.u[3] = d2(op.m[1][1]);
+            s.category = op.controls.empty() ? 0 : 1;
+            break;
+        case Operation::X:
+            s.target = int(op.target);
+            s.category = op.controls.empty() ? 0 : 1;
+            break;
+        case Operation::Swap:
+            s.a = int(op.a);
+            s.b = int(op.b);
+            s.category = 1;
+            break;
+        case Operation::Diagonal:
+            for (auto q : op.qubits) s.qubits.push_back(int(q));
+            for (auto& v : op.values) s.diag.push_back(d2(v));
+            s.category = op.qubits.size() > 1 ? 1 : 0;
+            break;
+        case Operation::Dense:
+            for (auto q : op.qubits) s.qubits.push_back(int(q));
+            s.pool_offset = pool_host_.size();
+            for (auto& v : op.values) pool_host_.push_back(d2(v));
+            s.category = 1;
+            break;
+        case Operation::Measure:
+            s.target = int(op.qubit);
+            s.cbit = int64_t(op.cbit);
+            s.category = 2;
+            break;
+        case Operation::Reset:
+            s.target = int(op.qubit);
+            s.cbit = -1;
+            s.category = 2;
+            break;
+        default: fail(kValueError, "unexpected operation");
+    }
+    steps_.push_back(std::move(s));
+}
+
+void Executor::run(const k::Batch& b, ProfileAcc* profile) {
+    if (!uploaded_) {
+        if (!pool_host_.empty()) {
+            pool_.alloc(pool_host_.size() * sizeof(double2), "gate matrices");
+            cuda_check(cudaMemcpyAsync(pool_.p, pool_host_.data(), pool_host_.size() * sizeof(double2),
+                                       cudaMemcpyHostToDevice, b.stream),
+                       "upload gate matrices");
+        }
+        uploaded_ = true;
+    }
+    std::vector<uint64_t> host_cbits;
+    for (const Step& s : steps_) {
+        if (profile && s.cond.n) {
+            // Profiling counts only executed operations (execution.rs:285-295),
+            // so the host reads the single trajectory's classical bits here.
+            host_cbits.resize(size_t(b.cwords));
+            cuda_check(cudaMemcpyAsync(host_cbits.data(), b.cbits, size_t(b.cwords) * 8, cudaMemcpyDeviceToHost,
+                                       b.stream),
+                       "read classical bits");
+            cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+            bool ok = true;
+            for (auto& c : s.host_conds) {
+                uint64_t v = 0;
+                for (uint64_t bit = 0; bit < c.creg_size; bit++) {
+                    uint64_t idx = c.creg_base + bit;
+                    v |= ((host_cbits[idx >> 6] >> (idx & 63)) & 1) << bit;
+                }
+                if (v != c.creg_value) ok = false;
+            }
+            if (!ok) continue;
+        }
+        auto t0 = std::chrono::steady_clock::now();
+        switch (s.type) {
+            case Operation::One: k::gate1q(b, s.target, s.controls, s.u, false, s.cond); break;
+            case Operation::X: k::gate1q(b, s.target, s.controls, s.u, true, s.cond); break;
+            case Operation::Swap: k::swap(b, s.a, s.b, s.controls, s.cond); break;
+            case Operation::Diagonal: k::diagonal(b, s.qubits, s.diag, s.cond); break;
+            case Operation::Dense: k::dense(b, s.qubits, pool_.as<double2>() + s.pool_offset, s.cond); break;
+            case Operation::Measure: k::measure(b, s.target, s.cbit, false, s.cond); break;
+            case Operation::Reset: k::measure(b, s.target, -1, true, s.cond); break;
+            default: break;
+        }
+        if (profile) {
+            cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (s.category == 0) {
+                profile->oq_calls++;
+                profile->oq_time += dt;
+            } else if (s.category == 1) {
+                profile->nq_calls++;
+                profile->nq_time += dt;
+            } else {
+                profile->mq_calls++;
+                profile->mq_time += dt;
+            }
+        }
+    }
+}
+
+}  // namespace dq

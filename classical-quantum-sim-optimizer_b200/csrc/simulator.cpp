@@ -1,0 +1,432 @@
+#include "simulator.hpp"
+
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <random>
+
+namespace dq {
+namespace {
+
+using clk = std::chrono::steady_clock;
+double since(clk::time_point t0) { return std::chrono::duration<double>(clk::now() - t0).count(); }
+
+// state_layout, shots.rs:22-31, for `amp` bytes per amplitude.
+void state_layout(uint64_t n, uint64_t amp, uint64_t* len, uint64_t* bytes) {
+    if (n >= 64) fail(kMemoryError, "State dimension overflow");
+    *len = uint64_t(1) << n;
+    unsigned __int128 b = (unsigned __int128)(*len) * amp;
+    if (b > kIsizeMax) fail(kMemoryError, "State byte size overflow");
+    *bytes = uint64_t(b);
+}
+
+// check_budget, shots.rs:43-48
+void check_budget(uint64_t required, uint64_t budget) {
+    if (required > budget)
+        fail(kMemoryError, "Simulation needs at least " + std::to_string(required) +
+                               " working bytes, exceeding max_memory_mb budget (" + std::to_string(budget) + " bytes)");
+}
+
+// format_bits, shots.rs:50-56: cbit 0 is the rightmost character.
+std::string format_bits(const uint8_t* cbits, uint64_t ncb) {
+    std::string s(ncb, '0');
+    for (uint64_t i = 0; i < ncb; i++) s[ncb - 1 - i] = char('0' + cbits[i]);
+    return s;
+}
+
+void upload_u64(void* dst, const std::vector<uint64_t>& v, cudaStream_t s) {
+    cuda_check(cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, s), "upload");
+}
+
+void check_err_flag(const StateBatch& st, cudaStream_t s) {
+    int flag = 0;
+    cuda_check(cudaMemcpyAsync(&flag, st.err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "read error flag");
+    cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+    if (flag) fail(kRuntimeError, "Cannot measure a state with nonfinite or zero norm");
+}
+
+void reset_bookkeeping(const StateBatch& st, uint64_t W, const std::vector<uint64_t>& seeds, cudaStream_t s) {
+    cuda_check(cudaMemsetAsync(st.cbits.p, 0, size_t(W) * st.cwords * 8, s), "clear cbits");
+    cuda_check(cudaMemsetAsync(st.draws.p, 0, size_t(W) * 8, s), "clear draws");
+    cuda_check(cudaMemsetAsync(st.err.p, 0, 16, s), "clear error flag");
+    upload_u64(st.seeds.p, seeds, s);
+}
+
+bool is_full_descending(const std::vector<uint64_t>& q, uint64_t n) {
+    if (q.size() != n) return false;
+    for (uint64_t t = 0; t < n; t++)
+        if (q[t] != n - 1 - t) return false;
+    return true;
+}
+
+// Probabilities of state 0 over `qubits` into a device buffer of 2^k doubles.
+void probs_to(const k::Batch& b, const std::vector<uint64_t>& qubits, double* out) {
+    if (is_full_descending(qubits, uint64_t(b.n))) {
+        k::norm2(b, out);
+    } else {
+        std::vector<int> q;
+        for (auto x : qubits) q.push_back(int(x));
+        k::marginal(b, q, out);
+    }
+}
+
+// Scan probabilities into a CDF on the device; returns the total.
+double build_cdf(cudaStream_t s, double* cdf, uint64_t len, DevMem& tmp) {
+    tmp.ensure(k::scan_tmp_size(len) * 8, "scan scratch");
+    k::scan(s, cdf, len, tmp.as<double>());
+    double total = 0;
+    cuda_check(cudaMemcpyAsync(&total, cdf + (len - 1), 8, cudaMemcpyDeviceToHost, s), "read total");
+    cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+    return total;
+}
+
+std::string json_double(double v) {
+    char buf[40];
+    std::snprintf(buf, sizeof buf, "%.17g", v);
+    std::string s(buf);
+    if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
+    return s;
+}
+
+}  // namespace
+
+std::vector<Operation> compile_json(const char* json, size_t len, uint64_t* n, uint64_t* ncb) {
+    Circuit c = parse_circuit(json, len);
+    validate_circuit(c);
+    if (n) *n = c.num_qubits();
+    if (ncb) *ncb = c.num_cbits();
+    return compile(c.instructions);
+}
+
+Simulator::Simulator(const Options& o) : opt_(o) {
+    // simulator.rs:234-246
+    if (o.max_memory_mb == 0 || o.max_memory_mb > kIsizeMax / (1024 * 1024))
+        fail(kValueError, "max_memory_mb must be positive and representable in bytes");
+    if (o.has_max_parallel_shots && o.max_parallel_shots == 0)
+        fail(kValueError, "max_parallel_shots must be positive or None");
+    budget_ = o.max_memory_mb * 1024 * 1024;
+}
+
+uint64_t Simulator::next_seed() {
+    if (opt_.has_seed) return opt_.seed;
+    std::random_device rd;
+    return (uint64_t(rd()) << 32) ^ uint64_t(rd());
+}
+
+ShotOutput Simulator::simulate_shots(const char* json, size_t len, uint64_t shots, bool profile, double* pre,
+                                     double* fus) {
+    auto total0 = clk::now();
+    profile = profile || opt_.profile;
+    Circuit c = parse_circuit(json, len);
+    validate_circuit(c);
+    double preprocessing = since(total0);
+    auto f0 = clk::now();
+    std::vector<Operation> plan = compile(c.instructions);
+    double fusion = since(f0);
+    uint64_t seed = next_seed();
+    auto s0 = clk::now();
+    ShotOutput out = run_shots(plan, c.num_qubits(), c.num_cbits(), shots, seed, profile);
+    double shots_total = since(s0);
+    if (pre) *pre = preprocessing;
+    if (fus) *fus = fusion;
+    if (profile) write_shots_profile(out, preprocessing, fusion, shots_total, since(total0), shots);
+    return out;
+}
+
+ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots,
+                                uint64_t seed, bool profile) {
+    ShotOutput out;
+    if (shots == 0) {
+        out.strategy = "empty";
+        return out;
+    }
+    const uint64_t amp = opt_.precision == Precision::C64 ? 8 : 16;
+    uint64_t len, state_bytes;
+    state_layout(n, amp, &len, &state_bytes);
+    if (state_bytes > kU64Max - ncb) fail(kMemoryError, "Working memory size overflow");
+    const uint64_t worker_bytes = state_bytes + ncb;
+    check_budget(worker_bytes, budget_);
+    size_t prefix_end = ops.size();
+    for (size_t i = 0; i < ops.size(); i++)
+        if (!ops[i].is_unitary()) {
+            prefix_end = i;
+            break;
+        }
+    bool terminal = true;
+    for (size_t i = prefix_end; i < ops.size(); i++)
+        if (ops[i].type != Operation::Measure) terminal = false;
+    const bool c64 = opt_.precision == Precision::C64;
+
+    if (opt_.sample_terminal && terminal) {
+        std::map<uint64_t, uint64_t> mapping;  // cbit -> qubit; the last write wins
+        for (size_t i = prefix_end; i < ops.size(); i++) mapping[ops[i].cbit] = ops[i].qubit;
+        if (mapping.empty()) {
+            out.strategy = "terminal_sampling";
+            out.counts[std::string(ncb, '0')] = shots;
+            return out;
+        }
+        std::vector<uint64_t> qubits;
+        for (auto& kv : mapping) qubits.push_back(kv.second);
+        std::sort(qubits.begin(), qubits.end());
+        qubits.erase(std::unique(qubits.begin(), qubits.end()), qubits.end());
+        std::reverse(qubits.begin(), qubits.end());
+        const uint64_t kq = qubits.size();
+        std::vector<std::pair<uint64_t, uint64_t>> shifts;  // (cbit, shift)
+        for (auto& kv : mapping) {
+            uint64_t pos = uint64_t(std::find(qubits.begin(), qubits.end(), kv.second) - qubits.begin());
+            shifts.emplace_back(kv.first, kq - 1 - pos);
+        }
+        if (kq >= 61) fail(kMemoryError, "Sampling memory overflow");
+        const uint64_t cdf_bytes = (uint64_t(1) << kq) * 8;
+        if (worker_bytes <= kU64Max - cdf_bytes && worker_bytes + cdf_bytes <= budget_) {
+            const uint64_t required = worker_bytes + cdf_bytes;
+            if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+            std::lock_guard<std::mutex> lk(dev_->mu);
+            dev_->activate();
+            cudaStream_t s = dev_->stream;
+            uint64_t kept_seed = seed;
+            {
+                StateBatch st;
+                st.allocate(int(n), 1, ncb, c64);
+                k::Batch b = st.view(s, 1);
+                k::init_basis(b);
+                reset_bookkeeping(st, 1, {kept_seed}, s);
+                Executor ex(ops, 0, prefix_end);
+                ex.run(b, nullptr);
+                DevMem cdf, tmp, idx;
+                const uint64_t clen = uint64_t(1) << kq;
+                cdf.alloc(clen * 8, "the sampling table");
+                probs_to(b, qubits, cdf.as<double>());
+                double total = build_cdf(s, cdf.as<double>(), clen, tmp);
+                if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
+                k::cdf_normalize(s, cdf.as<double>(), clen, total, false);
+                st.amps.release();  // the state is no longer needed (shots.rs:150)
+                idx.alloc(shots * 8, "sampled outcomes");
+                k::sample(s, cdf.as<double>(), clen, seed, shots, true, idx.as<uint64_t>());
+                std::vector<uint64_t> h(shots);
+                cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
+                cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+                std::unordered_map<uint64_t, uint64_t> sampled;
+                for (uint64_t v : h) sampled[v]++;
+                std::vector<uint8_t> cb(ncb, 0);
+                for (auto& kv : sampled) {
+                    for (auto& sh : shifts) cb[sh.first] = uint8_t((kv.first >> sh.second) & 1);
+                    out.counts[format_bits(cb.data(), ncb)] += kv.second;
+                }
+            }
+            out.strategy = "terminal_sampling";
+            out.parallel_shots = 1;
+            out.working_bytes = required;
+            out.prefix_ops = prefix_end;
+            return out;
+        }
+        // Fall back to trajectories when the sampling table exceeds the budget.
+    }
+
+    const bool cache_prefix = shots > 1 && prefix_end > 0 && state_bytes <= budget_ - worker_bytes;
+    const uint64_t prefix_bytes = cache_prefix ? state_bytes : 0;
+    // The device's concurrent-trajectory cap plays the role of Rayon's thread
+    // count: at most 65536 states, and no more than 2^28 amplitudes per batch.
+    const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(65536, (uint64_t(1) << 28) >> std::min<uint64_t>(n, 28)));
+    uint64_t workers = std::min(shots, opt_.has_max_parallel_shots ? opt_.max_parallel_shots : cap);
+    workers = std::min(workers, cap);
+    workers = std::min(workers, (budget_ - prefix_bytes) / worker_bytes);
+    workers = std::max<uint64_t>(workers, 1);
+
+    if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+    std::lock_guard<std::mutex> lk(dev_->mu);
+    dev_->activate();
+    cudaStream_t s = dev_->stream;
+    StateBatch prefix;
+    if (cache_prefix) {
+        prefix.allocate(int(n), 1, ncb, c64);
+        k::Batch pb = prefix.view(s, 1);
+        k::init_basis(pb);
+        reset_bookkeeping(prefix, 1, {seed}, s);
+        Executor pre(ops, 0, prefix_end);
+        pre.run(pb, nullptr);
+    }
+    StateBatch st;
+    st.allocate(int(n), workers, ncb, c64);
+    Executor ex(ops, cache_prefix ? prefix_end : 0, ops.size());
+    if (profile) out.shot_times.assign(shots, 0.0);
+    std::vector<uint64_t> hbits(size_t(workers) * st.cwords);
+    std::vector<uint8_t> cb(ncb);
+    for (uint64_t r0 = 0; r0 < shots; r0 += workers) {
+        const uint64_t Wr = std::min(workers, shots - r0);
+        auto t0 = clk::now();
+        k::Batch b = st.view(s, Wr);
+        if (cache_prefix)
+            k::broadcast(b, prefix.amps.p);
+        else
+            k::init_basis(b);
+        std::vector<uint64_t> seeds(Wr);
+        for (uint64_t i = 0; i < Wr; i++) seeds[i] = seed + r0 + i;  // wrapping, shots.rs:224
+        reset_bookkeeping(st, Wr, seeds, s);
+        ex.run(b, nullptr);
+        cuda_check(cudaMemcpyAsync(hbits.data(), st.cbits.p, size_t(Wr) * st.cwords * 8, cudaMemcpyDeviceToHost, s),
+                   "read classical bits");
+        check_err_flag(st, s);
+        for (uint64_t i = 0; i < Wr; i++) {
+            const uint64_t* w = hbits.data() + i * st.cwords;
+            for (uint64_t c = 0; c < ncb; c++) cb[c] = uint8_t((w[c >> 6] >> (c & 63)) & 1);
+            out.counts[format_bits(cb.data(), ncb)]++;
+        }
+        if (profile) {
+            double per = since(t0) / double(Wr);
+            for (uint64_t i = 0; i < Wr; i++) out.shot_times[r0 + i] = per;
+        }
+    }
+    out.strategy = "trajectories";
+    out.parallel_shots = workers;
+    out.working_bytes = prefix_bytes + workers * worker_bytes;
+    out.prefix_ops = cache_prefix ? prefix_end : 0;
+    return out;
+}
+
+std::unique_ptr<Result> Simulator::simulate(const char* json, size_t len) {
+    auto total0 = clk::now();
+    Circuit c = parse_circuit(json, len);
+    validate_circuit(c);
+    const uint64_t n = c.num_qubits(), ncb = c.num_cbits();
+    const uint64_t amp = opt_.precision == Precision::C64 ? 8 : 16;
+    uint64_t slen, bytes;
+    state_layout(n, amp, &slen, &bytes);
+    if (bytes > kU64Max - ncb) fail(kMemoryError, "Working memory size overflow");
+    check_budget(bytes + ncb, budget_);
+    std::vector<Operation> plan = compile(c.instructions);
+    uint64_t seed = next_seed();
+    if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+    std::lock_guard<std::mutex> lk(dev_->mu);
+    dev_->activate();
+    cudaStream_t s = dev_->stream;
+    auto res = std::make_unique<Result>();
+    res->dev = dev_;
+    res->n = n;
+    res->state.allocate(int(n), 1, ncb, opt_.precision == Precision::C64);
+    k::Batch b = res->state.view(s, 1);
+    k::init_basis(b);
+    reset_bookkeeping(res->state, 1, {seed}, s);
+    Executor ex(plan, 0, plan.size());
+    ProfileAcc acc;
+    ex.run(b, opt_.profile ? &acc : nullptr);
+    check_err_flag(res->state, s);
+    std::vector<uint64_t> hbits(res->state.cwords);
+    cuda_check(cudaMemcpyAsync(hbits.data(), res->state.cbits.p, hbits.size() * 8, cudaMemcpyDeviceToHost, s),
+               "read classical bits");
+    cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+    res->cbits.resize(ncb);
+    for (uint64_t i = 0; i < ncb; i++) res->cbits[i] = uint8_t((hbits[i >> 6] >> (i & 63)) & 1);
+    if (opt_.profile) {
+        res->profile.present = true;
+        res->profile.acc = acc;
+        res->profile.total_time = since(total0);
+    }
+    return res;
+}
+
+void Result::statevector(double* out) const {
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    const uint64_t len = uint64_t(1) << n;
+    if (!state.c64) {
+        cuda_check(cudaMemcpyAsync(out, state.amps.p, len * 16, cudaMemcpyDeviceToHost, dev->stream), "read state");
+        dev->sync();
+        return;
+    }
+    std::vector<float> tmp(len * 2);
+    cuda_check(cudaMemcpyAsync(tmp.data(), state.amps.p, len * 8, cudaMemcpyDeviceToHost, dev->stream), "read state");
+    dev->sync();
+    for (uint64_t i = 0; i < 2 * len; i++) out[i] = double(tmp[i]);
+}
+
+void Result::probabilities(const std::vector<uint64_t>& qubits, double* out) const {
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    const uint64_t m = uint64_t(1) << qubits.size();
+    DevMem buf;
+    buf.alloc(m * 8, "probabilities");
+    k::Batch b = state.view(dev->stream, 1);
+    probs_to(b, qubits, buf.as<double>());
+    cuda_check(cudaMemcpyAsync(out, buf.p, m * 8, cudaMemcpyDeviceToHost, dev->stream), "read probabilities");
+    dev->sync();
+}
+
+std::unordered_map<uint64_t, uint64_t> Result::counts(uint64_t shots, const std::vector<uint64_t>& qubits,
+                                                      uint64_t seed) const {
+    std::unordered_map<uint64_t, uint64_t> res;
+    if (shots == 0) return res;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    cudaStream_t s = dev->stream;
+    const uint64_t m = uint64_t(1) << qubits.size();
+    DevMem cdf, tmp, idx;
+    cdf.alloc(m * 8, "the sampling table");
+    k::Batch b = state.view(s, 1);
+    probs_to(b, qubits, cdf.as<double>());
+    double total = build_cdf(s, cdf.as<double>(), m, tmp);
+    if (!std::isfinite(total) || total <= 0.0) fail(kRuntimeError, "Cannot sample a state with nonfinite or zero norm");
+    k::cdf_normalize(s, cdf.as<double>(), m, total, true);
+    idx.alloc(shots * 8, "sampled outcomes");
+    k::sample(s, cdf.as<double>(), m, seed, shots, false, idx.as<uint64_t>());
+    std::vector<uint64_t> h(shots);
+    cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
+    dev->sync();
+    for (uint64_t v : h) res[v]++;
+    return res;
+}
+
+double Result::fidelity(const double* other, uint64_t len) const {
+    if (len != (uint64_t(1) << n)) return 0.0;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    DevMem o, part;
+    o.alloc(len * 16, "fidelity operand");
+    part.alloc(k::kDotBlocks * 16, "fidelity partial sums");
+    cuda_check(cudaMemcpyAsync(o.p, other, len * 16, cudaMemcpyHostToDevice, dev->stream), "upload operand");
+    k::Batch b = state.view(dev->stream, 1);
+    int nb = k::dot_partials(b, o.as<double2>(), part.as<double2>());
+    std::vector<double2> hp(nb);
+    cuda_check(cudaMemcpyAsync(hp.data(), part.p, nb * 16, cudaMemcpyDeviceToHost, dev->stream), "read partials");
+    dev->sync();
+    double re = 0, im = 0;
+    for (auto& v : hp) {
+        re += v.x;
+        im += v.y;
+    }
+    return re * re + im * im;
+}
+
+void write_shots_profile(const ShotOutput& out, double preprocessing, double fusion, double shots_total, double total,
+                         uint64_t shots) {
+    ::mkdir("dqsim_profiles", 0777);
+    struct stat stt;
+    if (::stat("dqsim_profiles", &stt) != 0 || !S_ISDIR(stt.st_mode))
+        fail(kRuntimeError, "Failed to write shots profile: cannot create dqsim_profiles");
+    auto ns = std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::system_clock::now().time_since_epoch())
+                  .count();
+    std::string path = "dqsim_profiles/statevector_shots_profile_" + std::to_string(ns) + ".json";
+    std::string j = "{\n";
+    j += "  \"preprocessing_time\": " + json_double(preprocessing) + ",\n";
+    j += "  \"fusion_time\": " + json_double(fusion) + ",\n";
+    j += "  \"shots_total_time\": " + json_double(shots_total) + ",\n";
+    j += "  \"total_time\": " + json_double(total) + ",\n";
+    j += "  \"num_shots\": " + std::to_string(shots) + ",\n";
+    j += "  \"shot_times\": [";
+    for (size_t i = 0; i < out.shot_times.size(); i++) j += (i ? ", " : "") + json_double(out.shot_times[i]);
+    j += "],\n";
+    j += "  \"execution_strategy\": \"" + out.strategy + "\",\n";
+    j += "  \"parallel_shots\": " + std::to_string(out.parallel_shots) + ",\n";
+    j += "  \"working_bytes\": " + std::to_string(out.working_bytes) + ",\n";
+    j += "  \"deterministic_prefix_ops\": " + std::to_string(out.prefix_ops) + "\n}";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) fail(kRuntimeError, "Failed to write shots profile: cannot open " + path);
+    size_t w = std::fwrite(j.data(), 1, j.size(), f);
+    std::fclose(f);
+    if (w != j.size()) fail(kRuntimeError, "Failed to write shots profile: short write");
+}
+
+}  // namespace dq

@@ -1,0 +1,92 @@
+// StatevectorSimulator / SimulationResult semantics on the device.
+//
+// Mirrors src/monolithic/statevector/simulator.rs:214-372 (constructor
+// checks, simulate, simulate_shots, result queries) and
+// src/monolithic/statevector/shots.rs:22-260 (budget arithmetic, terminal
+// sampling vs trajectories, per-shot ChaCha8 streams, last-write cbit mapping).
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "compile.hpp"
+#include "engine.hpp"
+
+namespace dq {
+
+enum class Precision { C128 = 0, C64 = 1 };
+
+struct Options {
+    bool has_seed = false;
+    uint64_t seed = 0;
+    bool profile = false;
+    uint64_t max_memory_mb = 1024;
+    bool has_max_parallel_shots = false;
+    uint64_t max_parallel_shots = 0;
+    bool sample_terminal = true;
+    Precision precision = Precision::C128;
+    int device = 0;
+};
+
+struct ShotOutput {
+    std::unordered_map<std::string, uint64_t> counts;
+    std::vector<double> shot_times;
+    std::string strategy;
+    uint64_t parallel_shots = 0;
+    uint64_t working_bytes = 0;
+    uint64_t prefix_ops = 0;
+};
+
+struct ProfileData {
+    bool present = false;
+    ProfileAcc acc;
+    double total_time = 0;
+};
+
+class Result {
+  public:
+    std::shared_ptr<Device> dev;
+    StateBatch state;
+    uint64_t n = 0;
+    std::vector<uint8_t> cbits;
+    ProfileData profile;
+
+    void statevector(double* out_interleaved) const;
+    // 2^k doubles; qubits[0] is the MSB of the output index.
+    void probabilities(const std::vector<uint64_t>& qubits, double* out) const;
+    std::unordered_map<uint64_t, uint64_t> counts(uint64_t shots, const std::vector<uint64_t>& qubits,
+                                                  uint64_t seed) const;
+    double fidelity(const double* other_interleaved, uint64_t len) const;
+};
+
+class Simulator {
+  public:
+    explicit Simulator(const Options& o);
+    ShotOutput simulate_shots(const char* json, size_t len, uint64_t shots, bool profile, double* preprocessing,
+                              double* fusion);
+    std::unique_ptr<Result> simulate(const char* json, size_t len);
+    const Options& options() const { return opt_; }
+    std::shared_ptr<Device> device() const { return dev_; }
+
+  private:
+    Options opt_;
+    uint64_t budget_ = 0;
+    std::shared_ptr<Device> dev_;
+    uint64_t next_seed();
+    ShotOutput run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots, uint64_t seed,
+                         bool profile);
+};
+
+// Writes dqsim_profiles/statevector_shots_profile_<unix_ns>.json
+// (src/profiling.rs:8-18); throws Error(kRuntimeError) on failure.
+void write_shots_profile(const ShotOutput& out, double preprocessing, double fusion, double shots_total,
+                         double total, uint64_t shots);
+
+// Parse + validate + compile with no device work (host logic only).
+std::vector<Operation> compile_json(const char* json, size_t len, uint64_t* n, uint64_t* ncb);
+
+}  // namespace dq

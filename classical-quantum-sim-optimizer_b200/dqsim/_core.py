@@ -1,0 +1,399 @@
+"""``dqsim._core`` on the B200 engine.
+
+Python surface of the reference's PyO3 module (src/lib.rs:16-31) for the dense
+statevector backend: ``StatevectorSimulator``, ``SimulationResult``,
+``SimulationProfile`` and the ``simulate_monolithic[_shots]`` wrappers, with
+the same signatures, defaults, result types and exception classes
+(src/monolithic/statevector/simulator.rs:14-372, src/simulator.rs:14-144,
+src/codecs.rs:29-64).  Every call goes through the C ABI declared in
+include/dqsim_sv.h (``libdqsim_sv.so``); ctypes releases the GIL for the
+duration of each call, as the reference does with ``py.allow_threads``.
+
+The other backends of the reference (MPS, stabilizer, P-block) are not part of
+this engine; their names exist and raise ``NotImplementedError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_LIB_NAME = "libdqsim_sv.so"
+_LIB_PATH = Path(__file__).resolve().parent / _LIB_NAME
+
+if not _LIB_PATH.exists():
+    raise ImportError(
+        f"{_LIB_NAME} is not built; run `make -C classical-quantum-sim-optimizer_b200/csrc` "
+        "(or __graft_entry__.build()) first"
+    )
+
+_lib = ctypes.CDLL(str(_LIB_PATH))
+
+_u64 = ctypes.c_uint64
+_P = ctypes.c_void_p
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [
+        ("has_seed", ctypes.c_int),
+        ("seed", _u64),
+        ("profile", ctypes.c_int),
+        ("max_memory_mb", _u64),
+        ("has_max_parallel_shots", ctypes.c_int),
+        ("max_parallel_shots", _u64),
+        ("sample_terminal", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class _Profile(ctypes.Structure):
+    _fields_ = [
+        ("apply_one_qubit_calls", _u64),
+        ("apply_one_qubit_time", ctypes.c_double),
+        ("apply_n_qubit_calls", _u64),
+        ("apply_n_qubit_time", ctypes.c_double),
+        ("measure_qubit_calls", _u64),
+        ("measure_qubit_time", ctypes.c_double),
+        ("total_time", ctypes.c_double),
+    ]
+
+
+def _sig(name, args, res=ctypes.c_int):
+    f = getattr(_lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+_last_error = _sig("dq_last_error", [], ctypes.c_char_p)
+_version = _sig("dq_version", [], ctypes.c_char_p)
+_sim_create = _sig("dq_sim_create", [ctypes.POINTER(_Options), ctypes.POINTER(_P)])
+_sim_destroy = _sig("dq_sim_destroy", [_P], None)
+_simulate_shots = _sig("dq_simulate_shots", [_P, ctypes.c_char_p, ctypes.c_size_t, _u64, ctypes.c_int,
+                                             ctypes.POINTER(_P)])
+_simulate = _sig("dq_simulate", [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_P)])
+_counts_size = _sig("dq_counts_size", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_counts_copy = _sig("dq_counts_copy", [_P, _P, _P])
+_counts_free = _sig("dq_counts_free", [_P], None)
+_res_nq = _sig("dq_result_num_qubits", [_P, ctypes.POINTER(_u64)])
+_res_ncb = _sig("dq_result_num_cbits", [_P, ctypes.POINTER(_u64)])
+_res_sv = _sig("dq_result_statevector", [_P, _P, _u64])
+_res_cbits = _sig("dq_result_classical_bits", [_P, _P, _u64])
+_res_profile = _sig("dq_result_profile", [_P, ctypes.POINTER(_Profile), ctypes.POINTER(ctypes.c_int)])
+_res_probs = _sig("dq_result_probabilities", [_P, _P, ctypes.c_size_t, ctypes.c_int, _P, _u64])
+_res_counts = _sig("dq_result_counts", [_P, _u64, _P, ctypes.c_size_t, ctypes.c_int, _u64, ctypes.c_int,
+                                        ctypes.POINTER(_P)])
+_res_fidelity = _sig("dq_result_fidelity", [_P, _P, _u64, ctypes.POINTER(ctypes.c_double)])
+_res_free = _sig("dq_result_free", [_P], None)
+_compile_dump = _sig("dq_compile_dump", [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p)])
+_string_free = _sig("dq_string_free", [ctypes.c_void_p], None)
+
+_ERRORS = {
+    1: ValueError,
+    2: MemoryError,
+    3: TypeError,
+    4: RuntimeError,
+    5: NotImplementedError,
+    6: RuntimeError,
+}
+
+PRECISIONS = {"complex128": 0, "c128": 0, "fp64": 0, "complex64": 1, "c64": 1, "fp32": 1}
+
+
+def _check(status):
+    if status != 0:
+        msg = _last_error().decode("utf-8", "replace")
+        raise _ERRORS.get(status, RuntimeError)(msg)
+
+
+def _as_u64(value, name):
+    """PyO3 usize/u64 extraction: ints only, in range."""
+    if isinstance(value, bool) or not isinstance(value, (int, np.integer)):
+        raise TypeError(f"argument '{name}': '{type(value).__name__}' object cannot be interpreted as an integer")
+    value = int(value)
+    if value < 0 or value > (1 << 64) - 1:
+        raise OverflowError(f"argument '{name}': out of range integral type conversion attempted")
+    return value
+
+
+def _as_bool(value, name):
+    if not isinstance(value, (bool, np.bool_)):
+        raise TypeError(f"argument '{name}': '{type(value).__name__}' object cannot be converted to 'PyBool'")
+    return bool(value)
+
+
+def _circuit_json(circuit):
+    text = circuit.model_dump_json()
+    if isinstance(text, bytes):
+        return text
+    if not isinstance(text, str):
+        raise TypeError("model_dump_json() must return a string")
+    return text.encode("utf-8")
+
+
+def _take_counts(handle):
+    try:
+        n, w = _u64(), _u64()
+        _check(_counts_size(handle, ctypes.byref(n), ctypes.byref(w)))
+        n, w = n.value, w.value
+        keys = ctypes.create_string_buffer(max(1, n * w))
+        counts = (_u64 * max(1, n))()
+        _check(_counts_copy(handle, keys, counts))
+        raw = keys.raw
+        return {raw[i * w:(i + 1) * w].decode("ascii"): int(counts[i]) for i in range(n)}
+    finally:
+        _counts_free(handle)
+
+
+def _qubit_list(qubits):
+    if qubits is None:
+        return None
+    return [_as_u64(q, "qubits") for q in qubits]
+
+
+class SimulationProfile:
+    """Per-category execution counters of one trajectory (simulator.rs:43-79)."""
+
+    __slots__ = ("apply_one_qubit_calls", "apply_one_qubit_time", "apply_n_qubit_calls", "apply_n_qubit_time",
+                 "measure_qubit_calls", "measure_qubit_time", "total_time")
+
+    def __init__(self, p):
+        for name in self.__slots__:
+            setattr(self, name, getattr(p, name))
+
+    def __repr__(self):
+        total = max(self.total_time, 1e-9)
+        return (
+            f"SimulationProfile (total: {self.total_time * 1000.0:.2f} ms)\n"
+            f"  apply_one_qubit : {self.apply_one_qubit_calls:4} calls  {self.apply_one_qubit_time * 1000.0:8.2f} ms"
+            f"  ({100.0 * self.apply_one_qubit_time / total:.1f}%)\n"
+            f"  apply_n_qubit   : {self.apply_n_qubit_calls:4} calls  {self.apply_n_qubit_time * 1000.0:8.2f} ms"
+            f"  ({100.0 * self.apply_n_qubit_time / total:.1f}%)\n"
+            f"  measure_qubit   : {self.measure_qubit_calls:4} calls  {self.measure_qubit_time * 1000.0:8.2f} ms"
+            f"  ({100.0 * self.measure_qubit_time / total:.1f}%)"
+        )
+
+
+class SimulationResult:
+    """A final state held in device memory (simulator.rs:85-191)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        n = _u64()
+        _check(_res_nq(handle, ctypes.byref(n)))
+        self._n = n.value
+        ncb = _u64()
+        _check(_res_ncb(handle, ctypes.byref(ncb)))
+        self._ncb = ncb.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _res_free(h)
+            self._h = None
+
+    @property
+    def num_qubits(self):
+        return self._n
+
+    @property
+    def statevector(self):
+        """An independent complex128 NumPy copy of shape (2^n,)."""
+        out = np.empty(1 << self._n, dtype=np.complex128)
+        _check(_res_sv(self._h, out.ctypes.data_as(_P), 2 * out.shape[0]))
+        return out
+
+    @property
+    def classical_bits(self):
+        buf = np.zeros(max(1, self._ncb), dtype=np.uint8)
+        _check(_res_cbits(self._h, buf.ctypes.data_as(_P), self._ncb))
+        return {i: int(buf[i]) for i in range(self._ncb)}
+
+    @property
+    def profile(self):
+        p, has = _Profile(), ctypes.c_int()
+        _check(_res_profile(self._h, ctypes.byref(p), ctypes.byref(has)))
+        return SimulationProfile(p) if has.value else None
+
+    def probabilities(self, qubits=None):
+        """{basis index: probability} for p > 0; qubits[0] is the output MSB."""
+        qs = _qubit_list(qubits)
+        k = self._n if qs is None else len(qs)
+        if qs is not None:
+            for i, q in enumerate(qs):
+                if q >= self._n or q in qs[:i]:
+                    raise ValueError("Query qubits must be distinct and within the statevector's range")
+        arr = np.asarray(qs if qs is not None else [0], dtype=np.uint64)
+        out = np.empty(1 << k, dtype=np.float64)
+        _check(_res_probs(self._h, arr.ctypes.data_as(_P), len(qs or []), 0 if qs is None else 1,
+                          out.ctypes.data_as(_P), out.shape[0]))
+        nz = np.flatnonzero(out > 0.0)
+        return dict(zip(nz.tolist(), out[nz].tolist()))
+
+    def counts(self, shots=1000, qubits=None, seed=None):
+        """Sample the current state; one ChaCha8 stream for all shots (engine.rs:457-507)."""
+        shots = _as_u64(shots, "shots")
+        qs = _qubit_list(qubits)
+        arr = np.asarray(qs if qs is not None else [0], dtype=np.uint64)
+        has_seed = seed is not None
+        seed_v = _as_u64(seed, "seed") if has_seed else 0
+        h = _P()
+        _check(_res_counts(self._h, shots, arr.ctypes.data_as(_P), len(qs or []), 0 if qs is None else 1, seed_v,
+                           1 if has_seed else 0, ctypes.byref(h)))
+        return _take_counts(h)
+
+    def fidelity(self, other):
+        """|<self|other>|^2 for a complex128 array; 0.0 on a length mismatch."""
+        arr = np.asarray(other)
+        if arr.dtype != np.complex128 or arr.ndim != 1:
+            raise TypeError("fidelity expects a one-dimensional complex128 array")
+        arr = np.ascontiguousarray(arr)
+        out = ctypes.c_double()
+        _check(_res_fidelity(self._h, arr.ctypes.data_as(_P), arr.shape[0], ctypes.byref(out)))
+        return out.value
+
+
+class StatevectorSimulator:
+    """Dense statevector simulator on one B200 (simulator.rs:213-372).
+
+    ``max_memory_mb`` bounds device working memory with the reference's
+    arithmetic (state + classical buffers + terminal CDF); ``max_parallel_shots``
+    bounds the trajectories one device batch runs at once.  ``precision``
+    selects the plain complex128 form (default) or the fused complex64 form.
+    """
+
+    def __init__(self, seed=None, profile=False, *, max_memory_mb=1024, max_parallel_shots=None,
+                 sample_terminal=True, precision="complex128", device=0):
+        o = _Options()
+        o.has_seed = 0 if seed is None else 1
+        o.seed = 0 if seed is None else _as_u64(seed, "seed")
+        o.profile = 1 if _as_bool(profile, "profile") else 0
+        o.max_memory_mb = _as_u64(max_memory_mb, "max_memory_mb")
+        o.has_max_parallel_shots = 0 if max_parallel_shots is None else 1
+        o.max_parallel_shots = 0 if max_parallel_shots is None else _as_u64(max_parallel_shots, "max_parallel_shots")
+        o.sample_terminal = 1 if _as_bool(sample_terminal, "sample_terminal") else 0
+        key = str(precision).lower()
+        if key not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(set(PRECISIONS))}")
+        o.precision = PRECISIONS[key]
+        o.device = int(device)
+        h = _P()
+        _check(_sim_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.precision = "complex64" if o.precision else "complex128"
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _sim_destroy(h)
+            self._h = None
+
+    def simulate_shots(self, circuit, shots=1000, profile=False):
+        """Classical-register counts (simulator.rs:256-317)."""
+        text = _circuit_json(circuit)
+        shots = _as_u64(shots, "shots")
+        profile = _as_bool(profile, "profile")
+        h = _P()
+        _check(_simulate_shots(self._h, text, len(text), shots, 1 if profile else 0, ctypes.byref(h)))
+        return _take_counts(h)
+
+    def simulate(self, circuit):
+        """One trajectory; measurements collapse the returned state (simulator.rs:319-371)."""
+        text = _circuit_json(circuit)
+        h = _P()
+        _check(_simulate(self._h, text, len(text), ctypes.byref(h)))
+        return SimulationResult(h)
+
+
+# ---------------------------------------------------------------------------
+# Wrappers, src/simulator.rs:14-144 and src/codecs.rs:29-64
+# ---------------------------------------------------------------------------
+def _parse_mode(mode):
+    key = str(mode).strip().lower().replace("-", "_")
+    if key in ("state_vector", "statevector", "sv"):
+        return "sv"
+    if key in ("mps", "matrix_product_state", "stabilizer", "stab"):
+        raise NotImplementedError(f"The {key!r} backend is not provided by the B200 statevector engine")
+    raise ValueError(f"Unsupported monolithic simulation mode {key!r}; expected 'state_vector' or 'mps'")
+
+
+_SV_OPTIONS = ("max_memory_mb", "max_parallel_shots", "sample_terminal", "precision", "device")
+
+
+def _parse_options(options):
+    out = {"max_memory_mb": 1024, "max_parallel_shots": None, "sample_terminal": True}
+    for key, value in options.items():
+        if key not in _SV_OPTIONS:
+            raise TypeError(f"Unsupported statevector option {key!r}")
+        out[key] = value
+    return out
+
+
+def simulate_monolithic(circuit, mode="state_vector", seed=None, profile=False, **options):
+    _parse_mode(mode)
+    opts = _parse_options(options)
+    return StatevectorSimulator(seed, profile, **opts).simulate(circuit)
+
+
+def simulate_monolithic_shots(circuit, mode="state_vector", shots=1000, seed=None, profile=False, **options):
+    _parse_mode(mode)
+    opts = _parse_options(options)
+    return StatevectorSimulator(seed, False, **opts).simulate_shots(circuit, shots, profile)
+
+
+def _not_provided(name):
+    def __init__(self, *args, **kwargs):
+        raise NotImplementedError(f"{name} is not provided by the B200 statevector engine")
+
+    return type(name, (), {"__init__": __init__, "__doc__": f"{name}: not provided (statevector engine only)."})
+
+
+MpsSimulator = _not_provided("MpsSimulator")
+MpsResult = _not_provided("MpsResult")
+StabilizerSimulator = _not_provided("StabilizerSimulator")
+StabilizerResult = _not_provided("StabilizerResult")
+PBlockSimulator = _not_provided("PBlockSimulator")
+PBlockResult = _not_provided("PBlockResult")
+
+
+def simulate_distributed(distributed, mode="p_block", seed=None, profile=False, **options):
+    raise NotImplementedError("The P-block backend is not provided by the B200 statevector engine")
+
+
+def simulate_distributed_shots(distributed, mode="p_block", shots=1000, seed=None, profile=False, **options):
+    raise NotImplementedError("The P-block backend is not provided by the B200 statevector engine")
+
+
+def compile_dump(circuit_json):
+    """Host-only: the fused operation list of a transport JSON string (for tests)."""
+    import json as _json
+
+    text = circuit_json.encode("utf-8") if isinstance(circuit_json, str) else circuit_json
+    out = ctypes.c_char_p()
+    _check(_compile_dump(text, len(text), ctypes.byref(out)))
+    try:
+        return _json.loads(out.value.decode("utf-8"))
+    finally:
+        _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+def library_path():
+    return str(_LIB_PATH)
+
+
+def version():
+    return _version().decode()
+
+
+__all__ = [
+    "MpsSimulator", "MpsResult", "PBlockResult", "PBlockSimulator", "SimulationProfile", "SimulationResult",
+    "StabilizerSimulator", "StabilizerResult", "StatevectorSimulator", "simulate_distributed",
+    "simulate_distributed_shots", "simulate_monolithic", "simulate_monolithic_shots",
+]
+
+if os.environ.get("DQSIM_DEBUG_LIB"):
+    print("dqsim loaded", _LIB_PATH)

@@ -1,0 +1,140 @@
+/*
+ * dqsim_sv.h - C ABI of the B200 dense-statevector engine.
+ *
+ * This is the drop-in seam for dqsim's StatevectorSimulator backend.  The
+ * reference binds the same operations through PyO3; every entry point below
+ * names the reference method it replaces (paths relative to the dqsim project
+ * root).  All functions return a dq_status; on failure dq_last_error() holds
+ * a message for the calling thread.  No C++ exceptions cross this boundary,
+ * no torch or CUDA types appear in the signatures, and every buffer is a
+ * plain host pointer with an explicit size.
+ *
+ * Conventions (src/types.rs, docs/simulators.md:5-90):
+ *   - circuits are the transport JSON produced by model_dump_json();
+ *   - amplitudes are little-endian: qubit 0 is the least significant bit;
+ *   - query qubit lists put their first qubit in the most significant bit;
+ *   - count keys are '0'/'1' strings, classical bit 0 rightmost.
+ */
+#ifndef DQSIM_SV_H
+#define DQSIM_SV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DQ_API __attribute__((visibility("default")))
+#else
+#define DQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; each maps to the Python exception the reference raises. */
+typedef enum dq_status {
+    DQ_OK = 0,
+    DQ_VALUE_ERROR = 1,     /* ValueError: parse, validation, query, options */
+    DQ_MEMORY_ERROR = 2,    /* MemoryError: budget or allocation failure */
+    DQ_TYPE_ERROR = 3,      /* TypeError: unsupported option */
+    DQ_RUNTIME_ERROR = 4,   /* RuntimeError: profile write, nonfinite norm */
+    DQ_NOT_IMPLEMENTED = 5, /* NotImplementedError: backend not provided */
+    DQ_CUDA_ERROR = 6       /* RuntimeError: CUDA failure */
+} dq_status;
+
+typedef enum dq_precision {
+    DQ_COMPLEX128 = 0, /* plain form: complex128 state, per-operation FP64 kernels */
+    DQ_COMPLEX64 = 1   /* fused form: complex64 state, fused <=5-qubit blocks */
+} dq_precision;
+
+typedef struct dq_sim dq_sim;
+typedef struct dq_result dq_result;
+typedef struct dq_counts dq_counts;
+
+/* Constructor options of StatevectorSimulator.__new__
+ * (src/monolithic/statevector/simulator.rs:225-254). */
+typedef struct dq_sim_options {
+    int has_seed;
+    uint64_t seed;
+    int profile;
+    uint64_t max_memory_mb;      /* default 1024; the budget of device working memory */
+    int has_max_parallel_shots;
+    uint64_t max_parallel_shots; /* concurrent device trajectories */
+    int sample_terminal;         /* default 1 */
+    int precision;               /* dq_precision, default DQ_COMPLEX128 */
+    int device;                  /* CUDA device ordinal, default 0 */
+} dq_sim_options;
+
+/* Per-category counters of SimulationProfile (simulator.rs:43-59). */
+typedef struct dq_profile {
+    uint64_t apply_one_qubit_calls;
+    double apply_one_qubit_time;
+    uint64_t apply_n_qubit_calls;
+    double apply_n_qubit_time;
+    uint64_t measure_qubit_calls;
+    double measure_qubit_time;
+    double total_time;
+} dq_profile;
+
+/* Message of the last failed call on this thread ("" if none). */
+DQ_API const char* dq_last_error(void);
+
+/* Library version string. */
+DQ_API const char* dq_version(void);
+
+/* Fill `opts` with the reference's defaults. */
+DQ_API void dq_sim_options_default(dq_sim_options* opts);
+
+/* StatevectorSimulator(seed, profile, *, max_memory_mb, max_parallel_shots,
+ * sample_terminal): simulator.rs:225-254.  Checks options only; the CUDA
+ * device is opened on first use. */
+DQ_API int dq_sim_create(const dq_sim_options* opts, dq_sim** out);
+DQ_API void dq_sim_destroy(dq_sim* sim);
+
+/* StatevectorSimulator.simulate_shots(circuit, shots, profile):
+ * simulator.rs:258-317 with run_shots, shots.rs:59-260.  With profile set,
+ * writes dqsim_profiles/statevector_shots_profile_<ns>.json. */
+DQ_API int dq_simulate_shots(dq_sim* sim, const char* json, size_t json_len, uint64_t shots, int profile,
+                      dq_counts** out);
+
+/* StatevectorSimulator.simulate(circuit): simulator.rs:320-371 (one trajectory). */
+DQ_API int dq_simulate(dq_sim* sim, const char* json, size_t json_len, dq_result** out);
+
+/* Count maps: `key_width` characters per key, keys concatenated without separators. */
+DQ_API int dq_counts_size(const dq_counts* c, uint64_t* n_keys, uint64_t* key_width);
+DQ_API int dq_counts_copy(const dq_counts* c, char* keys, uint64_t* counts);
+DQ_API void dq_counts_free(dq_counts* c);
+
+/* SimulationResult (simulator.rs:85-191). */
+DQ_API int dq_result_num_qubits(const dq_result* r, uint64_t* n);
+DQ_API int dq_result_num_cbits(const dq_result* r, uint64_t* n);
+/* .statevector: 2 * 2^n doubles (re, im interleaved), an independent copy. */
+DQ_API int dq_result_statevector(const dq_result* r, double* out, uint64_t out_len);
+/* .classical_bits: one byte (0/1) per classical bit. */
+DQ_API int dq_result_classical_bits(const dq_result* r, uint8_t* out, uint64_t out_len);
+/* .profile: *has = 0 when the simulator ran without profiling. */
+DQ_API int dq_result_profile(const dq_result* r, dq_profile* out, int* has);
+/* .probabilities(qubits): out receives 2^k doubles; qubits[0] is the MSB.
+ * has_qubits = 0 selects all qubits in descending order. */
+DQ_API int dq_result_probabilities(const dq_result* r, const uint64_t* qubits, size_t k, int has_qubits, double* out,
+                            uint64_t out_len);
+/* .counts(shots, qubits, seed): keys are k-bit strings, qubits[0] leftmost.
+ * has_seed = 0 draws a fresh seed. */
+DQ_API int dq_result_counts(const dq_result* r, uint64_t shots, const uint64_t* qubits, size_t k, int has_qubits,
+                     uint64_t seed, int has_seed, dq_counts** out);
+/* .fidelity(other): |<self|other>|^2; 0.0 when the lengths differ. */
+DQ_API int dq_result_fidelity(const dq_result* r, const double* other, uint64_t other_len, double* out);
+DQ_API void dq_result_free(dq_result* r);
+
+/* Host-only helpers (no device work): parse, validate and compile a circuit
+ * exactly as read_circuit + compile do (simulator.rs:204-211,
+ * execution.rs:368-416), returning the operation list as JSON text with
+ * doubles as 16-hex-digit bit patterns.  Free the text with dq_string_free. */
+DQ_API int dq_compile_dump(const char* json, size_t json_len, char** out_text);
+DQ_API void dq_string_free(char* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DQSIM_SV_H */
