@@ -1,12 +1,19 @@
 // extern "C" layer: exceptions become status codes plus a thread-local message.
+#include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <random>
 
 #include "../../include/dqsim_sv.h"
+#include "plan.hpp"
 #include "simulator.hpp"
 
 using namespace dq;
+
+struct dq_plan {
+    std::unique_ptr<Plan> impl;
+};
 
 struct dq_sim {
     std::unique_ptr<Simulator> impl;
@@ -96,6 +103,15 @@ int dq_sim_create(const dq_sim_options* opts, dq_sim** out) {
             fail(kValueError, "precision must be complex128 or complex64");
         o.precision = Precision(opts->precision);
         o.device = opts->device;
+        if (opts->execution < 0 || opts->execution > 2) fail(kValueError, "execution must be auto, per_gate or tiled");
+        if (opts->tile_qubits < 0 || opts->tile_qubits > 14 || (opts->tile_qubits > 0 && opts->tile_qubits < 5))
+            fail(kValueError, "tile_qubits must be 0 (auto) or between 5 and 14");
+        if (opts->tile_qubits == 14 && opts->precision == DQ_COMPLEX128)
+            fail(kValueError, "a 14-qubit complex128 tile exceeds shared memory");
+        if (opts->fusion_width < 0 || opts->fusion_width > 5) fail(kValueError, "fusion_width must be between 0 and 5");
+        o.execution = opts->execution;
+        o.tile_qubits = opts->tile_qubits;
+        o.fusion_width = opts->fusion_width;
         auto s = std::make_unique<dq_sim>();
         s->impl = std::make_unique<Simulator>(o);
         *out = s.release();
@@ -252,6 +268,74 @@ int dq_result_fidelity(const dq_result* r, const double* other, uint64_t other_l
 
 void dq_result_free(dq_result* r) { delete r; }
 
+int dq_plan_create(dq_sim* sim, const char* json, size_t len, uint64_t shots, dq_plan** out) {
+    return guard([&] {
+        need(sim, "sim");
+        need(json, "json");
+        need(out, "out");
+        auto p = std::make_unique<dq_plan>();
+        p->impl = std::make_unique<Plan>(*sim->impl, json, len, shots);
+        *out = p.release();
+    });
+}
+
+int dq_plan_run(dq_plan* p, int record, double* device_ms) {
+    return guard([&] {
+        need(p, "plan");
+        double ms = p->impl->run(record != 0);
+        if (device_ms) *device_ms = ms;
+    });
+}
+
+int dq_plan_stats(const dq_plan* p, double* ms, uint64_t* launches, double* bytes) {
+    return guard([&] {
+        need(p, "plan");
+        need(ms, "ms");
+        need(launches, "launches");
+        need(bytes, "bytes");
+        p->impl->stats(ms, launches, bytes);
+    });
+}
+
+int dq_plan_info(const dq_plan* p, uint64_t* num_qubits, uint64_t* num_ops, double* state_bytes) {
+    return guard([&] {
+        need(p, "plan");
+        if (num_qubits) *num_qubits = p->impl->num_qubits();
+        if (num_ops) *num_ops = p->impl->num_ops();
+        if (state_bytes) *state_bytes = p->impl->state_bytes();
+    });
+}
+
+int dq_plan_statevector(const dq_plan* p, double* out, uint64_t out_len) {
+    return guard([&] {
+        need(p, "plan");
+        need(out, "out");
+        if (out_len != (uint64_t(2) << p->impl->num_qubits())) fail(kValueError, "statevector buffer has the wrong length");
+        p->impl->statevector(out);
+    });
+}
+
+int dq_plan_samples(const dq_plan* p, uint64_t* out, uint64_t out_len) {
+    return guard([&] {
+        need(p, "plan");
+        need(out, "out");
+        if (out_len != p->impl->shots()) fail(kValueError, "sample buffer has the wrong length");
+        p->impl->samples(out);
+    });
+}
+
+int dq_plan_compare(const dq_plan* a, const dq_plan* b, double* fidelity, double* max_abs_err) {
+    return guard([&] {
+        need(a, "a");
+        need(b, "b");
+        need(fidelity, "fidelity");
+        need(max_abs_err, "max_abs_err");
+        a->impl->compare(*b->impl, fidelity, max_abs_err);
+    });
+}
+
+void dq_plan_free(dq_plan* p) { delete p; }
+
 int dq_compile_dump(const char* json, size_t len, char** out_text) {
     return guard([&] {
         need(json, "json");
@@ -262,6 +346,56 @@ int dq_compile_dump(const char* json, size_t len, char** out_text) {
         if (!buf) throw std::bad_alloc();
         std::memcpy(buf, s.c_str(), s.size() + 1);
         *out_text = buf;
+    });
+}
+
+int dq_tile_plan_dump(const char* json, size_t len, int tile_qubits, int fusion_width, char** out_text) {
+    return guard([&] {
+        need(json, "json");
+        need(out_text, "out_text");
+        uint64_t n = 0, ncb = 0;
+        auto ops = compile_json(json, len, &n, &ncb);
+        for (auto& op : ops)
+            if (!tileable(op)) fail(kValueError, "circuit has operations a tile pass cannot apply");
+        TilePlanOptions o;
+        o.m = tile_qubits;
+        o.fuse = std::min(fusion_width, kTileMaxDense);
+        std::vector<double2> pool;
+        auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
+        std::string s = "{\"n\":" + std::to_string(n) + ",\"passes\":[";
+        char buf[64];
+        for (size_t pi = 0; pi < passes.size(); pi++) {
+            const TilePass& p = passes[pi];
+            s += pi ? ",{" : "{";
+            s += "\"raw\":" + std::to_string(p.raw_ops) + ",\"qubits\":[";
+            for (size_t i = 0; i < p.qubits.size(); i++) s += (i ? "," : "") + std::to_string(p.qubits[i]);
+            s += "],\"ops\":[";
+            for (size_t oi = 0; oi < p.ops.size(); oi++) {
+                const TileOp& t = p.ops[oi];
+                s += oi ? ",{" : "{";
+                s += "\"type\":" + std::to_string(t.type) + ",\"k\":" + std::to_string(t.k) + ",\"ins\":[";
+                for (int i = 0; i < t.nins; i++) s += (i ? "," : "") + std::to_string(t.ins[i]);
+                s += "],\"q\":[";
+                for (int i = 0; i < t.k; i++) s += (i ? "," : "") + std::to_string(t.q[i]);
+                s += "],\"offs\":[";
+                for (int i = 0; t.type == TileOp::kDense && i < (1 << t.k); i++)
+                    s += (i ? "," : "") + std::to_string(t.offs[i]);
+                s += "],\"fixed\":" + std::to_string(t.fixed) + ",\"tbit\":" + std::to_string(t.tbit) +
+                     ",\"lowbit\":" + std::to_string(t.lowbit) + ",\"highbit\":" + std::to_string(t.highbit) +
+                     ",\"mat\":" + std::to_string(t.mat) + "}";
+            }
+            s += "]}";
+        }
+        s += "],\"pool\":[";
+        for (size_t i = 0; i < pool.size(); i++) {
+            std::snprintf(buf, sizeof buf, "%s[%.17g,%.17g]", i ? "," : "", pool[i].x, pool[i].y);
+            s += buf;
+        }
+        s += "]}";
+        char* out = static_cast<char*>(std::malloc(s.size() + 1));
+        if (!out) throw std::bad_alloc();
+        std::memcpy(out, s.c_str(), s.size() + 1);
+        *out_text = out;
     });
 }
 

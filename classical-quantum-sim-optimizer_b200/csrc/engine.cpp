@@ -87,11 +87,124 @@ namespace {
 double2 d2(cplx c) { return make_double2(c.re, c.im); }
 }  // namespace
 
-Executor::Executor(const std::vector<Operation>& ops, size_t begin, size_t end) {
+const char* kernel_class_name(int c) {
+    static const char* names[kcNumClasses] = {"gate1q", "controlled", "diagonal", "swap", "dense",
+                                              "measure", "tile", "fused", "sample"};
+    return (c >= 0 && c < kcNumClasses) ? names[c] : "?";
+}
+
+EventRecorder::~EventRecorder() {
+    for (auto& r : recs_) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : pool_) cudaEventDestroy(e);
+}
+
+cudaEvent_t EventRecorder::take() {
+    if (!pool_.empty()) {
+        cudaEvent_t e = pool_.back();
+        pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+void EventRecorder::begin(int cls, double bytes) {
+    Rec r{cls, bytes, take(), take()};
+    cuda_check(cudaEventRecord(r.a, stream_), "cudaEventRecord");
+    recs_.push_back(r);
+}
+
+void EventRecorder::end() { cuda_check(cudaEventRecord(recs_.back().b, stream_), "cudaEventRecord"); }
+
+void EventRecorder::collect(double* ms, uint64_t* launches, double* bytes) {
+    cuda_check(cudaStreamSynchronize(stream_), "stream synchronize");
+    for (int c = 0; c < kcNumClasses; c++) {
+        ms[c] = 0;
+        launches[c] = 0;
+        bytes[c] = 0;
+    }
+    for (auto& r : recs_) {
+        float t = 0;
+        cuda_check(cudaEventElapsedTime(&t, r.a, r.b), "cudaEventElapsedTime");
+        ms[r.cls] += t;
+        launches[r.cls] += 1;
+        bytes[r.cls] += r.bytes;
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+    }
+    recs_.clear();
+}
+
+double Executor::step_bytes(size_t i, const k::Batch& b) const {
+    const Step& s = steps_[i];
+    const double S = b.c64 ? 8.0 : 16.0;
+    const double full = S * double(uint64_t(1) << b.n) * double(b.W);
+    if (s.pass >= 0) return 2.0 * full;
+    switch (s.type) {
+        case Operation::One:
+        case Operation::X: return 2.0 * full / double(uint64_t(1) << s.controls.size());
+        case Operation::Swap: return full / double(uint64_t(1) << s.controls.size());
+        case Operation::Diagonal: {
+            int kq = int(s.qubits.size()), e = 0;
+            for (auto& d : s.diag)
+                if (!(d.x == 1.0 && d.y == 0.0)) e++;
+            if (e * 2 <= (1 << kq)) return 2.0 * full * e / double(1 << kq);
+            return 2.0 * full;
+        }
+        case Operation::Dense: return 2.0 * full;
+        case Operation::Measure:
+        case Operation::Reset: return 2.5 * full;
+        default: return 0.0;
+    }
+}
+
+Executor::Executor(const std::vector<Operation>& ops, size_t begin, size_t end, const ExecConfig& cfg) : cfg_(cfg) {
+    size_t seg = begin;
+    if (cfg_.fuse > kTileMaxDense) cfg_.fuse = kTileMaxDense;
     for (size_t i = begin; i < end; i++) {
+        if (cfg_.tiled && tileable(ops[i])) continue;
+        if (seg < i) lower_segment(ops, seg, i);
         std::vector<Condition> conds;
         lower(ops[i], conds);
+        seg = i + 1;
     }
+    if (seg < end) lower_segment(ops, seg, end);
+}
+
+void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end) {
+    if (!cfg_.tiled || cfg_.n < 1) {
+        for (size_t i = begin; i < end; i++) {
+            std::vector<Condition> conds;
+            lower(ops[i], conds);
+        }
+        return;
+    }
+    TilePlanOptions o;
+    o.m = cfg_.tile_m;
+    o.fuse = cfg_.fuse;
+    o.seeds = cfg_.seeds;
+    o.c64 = cfg_.c64;
+    std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
+    for (auto& p : ps) {
+        p.op_begin = int(tile_ops_host_.size());
+        tile_ops_host_.insert(tile_ops_host_.end(), p.ops.begin(), p.ops.end());
+        Step s;
+        s.pass = int(passes_.size());
+        s.type = Operation::Dense;
+        s.category = 1;
+        passes_.push_back(std::move(p));
+        steps_.push_back(std::move(s));
+    }
+}
+
+size_t Executor::raw_ops_in_passes() const {
+    size_t t = 0;
+    for (auto& p : passes_) t += size_t(p.raw_ops);
+    return t;
 }
 
 void Executor::lower(const Operation& op, std::vector<Condition>& conds) {
@@ -157,7 +270,7 @@ void Executor::lower(const Operation& op, std::vector<Condition>& conds) {
     steps_.push_back(std::move(s));
 }
 
-void Executor::run(const k::Batch& b, ProfileAcc* profile) {
+void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
     if (!uploaded_) {
         if (!pool_host_.empty()) {
             pool_.alloc(pool_host_.size() * sizeof(double2), "gate matrices");
@@ -165,10 +278,17 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile) {
                                        cudaMemcpyHostToDevice, b.stream),
                        "upload gate matrices");
         }
+        if (!tile_ops_host_.empty()) {
+            tile_ops_.alloc(tile_ops_host_.size() * sizeof(TileOp), "tile operations");
+            cuda_check(cudaMemcpyAsync(tile_ops_.p, tile_ops_host_.data(), tile_ops_host_.size() * sizeof(TileOp),
+                                       cudaMemcpyHostToDevice, b.stream),
+                       "upload tile operations");
+        }
         uploaded_ = true;
     }
     std::vector<uint64_t> host_cbits;
-    for (const Step& s : steps_) {
+    for (size_t si = 0; si < steps_.size(); si++) {
+        const Step& s = steps_[si];
         if (profile && s.cond.n) {
             // Profiling counts only executed operations (execution.rs:285-295),
             // so the host reads the single trajectory's classical bits here.
@@ -189,6 +309,32 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile) {
             if (!ok) continue;
         }
         auto t0 = std::chrono::steady_clock::now();
+        if (s.pass >= 0) {
+            const TilePass& p = passes_[size_t(s.pass)];
+            if (rec) rec->begin(kcTile, step_bytes(si, b));
+            const int m = int(p.qubits.size());
+            k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()), pool_.as<double2>(),
+                         p);
+            if (rec) rec->end();
+            if (profile) {
+                cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+                profile->nq_calls++;
+                profile->nq_time += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            }
+            continue;
+        }
+        if (rec) {
+            int cls = kcGate1q;
+            switch (s.type) {
+                case Operation::One: cls = s.controls.empty() ? kcGate1q : kcControlled; break;
+                case Operation::X: cls = kcControlled; break;
+                case Operation::Swap: cls = kcSwap; break;
+                case Operation::Diagonal: cls = kcDiagonal; break;
+                case Operation::Dense: cls = kcDense; break;
+                default: cls = kcMeasure; break;
+            }
+            rec->begin(cls, step_bytes(si, b));
+        }
         switch (s.type) {
             case Operation::One: k::gate1q(b, s.target, s.controls, s.u, false, s.cond); break;
             case Operation::X: k::gate1q(b, s.target, s.controls, s.u, true, s.cond); break;
@@ -199,6 +345,7 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile) {
             case Operation::Reset: k::measure(b, s.target, -1, true, s.cond); break;
             default: break;
         }
+        if (rec) rec->end();
         if (profile) {
             cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
             double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

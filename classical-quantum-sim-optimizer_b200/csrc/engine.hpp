@@ -10,6 +10,7 @@
 
 #include "compile.hpp"
 #include "kernels.hpp"
+#include "tile.hpp"
 
 namespace dq {
 
@@ -60,22 +61,78 @@ struct ProfileAcc {
     double oq_time = 0, nq_time = 0, mq_time = 0;
 };
 
-// A compiled operation list lowered to launch descriptors, with every dense
-// matrix uploaded once into a device pool.  `fuse_1q_runs` is off for the
-// reference-faithful per-gate form.
+// Kernel classes timed by the event recorder (bench and roofline).
+enum KernelClass : int {
+    kcGate1q = 0,    // uncontrolled 2x2 on pairs
+    kcControlled,    // controlled 2x2 / X on pairs
+    kcDiagonal,
+    kcSwap,
+    kcDense,
+    kcMeasure,
+    kcTile,          // shared-memory multi-gate pass
+    kcFused,         // tensor-core fused-block pass
+    kcSample,
+    kcNumClasses
+};
+const char* kernel_class_name(int c);
+
+// Records a CUDA event pair around each launch of the stream, tagged with a
+// kernel class and the launch's algorithmic bytes; durations are read after
+// the stream drains.
+class EventRecorder {
+  public:
+    explicit EventRecorder(cudaStream_t s) : stream_(s) {}
+    ~EventRecorder();
+    void begin(int cls, double bytes);
+    void end();
+    // Totals per class: milliseconds, launches, algorithmic bytes.
+    void collect(double* ms, uint64_t* launches, double* bytes);
+
+  private:
+    struct Rec {
+        int cls;
+        double bytes;
+        cudaEvent_t a, b;
+    };
+    cudaStream_t stream_;
+    std::vector<Rec> recs_;
+    std::vector<cudaEvent_t> pool_;
+    cudaEvent_t take();
+};
+
+// How an executor lowers unitary runs.
+struct ExecConfig {
+    bool tiled = false;  // shared-memory tile passes for unconditioned unitary runs
+    int tile_m = 12;     // tile qubits
+    int fuse = 2;        // widest fused dense operation inside a pass
+    int seeds = 6;       // planner candidates per pass
+    int n = 0;           // qubits of the state the plan runs on
+    bool c64 = false;
+};
+
+// A compiled operation list lowered to launch descriptors, with every matrix
+// uploaded once into a device pool.  Per-gate steps are one launch per
+// operation (the reference-faithful plain form); tiled steps run a planned
+// shared-memory pass over every tile of the state.
 class Executor {
   public:
-    Executor(const std::vector<Operation>& ops, size_t begin, size_t end);
+    Executor(const std::vector<Operation>& ops, size_t begin, size_t end, const ExecConfig& cfg = ExecConfig());
     // Launch every step on the batch (asynchronously unless `profile`).
-    void run(const k::Batch& b, ProfileAcc* profile);
+    void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr);
     size_t steps() const { return steps_.size(); }
+    // Algorithmic bytes one step moves for a batch (the roofline numerator).
+    double step_bytes(size_t i, const k::Batch& b) const;
+
+    size_t passes() const { return passes_.size(); }
+    size_t raw_ops_in_passes() const;
 
   private:
     struct Step {
+        int pass = -1;  // >= 0: a tile pass (index into passes_)
         Operation::Type type;
         int target = 0, a = 0, b = 0;
         std::vector<k::Ctl> controls;
-        double2 u[4];
+        double2 u[4] = {};
         std::vector<int> qubits;
         std::vector<double2> diag;
         size_t pool_offset = 0;  // Dense: index into the matrix pool (double2 units)
@@ -86,9 +143,13 @@ class Executor {
     };
     std::vector<Step> steps_;
     std::vector<double2> pool_host_;
-    DevMem pool_;
+    std::vector<TilePass> passes_;
+    std::vector<TileOp> tile_ops_host_;
+    DevMem pool_, tile_ops_;
     bool uploaded_ = false;
+    ExecConfig cfg_;
     void lower(const Operation& op, std::vector<Condition>& conds);
+    void lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end);
 };
 
 }  // namespace dq

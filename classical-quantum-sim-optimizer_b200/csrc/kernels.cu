@@ -452,6 +452,22 @@ __global__ void k_cdf_normalize(double* __restrict__ cdf, uint64_t len, double t
     }
 }
 
+__global__ void k_take_total(const double* __restrict__ cdf, uint64_t len, double* scalar, int* err) {
+    double t = cdf[len - 1];
+    *scalar = t;
+    if (!(isfinite(t) && t > 0.0)) *err = 1;
+}
+
+__global__ void k_cdf_normalize_dev(double* __restrict__ cdf, uint64_t len, const double* __restrict__ scalar,
+                                    int clamp) {
+    const double total = *scalar;
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x) {
+        double v = cdf[g] / total;
+        if (clamp) v = fmin(v, 1.0);
+        cdf[g] = (g == len - 1) ? 1.0 : v;
+    }
+}
+
 __global__ void k_sample(const double* __restrict__ cdf, uint64_t len, uint64_t seed, uint64_t shots, int per_shot,
                          uint64_t* __restrict__ out) {
     uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -482,6 +498,33 @@ __global__ void __launch_bounds__(256) k_dot(const V* __restrict__ a, const doub
     }
     block_sum2(re, im);
     if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(re, im);
+}
+
+template <typename VA, typename VB>
+__global__ void __launch_bounds__(256) k_compare(const VA* __restrict__ a, const VB* __restrict__ b, uint64_t len,
+                                                double* __restrict__ partial) {
+    double re = 0.0, im = 0.0, mx = 0.0;
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x) {
+        VA x = a[g];
+        VB y = b[g];
+        double xr = x.x, xi = x.y, yr = y.x, yi = y.y;
+        re += xr * yr + xi * yi;
+        im += xr * yi - xi * yr;
+        double dr = xr - yr, di = xi - yi;
+        mx = fmax(mx, sqrt(dr * dr + di * di));
+    }
+    block_sum2(re, im);
+    __shared__ double smx[32];
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) smx[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); w++) m = fmax(m, smx[w]);
+        partial[blockIdx.x * 3] = re;
+        partial[blockIdx.x * 3 + 1] = im;
+        partial[blockIdx.x * 3 + 2] = m;
+    }
 }
 
 __global__ void k_widen(const float2* __restrict__ s, double2* __restrict__ out, uint64_t len) {
@@ -726,6 +769,12 @@ void cdf_normalize(cudaStream_t s, double* cdf, uint64_t len, double total, bool
     check_launch("cdf_normalize");
 }
 
+void cdf_normalize_device(cudaStream_t s, double* cdf, uint64_t len, double* scalar, int* err, bool clamp) {
+    k_take_total<<<1, 1, 0, s>>>(cdf, len, scalar, err);
+    k_cdf_normalize_dev<<<stream_grid(len), 256, 0, s>>>(cdf, len, scalar, clamp ? 1 : 0);
+    check_launch("cdf_normalize_device");
+}
+
 void sample(cudaStream_t s, const double* cdf, uint64_t len, uint64_t seed, uint64_t shots, bool per_shot_seed,
             uint64_t* out) {
     if (shots == 0) return;
@@ -741,6 +790,22 @@ int dot_partials(const Batch& b, const double2* other, double2* partial) {
         k_dot<double2><<<kDotBlocks, 256, 0, b.stream>>>(static_cast<const double2*>(b.amps), other, len, partial);
     check_launch("dot");
     return kDotBlocks;
+}
+
+void compare(cudaStream_t s, const void* a, bool a64, const void* b, bool b64, uint64_t len, double* partial) {
+    if (!a64 && !b64)
+        k_compare<double2, double2><<<kDotBlocks, 256, 0, s>>>(static_cast<const double2*>(a),
+                                                               static_cast<const double2*>(b), len, partial);
+    else if (!a64 && b64)
+        k_compare<double2, float2><<<kDotBlocks, 256, 0, s>>>(static_cast<const double2*>(a),
+                                                              static_cast<const float2*>(b), len, partial);
+    else if (a64 && !b64)
+        k_compare<float2, double2><<<kDotBlocks, 256, 0, s>>>(static_cast<const float2*>(a),
+                                                              static_cast<const double2*>(b), len, partial);
+    else
+        k_compare<float2, float2><<<kDotBlocks, 256, 0, s>>>(static_cast<const float2*>(a),
+                                                             static_cast<const float2*>(b), len, partial);
+    check_launch("compare");
 }
 
 void widen(const Batch& b, double2* out) {

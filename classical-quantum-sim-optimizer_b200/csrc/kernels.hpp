@@ -75,6 +75,9 @@ size_t scan_tmp_size(uint64_t len);
 void scan(cudaStream_t s, double* x, uint64_t len, double* tmp);
 // cdf[i] = cdf[i] / total (clamped to 1 when clamp), cdf[len-1] = 1.
 void cdf_normalize(cudaStream_t s, double* cdf, uint64_t len, double total, bool clamp);
+// Same with the total taken from cdf[len-1] on the device (copied to `scalar`
+// first); sets *err when the total is not finite and positive.
+void cdf_normalize_device(cudaStream_t s, double* cdf, uint64_t len, double* scalar, int* err, bool clamp);
 // out[t] = min(partition_point(cdf, draw_t), len-1); per_shot_seed: draw_t is the
 // first draw of seed+t, otherwise draw t of the stream `seed`.
 void sample(cudaStream_t s, const double* cdf, uint64_t len, uint64_t seed, uint64_t shots, bool per_shot_seed,
@@ -84,6 +87,9 @@ int dot_partials(const Batch& b, const double2* other, double2* partial);
 constexpr int kDotBlocks = 1184;
 // c64 -> c128 widening copy of state 0.
 void widen(const Batch& b, double2* out);
+// Per-block partials of <a|b> and max |a_i - b_i| for two states of `len`
+// amplitudes, each c128 or c64; partial holds kDotBlocks * 3 doubles.
+void compare(cudaStream_t s, const void* a, bool a64, const void* b, bool b64, uint64_t len, double* partial);
 
 }  // namespace k
 }  // namespace dq

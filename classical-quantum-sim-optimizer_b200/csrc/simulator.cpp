@@ -93,6 +93,16 @@ std::string json_double(double v) {
 
 }  // namespace
 
+ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate) {
+    ExecConfig c;
+    c.c64 = o.precision == Precision::C64;
+    c.tiled = !force_per_gate && o.execution != 1;
+    c.tile_m = o.tile_qubits > 0 ? o.tile_qubits : (c.c64 ? 13 : 12);
+    c.fuse = o.fusion_width > 0 ? o.fusion_width : 2;
+    c.n = int(n);
+    return c;
+}
+
 std::vector<Operation> compile_json(const char* json, size_t len, uint64_t* n, uint64_t* ncb) {
     Circuit c = parse_circuit(json, len);
     validate_circuit(c);
@@ -183,7 +193,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
         const uint64_t cdf_bytes = (uint64_t(1) << kq) * 8;
         if (worker_bytes <= kU64Max - cdf_bytes && worker_bytes + cdf_bytes <= budget_) {
             const uint64_t required = worker_bytes + cdf_bytes;
-            if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+            ensure_device();
             std::lock_guard<std::mutex> lk(dev_->mu);
             dev_->activate();
             cudaStream_t s = dev_->stream;
@@ -194,7 +204,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 k::Batch b = st.view(s, 1);
                 k::init_basis(b);
                 reset_bookkeeping(st, 1, {kept_seed}, s);
-                Executor ex(ops, 0, prefix_end);
+                Executor ex(ops, 0, prefix_end, exec_config(opt_, n));
                 ex.run(b, nullptr);
                 DevMem cdf, tmp, idx;
                 const uint64_t clen = uint64_t(1) << kq;
@@ -236,7 +246,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
     workers = std::min(workers, (budget_ - prefix_bytes) / worker_bytes);
     workers = std::max<uint64_t>(workers, 1);
 
-    if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+    ensure_device();
     std::lock_guard<std::mutex> lk(dev_->mu);
     dev_->activate();
     cudaStream_t s = dev_->stream;
@@ -246,12 +256,12 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
         k::Batch pb = prefix.view(s, 1);
         k::init_basis(pb);
         reset_bookkeeping(prefix, 1, {seed}, s);
-        Executor pre(ops, 0, prefix_end);
+        Executor pre(ops, 0, prefix_end, exec_config(opt_, n));
         pre.run(pb, nullptr);
     }
     StateBatch st;
     st.allocate(int(n), workers, ncb, c64);
-    Executor ex(ops, cache_prefix ? prefix_end : 0, ops.size());
+    Executor ex(ops, cache_prefix ? prefix_end : 0, ops.size(), exec_config(opt_, n));
     if (profile) out.shot_times.assign(shots, 0.0);
     std::vector<uint64_t> hbits(size_t(workers) * st.cwords);
     std::vector<uint8_t> cb(ncb);
@@ -299,7 +309,7 @@ std::unique_ptr<Result> Simulator::simulate(const char* json, size_t len) {
     check_budget(bytes + ncb, budget_);
     std::vector<Operation> plan = compile(c.instructions);
     uint64_t seed = next_seed();
-    if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+    ensure_device();
     std::lock_guard<std::mutex> lk(dev_->mu);
     dev_->activate();
     cudaStream_t s = dev_->stream;
@@ -310,7 +320,8 @@ std::unique_ptr<Result> Simulator::simulate(const char* json, size_t len) {
     k::Batch b = res->state.view(s, 1);
     k::init_basis(b);
     reset_bookkeeping(res->state, 1, {seed}, s);
-    Executor ex(plan, 0, plan.size());
+    // Profiling times each reference operation, so it runs the per-gate form.
+    Executor ex(plan, 0, plan.size(), exec_config(opt_, n, opt_.profile));
     ProfileAcc acc;
     ex.run(b, opt_.profile ? &acc : nullptr);
     check_err_flag(res->state, s);

@@ -30,7 +30,13 @@ struct Options {
     bool sample_terminal = true;
     Precision precision = Precision::C128;
     int device = 0;
+    int execution = 0;      // 0 auto (tiled), 1 per-gate, 2 tiled
+    int tile_qubits = 0;    // 0: 12 for complex128, 13 for complex64
+    int fusion_width = 0;   // 0: 2
 };
+
+// Executor configuration for a state of n qubits under these options.
+ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate = false);
 
 struct ShotOutput {
     std::unordered_map<std::string, uint64_t> counts;
@@ -70,11 +76,17 @@ class Simulator {
                               double* fusion);
     std::unique_ptr<Result> simulate(const char* json, size_t len);
     const Options& options() const { return opt_; }
-    std::shared_ptr<Device> device() const { return dev_; }
+    // Opens the CUDA device on first use.
+    std::shared_ptr<Device> ensure_device() {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
+        return dev_;
+    }
 
   private:
     Options opt_;
     uint64_t budget_ = 0;
+    std::mutex mu_;
     std::shared_ptr<Device> dev_;
     uint64_t next_seed();
     ShotOutput run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots, uint64_t seed,

@@ -1,0 +1,659 @@
+// Shared-memory tile pass kernel and its host-side planner.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <set>
+
+#include "common.hpp"
+#include "tile.hpp"
+
+namespace dq {
+
+// ---------------------------------------------------------------------------
+// Dense matrices of operations (qubits[0] = MSB of the matrix index)
+// ---------------------------------------------------------------------------
+namespace {
+
+void op_matrix(const Operation& op, std::vector<uint64_t>& qs, std::vector<cplx>& mat) {
+    qs.clear();
+    auto controlled = [&](const std::vector<Control>& cs, int tk, auto&& inner) {
+        // qubits = controls..., targets...; identity unless every control matches.
+        for (auto& c : cs) qs.push_back(c.qubit);
+        int k = int(qs.size()) + tk;
+        int dim = 1 << k;
+        mat.assign(size_t(dim) * dim, cplx(0));
+        uint32_t want = 0;
+        for (size_t i = 0; i < cs.size(); i++)
+            if (cs[i].value) want |= 1u << (cs.size() - 1 - i);
+        for (int r = 0; r < dim; r++) {
+            uint32_t cr = uint32_t(r) >> tk;
+            if (cr != want) {
+                mat[size_t(r) * dim + r] = cplx(1);
+                continue;
+            }
+            for (int c = 0; c < (1 << tk); c++) {
+                int col = int((cr << tk) | uint32_t(c));
+                mat[size_t(r) * dim + col] = inner(r & ((1 << tk) - 1), c);
+            }
+        }
+    };
+    switch (op.type) {
+        case Operation::One:
+            controlled(op.controls, 1, [&](int r, int c) { return op.m[r][c]; });
+            qs.push_back(op.target);
+            break;
+        case Operation::X:
+            controlled(op.controls, 1, [&](int r, int c) { return cplx(r != c ? 1.0 : 0.0); });
+            qs.push_back(op.target);
+            break;
+        case Operation::Swap:
+            controlled(op.controls, 2, [&](int r, int c) {
+                int sw = ((c & 1) << 1) | ((c >> 1) & 1);
+                return cplx(r == sw ? 1.0 : 0.0);
+            });
+            qs.push_back(op.a);
+            qs.push_back(op.b);
+            break;
+        case Operation::Diagonal: {
+            qs = op.qubits;
+            size_t dim = op.values.size();
+            mat.assign(dim * dim, cplx(0));
+            for (size_t i = 0; i < dim; i++) mat[i * dim + i] = op.values[i];
+            break;
+        }
+        case Operation::Dense:
+            qs = op.qubits;
+            mat = op.values;
+            break;
+        default: fail(kValueError, "operation has no matrix form");
+    }
+}
+
+// E = op matrix embedded on block qubits `bq` (MSB-first), then out = E * acc.
+void left_multiply(const std::vector<uint64_t>& bq, std::vector<cplx>& acc, const std::vector<uint64_t>& oq,
+                   const std::vector<cplx>& om) {
+    const int k = int(bq.size()), ko = int(oq.size());
+    const int dim = 1 << k, odim = 1 << ko;
+    std::vector<int> pos(ko);  // bit position (LSB = 0) of each op qubit in the block index
+    uint32_t opmask = 0;
+    for (int t = 0; t < ko; t++) {
+        int idx = int(std::find(bq.begin(), bq.end(), oq[t]) - bq.begin());
+        pos[t] = k - 1 - idx;
+        opmask |= 1u << pos[t];
+    }
+    auto extract = [&](int j) {
+        int v = 0;
+        for (int t = 0; t < ko; t++) v = (v << 1) | ((j >> pos[t]) & 1);
+        return v;
+    };
+    auto deposit = [&](int v) {
+        int j = 0;
+        for (int t = 0; t < ko; t++)
+            if ((v >> (ko - 1 - t)) & 1) j |= 1 << pos[t];
+        return j;
+    };
+    std::vector<cplx> out(size_t(dim) * dim, cplx(0));
+    for (int r = 0; r < dim; r++) {
+        int ro = extract(r);
+        int rest = r & ~int(opmask);
+        for (int c = 0; c < dim; c++) {
+            cplx s(0);
+            for (int x = 0; x < odim; x++) {
+                cplx e = om[size_t(ro) * odim + x];
+                if (e.re == 0.0 && e.im == 0.0) continue;
+                int mid = rest | deposit(x);
+                s = s + e * acc[size_t(mid) * dim + c];
+            }
+            out[size_t(r) * dim + c] = s;
+        }
+    }
+    acc.swap(out);
+}
+
+bool is_identity_1(const cplx& v) { return v.re == 1.0 && v.im == 0.0; }
+
+}  // namespace
+
+std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
+    if (width <= 1) return ops;
+    const size_t N = ops.size();
+    std::vector<std::vector<uint64_t>> qs(N);
+    for (size_t i = 0; i < N; i++) qs[i] = ops[i].touched();
+    std::vector<char> done(N, 0);
+    std::vector<Operation> out;
+    for (size_t first = 0; first < N; first++) {
+        if (done[first]) continue;
+        if (qs[first].size() > size_t(width)) {
+            done[first] = 1;
+            out.push_back(ops[first]);
+            continue;
+        }
+        std::vector<size_t> members{first};
+        std::vector<uint64_t> bq = qs[first];
+        done[first] = 1;
+        // qubits blocked by an unfused operation that stays after this block
+        std::set<uint64_t> blocked;
+        for (size_t o = first + 1; o < N; o++) {
+            if (done[o]) continue;
+            bool touches_blocked = false;
+            for (auto q : qs[o])
+                if (blocked.count(q)) touches_blocked = true;
+            std::set<uint64_t> uni(bq.begin(), bq.end());
+            for (auto q : qs[o]) uni.insert(q);
+            if (!touches_blocked && uni.size() <= size_t(width)) {
+                for (auto q : qs[o])
+                    if (std::find(bq.begin(), bq.end(), q) == bq.end()) bq.push_back(q);
+                members.push_back(o);
+                done[o] = 1;
+            } else {
+                for (auto q : qs[o]) blocked.insert(q);
+            }
+            if (blocked.size() >= 64) break;
+        }
+        if (members.size() == 1) {
+            out.push_back(ops[first]);
+            continue;
+        }
+        std::sort(bq.begin(), bq.end(), std::greater<uint64_t>());
+        const int dim = 1 << bq.size();
+        std::vector<cplx> acc(size_t(dim) * dim, cplx(0));
+        for (int i = 0; i < dim; i++) acc[size_t(i) * dim + i] = cplx(1);
+        std::vector<uint64_t> oq;
+        std::vector<cplx> om;
+        for (size_t mi : members) {
+            op_matrix(ops[mi], oq, om);
+            left_multiply(bq, acc, oq, om);
+        }
+        Operation d;
+        d.type = Operation::Dense;
+        d.qubits = bq;
+        d.values = acc;
+        // Keep diagonal structure (cheaper kernels) when the product is diagonal.
+        bool diag = true;
+        for (int r = 0; r < dim && diag; r++)
+            for (int c = 0; c < dim; c++)
+                if (r != c && (acc[size_t(r) * dim + c].re != 0.0 || acc[size_t(r) * dim + c].im != 0.0)) {
+                    diag = false;
+                    break;
+                }
+        if (diag) {
+            d.type = Operation::Diagonal;
+            std::vector<cplx> dv(dim);
+            for (int i = 0; i < dim; i++) dv[i] = acc[size_t(i) * dim + i];
+            d.values = dv;
+        }
+        out.push_back(std::move(d));
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Pass planner
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Dag {
+    std::vector<std::vector<uint64_t>> qs;
+    std::vector<std::vector<size_t>> per_qubit;  // op indices touching each qubit, in order
+};
+
+struct PlanState {
+    std::vector<size_t> head;   // per qubit: position in per_qubit list
+    std::vector<char> done;
+    size_t first_open = 0;
+};
+
+bool ready(const Dag& g, const PlanState& s, size_t o) {
+    for (auto q : g.qs[o])
+        if (g.per_qubit[q][s.head[q]] != o) return false;
+    return true;
+}
+
+void take(const Dag& g, PlanState& s, size_t o) {
+    s.done[o] = 1;
+    for (auto q : g.qs[o]) s.head[q]++;
+    while (s.first_open < s.done.size() && s.done[s.first_open]) s.first_open++;
+}
+
+bool subset(const std::vector<uint64_t>& a, const std::vector<char>& inT) {
+    for (auto q : a)
+        if (!inT[q]) return false;
+    return true;
+}
+
+// Absorb every ready op inside T until nothing changes; returns ops taken.
+size_t closure(const Dag& g, PlanState& s, const std::vector<char>& inT, std::vector<size_t>* taken) {
+    size_t count = 0;
+    bool changed = true;
+    while (changed) {
+        changed = false;
+        for (size_t o = s.first_open; o < s.done.size(); o++) {
+            if (s.done[o] || !subset(g.qs[o], inT) || !ready(g, s, o)) continue;
+            take(g, s, o);
+            if (taken) taken->push_back(o);
+            count++;
+            changed = true;
+        }
+    }
+    return count;
+}
+
+// Grow T from a seed op and absorb; returns (ops, T) without committing.
+size_t grow(const Dag& g, PlanState s, size_t seed, int m, int n, std::vector<char>& inT, std::vector<size_t>* taken) {
+    inT.assign(n, 0);
+    int size = 0;
+    for (auto q : g.qs[seed])
+        if (!inT[q]) {
+            inT[q] = 1;
+            size++;
+        }
+    size_t total = closure(g, s, inT, taken);
+    while (size < m) {
+        // the ready op needing the fewest new qubits (earliest on ties)
+        size_t best = SIZE_MAX;
+        int best_new = 1 << 30;
+        for (size_t o = s.first_open; o < s.done.size(); o++) {
+            if (s.done[o] || !ready(g, s, o)) continue;
+            int nw = 0;
+            for (auto q : g.qs[o]) nw += inT[q] ? 0 : 1;
+            if (nw == 0 || size + nw > m) continue;
+            if (nw < best_new) {
+                best_new = nw;
+                best = o;
+                if (nw == 1) break;
+            }
+        }
+        if (best == SIZE_MAX) break;
+        for (auto q : g.qs[best])
+            if (!inT[q]) {
+                inT[q] = 1;
+                size++;
+            }
+        total += closure(g, s, inT, taken);
+    }
+    return total;
+}
+
+TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::vector<double2>& pool,
+                     std::vector<TileOp>& out) {
+    TileOp t;
+    std::memset(&t, 0, sizeof t);
+    auto L = [&](uint64_t q) { return local[q]; };
+    auto set_ins = [&](std::vector<int> pos) {
+        std::sort(pos.begin(), pos.end());
+        t.nins = int(pos.size());
+        for (size_t i = 0; i < pos.size(); i++) t.ins[i] = pos[i];
+    };
+    auto d2 = [](cplx c) { return make_double2(c.re, c.im); };
+    switch (op.type) {
+        case Operation::One:
+        case Operation::X: {
+            t.type = op.type == Operation::One ? TileOp::kOne : TileOp::kX;
+            std::vector<int> pos{L(op.target)};
+            for (auto& c : op.controls) {
+                pos.push_back(L(c.qubit));
+                if (c.value) t.fixed |= 1u << L(c.qubit);
+            }
+            set_ins(pos);
+            t.tbit = 1u << L(op.target);
+            t.mat = int(pool.size());
+            if (op.type == Operation::One) {
+                pool.push_back(d2(op.m[0][0]));
+                pool.push_back(d2(op.m[0][1]));
+                pool.push_back(d2(op.m[1][0]));
+                pool.push_back(d2(op.m[1][1]));
+            }
+            out.push_back(t);
+            break;
+        }
+        case Operation::Swap: {
+            t.type = TileOp::kSwap;
+            std::vector<int> pos{L(op.a), L(op.b)};
+            for (auto& c : op.controls) {
+                pos.push_back(L(c.qubit));
+                if (c.value) t.fixed |= 1u << L(c.qubit);
+            }
+            set_ins(pos);
+            int lo = std::min(L(op.a), L(op.b)), hi = std::max(L(op.a), L(op.b));
+            t.lowbit = 1u << lo;
+            t.highbit = 1u << hi;
+            out.push_back(t);
+            break;
+        }
+        case Operation::Diagonal: {
+            const int kq = int(op.qubits.size());
+            std::vector<int> nontrivial;
+            for (int j = 0; j < (1 << kq); j++)
+                if (!is_identity_1(op.values[j])) nontrivial.push_back(j);
+            if (nontrivial.empty()) break;
+            std::vector<int> lq;
+            for (auto q : op.qubits) lq.push_back(L(q));
+            if (int(nontrivial.size()) * 2 <= (1 << kq)) {
+                for (int j : nontrivial) {
+                    TileOp e;
+                    std::memset(&e, 0, sizeof e);
+                    e.type = TileOp::kDiagEntry;
+                    std::vector<int> pos(lq);
+                    std::sort(pos.begin(), pos.end());
+                    e.nins = int(pos.size());
+                    for (size_t i = 0; i < pos.size(); i++) e.ins[i] = pos[i];
+                    for (int b = 0; b < kq; b++)
+                        if ((j >> (kq - 1 - b)) & 1) e.fixed |= 1u << lq[b];
+                    e.mat = int(pool.size());
+                    pool.push_back(d2(op.values[j]));
+                    out.push_back(e);
+                }
+            } else {
+                t.type = TileOp::kDiagFull;
+                t.k = kq;
+                for (int b = 0; b < kq; b++) t.q[b] = lq[b];
+                t.mat = int(pool.size());
+                for (auto& v : op.values) pool.push_back(d2(v));
+                out.push_back(t);
+            }
+            break;
+        }
+        case Operation::Dense: {
+            t.type = TileOp::kDense;
+            t.k = int(op.qubits.size());
+            std::vector<int> lq;
+            for (auto q : op.qubits) lq.push_back(L(q));
+            for (int b = 0; b < t.k; b++) t.q[b] = lq[b];
+            set_ins(lq);
+            for (int j = 0; j < (1 << t.k); j++) {
+                uint32_t o = 0;
+                for (int b = 0; b < t.k; b++)
+                    if ((j >> (t.k - 1 - b)) & 1) o |= 1u << lq[b];
+                t.offs[j] = o;
+            }
+            t.mat = int(pool.size());
+            for (auto& v : op.values) pool.push_back(d2(v));
+            out.push_back(t);
+            break;
+        }
+        default: fail(kValueError, "operation cannot run inside a tile pass");
+    }
+    return t;
+}
+
+}  // namespace
+
+std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                                 const TilePlanOptions& opt, std::vector<double2>* pool) {
+    std::vector<TilePass> passes;
+    const size_t N = end - begin;
+    if (N == 0) return passes;
+    // A pass holds every qubit of each of its operations.
+    int widest = 1;
+    for (size_t i = begin; i < end; i++) widest = std::max(widest, int(ops[i].touched().size()));
+    const int m = std::min(std::max(opt.m, widest), n);
+    Dag g;
+    g.qs.resize(N);
+    g.per_qubit.assign(n, {});
+    for (size_t i = 0; i < N; i++) {
+        g.qs[i] = ops[begin + i].touched();
+        for (auto q : g.qs[i]) g.per_qubit[q].push_back(i);
+    }
+    PlanState s;
+    s.head.assign(n, 0);
+    s.done.assign(N, 0);
+    while (s.first_open < N) {
+        // candidate seeds: the first `seeds` ready ops
+        std::vector<size_t> seeds;
+        for (size_t o = s.first_open; o < N && int(seeds.size()) < std::max(1, opt.seeds); o++)
+            if (!s.done[o] && ready(g, s, o)) seeds.push_back(o);
+        size_t best_seed = seeds[0], best_count = 0;
+        for (size_t sd : seeds) {
+            std::vector<char> inT;
+            size_t c = grow(g, s, sd, m, n, inT, nullptr);
+            if (c > best_count) {
+                best_count = c;
+                best_seed = sd;
+            }
+        }
+        std::vector<char> inT;
+        std::vector<size_t> taken;
+        grow(g, s, best_seed, m, n, inT, &taken);
+        for (size_t o : taken) take(g, s, o);
+        // pad T to m qubits with the lowest free qubits (longer contiguous rows)
+        int size = 0;
+        for (int q = 0; q < n; q++) size += inT[q];
+        for (int q = 0; q < n && size < m; q++)
+            if (!inT[q]) {
+                inT[q] = 1;
+                size++;
+            }
+        TilePass p;
+        for (int q = 0; q < n; q++)
+            if (inT[q]) p.qubits.push_back(q);
+        std::vector<int> local(n, -1);
+        for (size_t i = 0; i < p.qubits.size(); i++) local[p.qubits[i]] = int(i);
+        std::vector<Operation> pass_ops;
+        for (size_t o : taken) pass_ops.push_back(ops[begin + o]);
+        p.raw_ops = int(pass_ops.size());
+        std::vector<Operation> fused = fuse_ops(pass_ops, opt.fuse);
+        for (auto& op : fused) lower_tile_op(op, local, *pool, p.ops);
+        passes.push_back(std::move(p));
+    }
+    return passes;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel
+// ---------------------------------------------------------------------------
+namespace k {
+namespace {
+
+constexpr int kTileThreads = 256;
+
+struct TileQubits {
+    int m;
+    int q[20];
+};
+
+__device__ __forceinline__ uint32_t expand_local(uint32_t j, const TileOp& op) {
+#pragma unroll
+    for (int t = 0; t < 7; t++) {
+        if (t < op.nins) {
+            uint32_t low = (1u << op.ins[t]) - 1;
+            j = (j & low) | ((j & ~low) << 1);
+        }
+    }
+    return j;
+}
+
+template <typename V, int K>
+__device__ void tile_dense(V* __restrict__ tile, const TileOp& op, int m, const double2* __restrict__ pool) {
+    constexpr int D = 1 << K;
+    const uint32_t items = 1u << (m - K);
+    const double2* mat = pool + op.mat;
+    for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
+        const uint32_t base = expand_local(j, op);
+        V v[D];
+#pragma unroll
+        for (int c = 0; c < D; c++) v[c] = tile[base | op.offs[c]];
+#pragma unroll 1
+        for (int r = 0; r < D; r++) {
+            V acc = dev::czero<V>();
+#pragma unroll
+            for (int c = 0; c < D; c++) acc = dev::cadd(acc, dev::cmul(dev::from_d2<V>(__ldg(mat + r * D + c)), v[c]));
+            tile[base | op.offs[r]] = acc;
+        }
+    }
+}
+
+template <typename V>
+__device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const double2* __restrict__ pool) {
+    switch (op.type) {
+        case TileOp::kOne:
+        case TileOp::kX: {
+            const uint32_t items = 1u << (m - op.nins);
+            const bool is_x = op.type == TileOp::kX;
+            V u00 = dev::czero<V>(), u01 = u00, u10 = u00, u11 = u00;
+            if (!is_x) {
+                u00 = dev::from_d2<V>(__ldg(pool + op.mat));
+                u01 = dev::from_d2<V>(__ldg(pool + op.mat + 1));
+                u10 = dev::from_d2<V>(__ldg(pool + op.mat + 2));
+                u11 = dev::from_d2<V>(__ldg(pool + op.mat + 3));
+            }
+            for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
+                const uint32_t i0 = expand_local(j, op) | op.fixed, i1 = i0 | op.tbit;
+                V a = tile[i0], b = tile[i1];
+                if (is_x) {
+                    tile[i0] = b;
+                    tile[i1] = a;
+                } else {
+                    tile[i0] = dev::cadd(dev::cmul(u00, a), dev::cmul(u01, b));
+                    tile[i1] = dev::cadd(dev::cmul(u10, a), dev::cmul(u11, b));
+                }
+            }
+            break;
+        }
+        case TileOp::kDiagEntry: {
+            const uint32_t items = 1u << (m - op.nins);
+            const V v = dev::from_d2<V>(__ldg(pool + op.mat));
+            for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
+                const uint32_t i = expand_local(j, op) | op.fixed;
+                tile[i] = dev::cmul(tile[i], v);
+            }
+            break;
+        }
+        case TileOp::kDiagFull: {
+            const uint32_t items = 1u << m;
+            for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
+                uint32_t jj = 0;
+                for (int b = 0; b < op.k; b++) jj = (jj << 1) | ((i >> op.q[b]) & 1u);
+                tile[i] = dev::cmul(tile[i], dev::from_d2<V>(__ldg(pool + op.mat + jj)));
+            }
+            break;
+        }
+        case TileOp::kSwap: {
+            const uint32_t items = 1u << (m - op.nins);
+            for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
+                const uint32_t i = expand_local(j, op) | op.fixed;
+                V a = tile[i | op.lowbit];
+                tile[i | op.lowbit] = tile[i | op.highbit];
+                tile[i | op.highbit] = a;
+            }
+            break;
+        }
+        case TileOp::kDense:
+            switch (op.k) {
+                case 1: tile_dense<V, 1>(tile, op, m, pool); break;
+                case 2: tile_dense<V, 2>(tile, op, m, pool); break;
+                case 3: tile_dense<V, 3>(tile, op, m, pool); break;
+            }
+            break;
+    }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kTileThreads) k_tile(V* __restrict__ s, int n, int m, TileQubits tq,
+                                                       const TileOp* __restrict__ ops, int nops,
+                                                       const double2* __restrict__ pool, uint64_t total_tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    const int lb = m < 6 ? m : 6;
+    uint64_t* lo_tab = reinterpret_cast<uint64_t*>(smem_raw + (sizeof(V) << m));
+    uint64_t* hi_tab = lo_tab + (1 << lb);
+    // offsets of tile-local index bits: low lb bits and the rest
+    for (int e = threadIdx.x; e < (1 << lb); e += blockDim.x) {
+        uint64_t off = 0;
+        for (int b = 0; b < lb; b++)
+            if ((e >> b) & 1) off |= uint64_t(1) << tq.q[b];
+        lo_tab[e] = off;
+    }
+    for (int e = threadIdx.x; e < (1 << (m - lb)); e += blockDim.x) {
+        uint64_t off = 0;
+        for (int b = 0; b < m - lb; b++)
+            if ((e >> b) & 1) off |= uint64_t(1) << tq.q[lb + b];
+        hi_tab[e] = off;
+    }
+    __syncthreads();
+    const int rest = n - m;
+    const uint32_t size = 1u << m;
+    const uint32_t lmask = (1u << lb) - 1;
+    for (uint64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        const uint64_t st = t >> rest;
+        uint64_t tid = t & ((uint64_t(1) << rest) - 1);
+        // insert zeros at the tile qubits (ascending)
+        for (int b = 0; b < m; b++) {
+            uint64_t low = (uint64_t(1) << tq.q[b]) - 1;
+            tid = (tid & low) | ((tid & ~low) << 1);
+        }
+        V* __restrict__ g = s + ((st << n) | tid);
+        constexpr int U = 4;
+        for (uint32_t e0 = threadIdx.x; e0 < size; e0 += blockDim.x * U) {
+            V r[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                uint32_t e = e0 + u * blockDim.x;
+                if (e < size) r[u] = g[lo_tab[e & lmask] | hi_tab[e >> lb]];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                uint32_t e = e0 + u * blockDim.x;
+                if (e < size) tile[e] = r[u];
+            }
+        }
+        __syncthreads();
+        for (int i = 0; i < nops; i++) {
+            tile_apply<V>(tile, ops[i], m, pool);
+            __syncthreads();
+        }
+        for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) g[lo_tab[e & lmask] | hi_tab[e >> lb]] = tile[e];
+        __syncthreads();
+    }
+}
+
+int sm_count() {
+    static int c = 0;
+    if (!c) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        if (c <= 0) c = 148;
+    }
+    return c;
+}
+
+template <typename V>
+void tile_pass_t(const Batch& b, int m, const TileOp* ops, int nops, const double2* pool, const TilePass& hp) {
+    TileQubits tq{};
+    tq.m = m;
+    for (int i = 0; i < m; i++) tq.q[i] = hp.qubits[i];
+    const size_t smem = tile_smem_bytes(m, sizeof(V) == 8);
+    static size_t configured[2] = {0, 0};
+    size_t& conf = configured[sizeof(V) == 8 ? 1 : 0];
+    if (smem > conf) {
+        cudaFuncSetAttribute(k_tile<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        conf = smem;
+    }
+    const uint64_t total = b.W << (b.n - m);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<V>, kTileThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = std::min<uint64_t>(total, uint64_t(sm_count()) * per_sm);
+    k_tile<V><<<unsigned(grid), kTileThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq, ops, nops, pool,
+                                                                 total);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(kCudaError, std::string("tile pass: ") + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+size_t tile_smem_bytes(int m, bool c64) {
+    int lb = m < 6 ? m : 6;
+    return (size_t(c64 ? 8 : 16) << m) + 8 * ((size_t(1) << lb) + (size_t(1) << (m - lb)));
+}
+
+void tile_pass(const Batch& b, const int* /*tile_qubits_dev*/, int m, const TileOp* ops_dev, int nops,
+               const double2* pool_dev, const TilePass& host_pass) {
+    if (b.c64)
+        tile_pass_t<float2>(b, m, ops_dev, nops, pool_dev, host_pass);
+    else
+        tile_pass_t<double2>(b, m, ops_dev, nops, pool_dev, host_pass);
+}
+
+}  // namespace k
+}  // namespace dq

@@ -22,6 +22,8 @@ from ._core import (
     simulate_monolithic_shots,
 )
 
+from . import workloads  # noqa: E402  (seeded benchmark circuits)
+
 __all__ = [
     "MpsSimulator",
     "MpsResult",

@@ -47,6 +47,9 @@ class _Options(ctypes.Structure):
         ("sample_terminal", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("execution", ctypes.c_int),
+        ("tile_qubits", ctypes.c_int),
+        ("fusion_width", ctypes.c_int),
     ]
 
 
@@ -267,7 +270,8 @@ class StatevectorSimulator:
     """
 
     def __init__(self, seed=None, profile=False, *, max_memory_mb=1024, max_parallel_shots=None,
-                 sample_terminal=True, precision="complex128", device=0):
+                 sample_terminal=True, precision="complex128", device=0, execution="auto", tile_qubits=0,
+                 fusion_width=0):
         o = _Options()
         o.has_seed = 0 if seed is None else 1
         o.seed = 0 if seed is None else _as_u64(seed, "seed")
@@ -281,6 +285,12 @@ class StatevectorSimulator:
             raise ValueError(f"precision must be one of {sorted(set(PRECISIONS))}")
         o.precision = PRECISIONS[key]
         o.device = int(device)
+        modes = {"auto": 0, "per_gate": 1, "tiled": 2}
+        if execution not in modes:
+            raise ValueError("execution must be 'auto', 'per_gate' or 'tiled'")
+        o.execution = modes[execution]
+        o.tile_qubits = int(tile_qubits)
+        o.fusion_width = int(fusion_width)
         h = _P()
         _check(_sim_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
@@ -321,7 +331,8 @@ def _parse_mode(mode):
     raise ValueError(f"Unsupported monolithic simulation mode {key!r}; expected 'state_vector' or 'mps'")
 
 
-_SV_OPTIONS = ("max_memory_mb", "max_parallel_shots", "sample_terminal", "precision", "device")
+_SV_OPTIONS = ("max_memory_mb", "max_parallel_shots", "sample_terminal", "precision", "device", "execution",
+               "tile_qubits", "fusion_width")
 
 
 def _parse_options(options):
@@ -368,6 +379,70 @@ def simulate_distributed_shots(distributed, mode="p_block", shots=1000, seed=Non
     raise NotImplementedError("The P-block backend is not provided by the B200 statevector engine")
 
 
+_plan_create = _sig("dq_plan_create", [_P, ctypes.c_char_p, ctypes.c_size_t, _u64, ctypes.POINTER(_P)])
+_plan_run = _sig("dq_plan_run", [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)])
+_plan_stats = _sig("dq_plan_stats", [_P, _P, _P, _P])
+_plan_info = _sig("dq_plan_info", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_double)])
+_plan_sv = _sig("dq_plan_statevector", [_P, _P, _u64])
+_plan_samples = _sig("dq_plan_samples", [_P, _P, _u64])
+_plan_free = _sig("dq_plan_free", [_P], None)
+_plan_compare = _sig("dq_plan_compare", [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)])
+
+KERNEL_CLASSES = ("gate1q", "controlled", "diagonal", "swap", "dense", "measure", "tile", "fused", "sample")
+
+
+class PreparedCircuit:
+    """A circuit compiled and resident on the device, run many times (dq_plan_*)."""
+
+    def __init__(self, simulator, circuit, shots=0):
+        text = _circuit_json(circuit)
+        h = _P()
+        _check(_plan_create(simulator._h, text, len(text), _as_u64(shots, "shots"), ctypes.byref(h)))
+        self._h = h
+        self._sim = simulator
+        nq, nops, sb = _u64(), _u64(), ctypes.c_double()
+        _check(_plan_info(h, ctypes.byref(nq), ctypes.byref(nops), ctypes.byref(sb)))
+        self.num_qubits, self.num_ops, self.state_bytes = nq.value, nops.value, sb.value
+        self.shots = shots
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _plan_free(h)
+            self._h = None
+
+    def run(self, record=False):
+        """Device milliseconds of one run (CUDA events on the engine stream)."""
+        ms = ctypes.c_double()
+        _check(_plan_run(self._h, 1 if record else 0, ctypes.byref(ms)))
+        return ms.value
+
+    def stats(self):
+        n = len(KERNEL_CLASSES)
+        ms = np.zeros(n)
+        launches = np.zeros(n, dtype=np.uint64)
+        nbytes = np.zeros(n)
+        _check(_plan_stats(self._h, ms.ctypes.data_as(_P), launches.ctypes.data_as(_P), nbytes.ctypes.data_as(_P)))
+        return {k: {"ms": float(ms[i]), "launches": int(launches[i]), "bytes": float(nbytes[i])}
+                for i, k in enumerate(KERNEL_CLASSES) if launches[i]}
+
+    def statevector(self):
+        out = np.empty(1 << self.num_qubits, dtype=np.complex128)
+        _check(_plan_sv(self._h, out.ctypes.data_as(_P), 2 * out.shape[0]))
+        return out
+
+    def samples(self):
+        out = np.empty(self.shots, dtype=np.uint64)
+        _check(_plan_samples(self._h, out.ctypes.data_as(_P), self.shots))
+        return out
+
+    def compare(self, other):
+        """(fidelity |<self|other>|^2, max amplitude error) of the two final states."""
+        f, e = ctypes.c_double(), ctypes.c_double()
+        _check(_plan_compare(self._h, other._h, ctypes.byref(f), ctypes.byref(e)))
+        return f.value, e.value
+
+
 def compile_dump(circuit_json):
     """Host-only: the fused operation list of a transport JSON string (for tests)."""
     import json as _json
@@ -375,6 +450,23 @@ def compile_dump(circuit_json):
     text = circuit_json.encode("utf-8") if isinstance(circuit_json, str) else circuit_json
     out = ctypes.c_char_p()
     _check(_compile_dump(text, len(text), ctypes.byref(out)))
+    try:
+        return _json.loads(out.value.decode("utf-8"))
+    finally:
+        _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+_tile_plan_dump = _sig("dq_tile_plan_dump", [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_char_p)])
+
+
+def tile_plan_dump(circuit_json, tile_qubits=12, fusion_width=2):
+    """Host-only: the shared-memory pass plan of a unitary circuit (for tests and inspection)."""
+    import json as _json
+
+    text = circuit_json.encode("utf-8") if isinstance(circuit_json, str) else circuit_json
+    out = ctypes.c_char_p()
+    _check(_tile_plan_dump(text, len(text), int(tile_qubits), int(fusion_width), ctypes.byref(out)))
     try:
         return _json.loads(out.value.decode("utf-8"))
     finally:

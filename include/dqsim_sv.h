@@ -63,6 +63,9 @@ typedef struct dq_sim_options {
     int sample_terminal;         /* default 1 */
     int precision;               /* dq_precision, default DQ_COMPLEX128 */
     int device;                  /* CUDA device ordinal, default 0 */
+    int execution;               /* 0 auto (shared-memory tile passes), 1 per-gate, 2 tiled */
+    int tile_qubits;             /* qubits per shared-memory tile; 0 = 12 (complex128) / 13 (complex64) */
+    int fusion_width;            /* widest fused dense operation inside a tile; 0 = 2 */
 } dq_sim_options;
 
 /* Per-category counters of SimulationProfile (simulator.rs:43-59). */
@@ -126,11 +129,51 @@ DQ_API int dq_result_counts(const dq_result* r, uint64_t shots, const uint64_t* 
 DQ_API int dq_result_fidelity(const dq_result* r, const double* other, uint64_t other_len, double* out);
 DQ_API void dq_result_free(dq_result* r);
 
+/* Prepared circuits: parse, validate, compile and lower once, keep the state
+ * and sampling buffers resident, then run repeatedly.  The reference reuses a
+ * compiled plan and one prefix evolution for every shot of a call
+ * (src/monolithic/statevector/shots.rs:125-158); a dq_plan extends that reuse
+ * across calls and is what device-timed benchmarks drive.  A run starts from
+ * |0...0>, applies every operation and, for a circuit ending in measurements,
+ * draws `shots` terminal samples with the per-shot ChaCha8 streams of
+ * shots.rs:153-158.  Kernel-class statistics use the dq_kernel_class order. */
+typedef struct dq_plan dq_plan;
+typedef enum dq_kernel_class {
+    DQ_K_GATE1Q = 0,
+    DQ_K_CONTROLLED = 1,
+    DQ_K_DIAGONAL = 2,
+    DQ_K_SWAP = 3,
+    DQ_K_DENSE = 4,
+    DQ_K_MEASURE = 5,
+    DQ_K_TILE = 6,
+    DQ_K_FUSED = 7,
+    DQ_K_SAMPLE = 8,
+    DQ_K_NUM_CLASSES = 9
+} dq_kernel_class;
+DQ_API int dq_plan_create(dq_sim* sim, const char* json, size_t json_len, uint64_t shots, dq_plan** out);
+/* One run; *device_ms is the CUDA-event time on the engine stream.  With
+ * record != 0 every launch is bracketed by events for dq_plan_stats. */
+DQ_API int dq_plan_run(dq_plan* p, int record, double* device_ms);
+/* Per kernel class of the last recorded run: milliseconds, launches and
+ * algorithmic bytes (arrays of DQ_K_NUM_CLASSES entries). */
+DQ_API int dq_plan_stats(const dq_plan* p, double* ms, uint64_t* launches, double* bytes);
+DQ_API int dq_plan_info(const dq_plan* p, uint64_t* num_qubits, uint64_t* num_ops, double* state_bytes);
+DQ_API int dq_plan_statevector(const dq_plan* p, double* out, uint64_t out_len);
+DQ_API int dq_plan_samples(const dq_plan* p, uint64_t* out, uint64_t out_len);
+/* State fidelity |<a|b>|^2 and max amplitude error of two plans' final states
+ * (same qubit count, any precisions), computed on the device. */
+DQ_API int dq_plan_compare(const dq_plan* a, const dq_plan* b, double* fidelity, double* max_abs_err);
+DQ_API void dq_plan_free(dq_plan* p);
+
 /* Host-only helpers (no device work): parse, validate and compile a circuit
  * exactly as read_circuit + compile do (simulator.rs:204-211,
  * execution.rs:368-416), returning the operation list as JSON text with
  * doubles as 16-hex-digit bit patterns.  Free the text with dq_string_free. */
 DQ_API int dq_compile_dump(const char* json, size_t json_len, char** out_text);
+/* Host-only: the shared-memory tile plan of the circuit's unitary operations
+ * (tile qubits, tile-local operations, matrix pool) as JSON text.  No
+ * counterpart in the reference; it exposes the planner for inspection. */
+DQ_API int dq_tile_plan_dump(const char* json, size_t json_len, int tile_qubits, int fusion_width, char** out_text);
 DQ_API void dq_string_free(char* s);
 
 #ifdef __cplusplus

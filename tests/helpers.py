@@ -5,6 +5,8 @@ import math
 
 import numpy as np
 
+from dqsim import workloads
+
 
 class Circuit:
     """Minimal transport object (tests/test_statevector.py:27-38 of the reference)."""
@@ -89,46 +91,15 @@ def random_circuit(seed, n, depth, generic=True, barriers=True):
 
 
 def brickwork(n, depth, seed=0, measure=True):
-    """U3 on every qubit, then CX (2i,2i+1) on even layers and (2i+1,2i+2) on odd layers."""
-    rng = np.random.default_rng(seed)
-    ins = []
-    for layer in range(depth):
-        for q in range(n):
-            th, ph, la = rng.uniform(0.0, 2 * math.pi, size=3)
-            ins.append(inst("u3", qubit=q, theta=float(th), phi=float(ph), lam=float(la)))
-        start = 0 if layer % 2 == 0 else 1
-        for a in range(start, n - 1, 2):
-            ins.append(inst("cx", control=a, target=a + 1))
-    if measure:
-        ins += [inst("measure", qubit=q, cbit=q) for q in range(n)]
-    return Circuit(n, ins, n if measure else 0)
+    return workloads.brickwork(n, depth, seed=seed, measure=measure)
 
 
 def qft(n, seed=0):
-    """Seeded basis state + H on a random half, then QFT with CP(2pi/2^k) and the swap network."""
-    rng = np.random.default_rng(seed)
-    ins = [inst("x", qubit=q) for q in range(n) if rng.random() < 0.5]
-    for q in rng.choice(n, size=n // 2, replace=False).tolist():
-        ins.append(inst("h", qubit=q))
-    for j in range(n - 1, -1, -1):
-        ins.append(inst("h", qubit=j))
-        for k in range(j - 1, -1, -1):
-            ins.append(inst("cp", control=k, target=j, lam=2 * math.pi / 2 ** (j - k + 1)))
-    for q in range(n // 2):
-        ins.append(inst("swap", a=q, b=n - 1 - q))
-    return Circuit(n, ins)
+    return workloads.qft(n, seed=seed)
 
 
 def hea(n, depth, seed):
-    rng = np.random.default_rng(seed)
-    ins = []
-    for _ in range(depth):
-        for q in range(n):
-            ins.append(inst("ry", qubit=q, theta=float(rng.uniform(0, 2 * math.pi))))
-            ins.append(inst("rz", qubit=q, phi=float(rng.uniform(0, 2 * math.pi))))
-        for q in range(n - 1):
-            ins.append(inst("cz", control=q, target=q + 1))
-    return Circuit(n, ins)
+    return workloads.hea(n, depth, seed)
 
 
 def assert_distribution(counts, expected, shots, delta=0.08):
