@@ -133,8 +133,9 @@ def max_over_ranks(pg, local, value):
     return float(t.item())
 
 
-def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed):
-    sim = dqsim.StatevectorSimulator(seed=seed, max_memory_mb=1 << 20, precision=precision, device=local)
+def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed, execution="auto"):
+    sim = dqsim.StatevectorSimulator(seed=seed, max_memory_mb=1 << 20, precision=precision, device=local,
+                                     execution=execution)
     plan = dqsim._core.PreparedCircuit(sim, circuit, shots=shots)
     for _ in range(warmup):
         plan.run()
@@ -226,11 +227,35 @@ def main():
     peak, peak_kind = peaks()
     circuit = dqsim.workloads.brickwork(args.qubits, args.depth, seed=args.seed, measure=True)
 
-    # Plain complex128 form (the reference's arithmetic, one pass per operation).
-    sim128, plan128 = time_form(dqsim, circuit, "complex128", local, 1, 1, args.shots, args.seed)
+    def bytes_of(stats):
+        return sum(v["bytes"] for k, v in stats.items() if k != "sample")
+
+    def summarize(stats, ms_):
+        gbs = bytes_of(stats) / (ms_ * 1e-3) / 1e9
+        return {"s": ms_ * 1e-3, "gbs": gbs, "frac_of_hbm": gbs / peak, "kernels": stats}
+
+    # Plain complex128 form: the reference's arithmetic, one HBM pass per operation.
+    sim128, plan128 = time_form(dqsim, circuit, "complex128", local, 1, 0, args.shots, args.seed,
+                                execution="per_gate")
     t128 = [plan128.run() for _ in range(args.plain_steps)]
     plan128.run(record=True)
     st128 = plan128.stats()
+    ms128 = statistics.mean(t128)
+    per_gate = st128.get("gate1q")
+    plain_kernel = None
+    if per_gate:
+        ach = per_gate["bytes"] / (per_gate["ms"] * 1e-3) / 1e9
+        plain_kernel = {"kernel": "gate1q (c128, per-gate)", "achieved": ach, "frac": ach / peak,
+                        "launches": per_gate["launches"]}
+
+    # complex128 with shared-memory tile passes (same FP64 arithmetic, fused 4x4 within a pass).
+    simt, plant = time_form(dqsim, circuit, "complex128", local, 1, 1, args.shots, args.seed)
+    tt = [plant.run() for _ in range(args.plain_steps)]
+    plant.run(record=True)
+    stt = plant.stats()
+    mst = statistics.mean(tt)
+    tiled_fid, tiled_err = plant.compare(plan128)
+    del plant, simt
 
     # Complex64 form (the chosen form).
     sim64, plan64 = time_form(dqsim, circuit, "complex64", local, 1, args.warmup, args.shots, args.seed)
@@ -244,12 +269,7 @@ def main():
     fidelity, max_err = plan64.compare(plan128)
     del plan128, sim128
 
-    def bytes_of(stats):
-        return sum(v["bytes"] for k, v in stats.items() if k != "sample")
-
     gb64 = bytes_of(st64) / (ms * 1e-3) / 1e9
-    ms128 = statistics.mean(t128)
-    gb128 = bytes_of(st128) / (ms128 * 1e-3) / 1e9
     dom = max(st64.items(), key=lambda kv: kv[1]["ms"])
     dom_achieved = dom[1]["bytes"] / (dom[1]["ms"] * 1e-3) / 1e9
 
@@ -280,10 +300,10 @@ def main():
         "vs_baseline": None, "dtype": "c64 (f32, FP64 reductions)", "data": "synthetic",
         "config": workload_config(args),
         "forms": {
-            "complex64": {"s": ms * 1e-3, "gbs": gb64, "frac_of_hbm": gb64 / peak, "fidelity": fidelity,
-                          "max_amp_err": max_err, "kernels": st64},
-            "complex128": {"s": ms128 * 1e-3, "gbs": gb128, "frac_of_hbm": gb128 / peak, "kernels": st128},
-            "speedup_c64_vs_c128": ms128 / ms,
+            "complex64": {**summarize(st64, ms), "fidelity": fidelity, "max_amp_err": max_err},
+            "complex128_per_gate": {**summarize(st128, ms128), "dominant": plain_kernel},
+            "complex128_tiled": {**summarize(stt, mst), "fidelity": tiled_fid, "max_amp_err": tiled_err},
+            "speedup_c64_vs_plain": ms128 / ms,
         },
         "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                      "frac": dom_achieved / peak, "peak_kind": peak_kind, "traffic": None},

@@ -6,6 +6,7 @@
 #include <random>
 
 #include "../../include/dqsim_sv.h"
+#include "batch.hpp"
 #include "plan.hpp"
 #include "simulator.hpp"
 
@@ -13,6 +14,9 @@ using namespace dq;
 
 struct dq_plan {
     std::unique_ptr<Plan> impl;
+};
+struct dq_batch {
+    std::unique_ptr<BatchRun> impl;
 };
 
 struct dq_sim {
@@ -335,6 +339,94 @@ int dq_plan_compare(const dq_plan* a, const dq_plan* b, double* fidelity, double
 }
 
 void dq_plan_free(dq_plan* p) { delete p; }
+
+int dq_batch_create(dq_sim* sim, const char* const* jsons, const size_t* lens, uint64_t count, uint64_t shots,
+                    int autotune, dq_batch** out) {
+    return guard([&] {
+        need(sim, "sim");
+        need(out, "out");
+        if (count == 0) fail(kValueError, "a batch needs at least one circuit");
+        need(jsons, "jsons");
+        need(lens, "json_lens");
+        std::vector<std::string> texts;
+        for (uint64_t i = 0; i < count; i++) {
+            need(jsons[i], "json");
+            texts.emplace_back(jsons[i], lens[i]);
+        }
+        BatchTuning t;
+        if (autotune) {
+            const bool c64 = sim->impl->options().precision == Precision::C64;
+            std::map<uint64_t, size_t> first;
+            for (size_t i = 0; i < texts.size(); i++) {
+                uint64_t n = 0;
+                compile_json(texts[i].data(), texts[i].size(), &n, nullptr);
+                first.emplace(n, i);
+            }
+            for (auto& kv : first) {
+                TuneResult r = autotune_tile(*sim->impl, texts[kv.second], c64);
+                t.per_n[kv.first] = {r.tile_m, r.fuse};
+            }
+        }
+        auto b = std::make_unique<dq_batch>();
+        b->impl = std::make_unique<BatchRun>(*sim->impl, texts, shots, t);
+        *out = b.release();
+    });
+}
+
+int dq_batch_run(dq_batch* b, int use_graph, double* device_ms) {
+    return guard([&] {
+        need(b, "batch");
+        double ms = b->impl->run(use_graph != 0);
+        if (device_ms) *device_ms = ms;
+    });
+}
+
+int dq_batch_counts(const dq_batch* b, uint64_t index, dq_counts** out) {
+    return guard([&] {
+        need(b, "batch");
+        need(out, "out");
+        if (index >= b->impl->size()) fail(kValueError, "batch index out of range");
+        auto m = b->impl->counts(size_t(index));
+        auto c = std::make_unique<dq_counts>();
+        for (auto& kv : m) {
+            c->width = kv.first.size();
+            c->keys.push_back(kv.first);
+            c->counts.push_back(kv.second);
+        }
+        *out = c.release();
+    });
+}
+
+int dq_batch_expect_zz(const dq_batch* b, double* out, uint64_t count) {
+    return guard([&] {
+        need(b, "batch");
+        need(out, "out");
+        if (count != b->impl->size()) fail(kValueError, "expectation buffer has the wrong length");
+        auto v = b->impl->expect_zz();
+        std::copy(v.begin(), v.end(), out);
+    });
+}
+
+int dq_batch_statevector(const dq_batch* b, uint64_t index, double* out, uint64_t out_len) {
+    return guard([&] {
+        need(b, "batch");
+        need(out, "out");
+        if (index >= b->impl->size()) fail(kValueError, "batch index out of range");
+        if (out_len != (uint64_t(2) << b->impl->num_qubits(size_t(index))))
+            fail(kValueError, "statevector buffer has the wrong length");
+        b->impl->statevector(size_t(index), out);
+    });
+}
+
+int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items) {
+    return guard([&] {
+        need(b, "batch");
+        if (passes) *passes = b->impl->passes();
+        if (items) *items = b->impl->items();
+    });
+}
+
+void dq_batch_free(dq_batch* b) { delete b; }
 
 int dq_compile_dump(const char* json, size_t len, char** out_text) {
     return guard([&] {

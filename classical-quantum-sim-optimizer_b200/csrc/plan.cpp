@@ -18,9 +18,11 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
     for (size_t i = prefix_end_; i < ops_.size(); i++)
         if (ops_[i].type != Operation::Measure) terminal_ = false;
     dev_ = sim.ensure_device();
-    std::lock_guard<std::mutex> lk(dev_->mu);
-    dev_->activate();
-    st_.allocate(int(n_), 1, ncb_, opt_.precision == Precision::C64);
+    {
+        std::lock_guard<std::mutex> lk(dev_->mu);
+        dev_->activate();
+        st_.allocate(int(n_), 1, ncb_, opt_.precision == Precision::C64);
+    }
     if (terminal_ && prefix_end_ < ops_.size() && shots_ > 0) {
         for (size_t i = prefix_end_; i < ops_.size(); i++) sample_qubits_.push_back(ops_[i].qubit);
         std::sort(sample_qubits_.begin(), sample_qubits_.end());

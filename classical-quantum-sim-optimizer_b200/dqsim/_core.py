@@ -443,6 +443,68 @@ class PreparedCircuit:
         return f.value, e.value
 
 
+_batch_create = _sig("dq_batch_create", [_P, _P, _P, _u64, _u64, ctypes.c_int, ctypes.POINTER(_P)])
+_batch_run = _sig("dq_batch_run", [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)])
+_batch_counts = _sig("dq_batch_counts", [_P, _u64, ctypes.POINTER(_P)])
+_batch_zz = _sig("dq_batch_expect_zz", [_P, _P, _u64])
+_batch_sv = _sig("dq_batch_statevector", [_P, _u64, _P, _u64])
+_batch_info = _sig("dq_batch_info", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_batch_free = _sig("dq_batch_free", [_P], None)
+
+
+class BatchedCircuits:
+    """Many terminal-measurement circuits of uneven sizes in one persistent launch (dq_batch_*).
+
+    Seeds: circuit i samples with seed + i * 0x9E3779B97F4A7C15 (mod 2^64), shot t
+    of it with ChaCha8 seed_from_u64(that + t), as a single simulate_shots call would.
+    """
+
+    def __init__(self, simulator, circuits, shots=1024, autotune=False):
+        texts = [_circuit_json(c) for c in circuits]
+        self._keep = [ctypes.create_string_buffer(t, len(t)) for t in texts]
+        ptrs = (ctypes.c_void_p * len(texts))(*[ctypes.cast(b, ctypes.c_void_p) for b in self._keep])
+        lens = (ctypes.c_size_t * len(texts))(*[len(t) for t in texts])
+        h = _P()
+        _check(_batch_create(simulator._h, ctypes.cast(ptrs, _P), ctypes.cast(lens, _P), len(texts),
+                             _as_u64(shots, "shots"), 1 if autotune else 0, ctypes.byref(h)))
+        self._h = h
+        self._sim = simulator
+        self.size = len(texts)
+        self.num_qubits = [c.num_qubits if hasattr(c, "num_qubits") else None for c in circuits]
+        p, i = _u64(), _u64()
+        _check(_batch_info(h, ctypes.byref(p), ctypes.byref(i)))
+        self.passes, self.items = p.value, i.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _batch_free(h)
+            self._h = None
+
+    def run(self, use_graph=True):
+        ms = ctypes.c_double()
+        _check(_batch_run(self._h, 1 if use_graph else 0, ctypes.byref(ms)))
+        return ms.value
+
+    def counts(self, i):
+        h = _P()
+        _check(_batch_counts(self._h, i, ctypes.byref(h)))
+        return _take_counts(h)
+
+    def expect_zz(self):
+        out = np.empty(self.size)
+        _check(_batch_zz(self._h, out.ctypes.data_as(_P), self.size))
+        return out
+
+    def statevector(self, i, n):
+        out = np.empty(1 << n, dtype=np.complex128)
+        _check(_batch_sv(self._h, i, out.ctypes.data_as(_P), 2 * out.shape[0]))
+        return out
+
+
+BATCH_SEED_STRIDE = 0x9E3779B97F4A7C15
+
+
 def compile_dump(circuit_json):
     """Host-only: the fused operation list of a transport JSON string (for tests)."""
     import json as _json

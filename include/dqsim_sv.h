@@ -165,6 +165,24 @@ DQ_API int dq_plan_samples(const dq_plan* p, uint64_t* out, uint64_t out_len);
 DQ_API int dq_plan_compare(const dq_plan* a, const dq_plan* b, double* fidelity, double* max_abs_err);
 DQ_API void dq_plan_free(dq_plan* p);
 
+/* Batched circuits: many circuits of uneven qubit counts, each a unitary
+ * prefix followed only by measurements, run in one persistent kernel over
+ * (circuit, pass, tile) work items, then sampled with `shots` terminal
+ * samples each (per-shot ChaCha8 streams as shots.rs:153-158) and reduced to
+ * <Z0 Z1>.  No counterpart in the reference, which runs one circuit per call;
+ * each circuit's counts follow the reference's terminal-sampling semantics
+ * (shots.rs:93-176).  autotune != 0 times candidate tile shapes and fusion
+ * widths per qubit count first.  A run can replay a captured CUDA graph. */
+typedef struct dq_batch dq_batch;
+DQ_API int dq_batch_create(dq_sim* sim, const char* const* jsons, const size_t* json_lens, uint64_t count,
+                           uint64_t shots, int autotune, dq_batch** out);
+DQ_API int dq_batch_run(dq_batch* b, int use_graph, double* device_ms);
+DQ_API int dq_batch_counts(const dq_batch* b, uint64_t index, dq_counts** out);
+DQ_API int dq_batch_expect_zz(const dq_batch* b, double* out, uint64_t count);
+DQ_API int dq_batch_statevector(const dq_batch* b, uint64_t index, double* out, uint64_t out_len);
+DQ_API int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items);
+DQ_API void dq_batch_free(dq_batch* b);
+
 /* Host-only helpers (no device work): parse, validate and compile a circuit
  * exactly as read_circuit + compile do (simulator.rs:204-211,
  * execution.rs:368-416), returning the operation list as JSON text with
