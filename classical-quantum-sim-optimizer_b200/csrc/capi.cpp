@@ -7,6 +7,7 @@
 
 #include "../../include/dqsim_sv.h"
 #include "batch.hpp"
+#include "cost.hpp"
 #include "plan.hpp"
 #include "simulator.hpp"
 
@@ -17,6 +18,9 @@ struct dq_plan {
 };
 struct dq_batch {
     std::unique_ptr<BatchRun> impl;
+};
+struct dq_cost_model {
+    std::unique_ptr<CostModel> impl;
 };
 
 struct dq_sim {
@@ -427,6 +431,147 @@ int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items) {
 }
 
 void dq_batch_free(dq_batch* b) { delete b; }
+
+int dq_cost_model_create(int device, uint64_t seed, dq_cost_model** out) {
+    return guard([&] {
+        need(out, "out");
+        auto m = std::make_unique<dq_cost_model>();
+        m->impl = std::make_unique<CostModel>(device, seed);
+        *out = m.release();
+    });
+}
+
+void dq_cost_model_free(dq_cost_model* m) { delete m; }
+
+int dq_cost_model_add_samples(dq_cost_model* m, const float* features, const float* log_cycles, uint64_t n) {
+    return guard([&] {
+        need(m, "model");
+        if (n) {
+            need(features, "features");
+            need(log_cycles, "log_cycles");
+        }
+        m->impl->add_samples(features, log_cycles, size_t(n));
+    });
+}
+
+int dq_cost_model_record(dq_cost_model* m, dq_sim* sim, const char* json, size_t len, uint64_t* added) {
+    return guard([&] {
+        need(m, "model");
+        need(sim, "sim");
+        need(json, "json");
+        Plan p(*sim->impl, json, len, 0);
+        std::vector<float> X, y;
+        p.record_costs(X, y);
+        m->impl->add_samples(X.data(), y.data(), y.size());
+        if (added) *added = y.size();
+    });
+}
+
+int dq_cost_model_num_samples(const dq_cost_model* m, uint64_t* n) {
+    return guard([&] {
+        need(m, "model");
+        need(n, "n");
+        *n = m->impl->num_samples();
+    });
+}
+
+int dq_cost_model_samples(const dq_cost_model* m, float* features, float* log_cycles, uint64_t n) {
+    return guard([&] {
+        need(m, "model");
+        if (n != m->impl->num_samples()) fail(kValueError, "sample buffers have the wrong length");
+        m->impl->copy_samples(features, log_cycles);
+    });
+}
+
+int dq_cost_model_train(dq_cost_model* m, int epochs, float lr, double* final_mse) {
+    return guard([&] {
+        need(m, "model");
+        if (epochs < 1 || !(lr > 0.f)) fail(kValueError, "epochs must be positive and lr > 0");
+        double l = m->impl->train(epochs, lr);
+        if (final_mse) *final_mse = l;
+    });
+}
+
+int dq_cost_model_predict(const dq_cost_model* m, const float* features, uint64_t n, float* log_cycles) {
+    return guard([&] {
+        need(m, "model");
+        if (n) {
+            need(features, "features");
+            need(log_cycles, "log_cycles");
+        }
+        m->impl->predict(features, size_t(n), log_cycles);
+    });
+}
+
+int dq_cost_model_gradients(const dq_cost_model* m, const float* features, const float* log_cycles, uint64_t n,
+                            float* grads) {
+    return guard([&] {
+        need(m, "model");
+        need(features, "features");
+        need(log_cycles, "log_cycles");
+        need(grads, "grads");
+        m->impl->gradients(features, log_cycles, size_t(n), grads);
+    });
+}
+
+int dq_cost_model_get_params(const dq_cost_model* m, float* out, uint64_t len) {
+    return guard([&] {
+        need(m, "model");
+        need(out, "out");
+        if (len != uint64_t(kMlpParams + 2)) fail(kValueError, "parameter buffer must hold DQ_MLP_PARAMS floats");
+        m->impl->get_params(out);
+    });
+}
+
+int dq_cost_model_set_params(dq_cost_model* m, const float* in, uint64_t len) {
+    return guard([&] {
+        need(m, "model");
+        need(in, "in");
+        if (len != uint64_t(kMlpParams + 2)) fail(kValueError, "parameter buffer must hold DQ_MLP_PARAMS floats");
+        m->impl->set_params(in);
+    });
+}
+
+int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m) {
+    return guard([&] {
+        need(sim, "sim");
+        if (m && !m->impl->trained()) fail(kValueError, "attach a trained cost model");
+        sim->impl->set_cost_model(m ? m->impl.get() : nullptr);
+    });
+}
+
+int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int* used_learned, int* rejected) {
+    return guard([&] {
+        need(p, "plan");
+        double a, b;
+        int u, r;
+        p->impl->planner(&a, &b, &u, &r);
+        if (learned_ms) *learned_ms = a;
+        if (greedy_ms) *greedy_ms = b;
+        if (used_learned) *used_learned = u;
+        if (rejected) *rejected = r;
+    });
+}
+
+int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops) {
+    return guard([&] {
+        need(p, "plan");
+        if (passes) *passes = p->impl->passes();
+        if (tile_ops) *tile_ops = p->impl->tile_ops();
+    });
+}
+
+int dq_sim_planner_log(dq_sim* sim, char** out_text) {
+    return guard([&] {
+        need(sim, "sim");
+        need(out_text, "out_text");
+        std::string s = sim->impl->planner_log();
+        char* buf = static_cast<char*>(std::malloc(s.size() + 1));
+        if (!buf) throw std::bad_alloc();
+        std::memcpy(buf, s.c_str(), s.size() + 1);
+        *out_text = buf;
+    });
+}
 
 int dq_compile_dump(const char* json, size_t len, char** out_text) {
     return guard([&] {

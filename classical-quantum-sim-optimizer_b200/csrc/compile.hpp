@@ -35,6 +35,7 @@ struct Operation {
     uint64_t qubit = 0, cbit = 0;  // Measure, Reset
     Condition condition;           // Conditional
     std::shared_ptr<Operation> inner;
+    int fused_count = 1;           // operations multiplied into this one by a fusion pass
 
     bool is_unitary() const { return type != Measure && type != Reset && type != Conditional; }
     // Qubits the operation reads or writes (conditions excluded).

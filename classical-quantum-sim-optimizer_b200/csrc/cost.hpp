@@ -1,0 +1,65 @@
+// Learned cost model for the fusion planner.
+//
+// A 16 -> 64 -> 64 -> 1 MLP (ReLU, FP32) predicts the log of the device
+// cycles one tile-local operation costs per tile, from its kind, width, the
+// tile-local positions of its qubits (stride and bank-conflict class), how
+// many gates were fused into it, its work per tile and the tile size.  It is
+// trained on timings the engine records itself (an instrumented tile pass
+// reads clock64() around every operation), by CUDA kernels written here:
+// one CTA runs mini-batch forward, backward and Adam steps; inference is one
+// thread per candidate.  The planner asks it which fusion width makes each
+// pass cheapest; the greedy fixed-width plan stays the fallback and the judge.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tile.hpp"
+
+namespace dq {
+
+constexpr int kMlpF = 16;   // features
+constexpr int kMlpH = 64;   // hidden width
+constexpr int kMlpB = 128;  // training mini-batch
+constexpr int kMlpParams = kMlpH * kMlpF + kMlpH + kMlpH * kMlpH + kMlpH + kMlpH + 1;
+
+// Features of one tile-local operation in a pass of m tile qubits.
+void tile_op_features(const TileOp& op, int m, bool c64, float* out);
+
+class CostModel {
+  public:
+    CostModel(int device, uint64_t seed);
+    ~CostModel();
+    void add_samples(const float* X, const float* y, size_t n);
+    size_t num_samples() const { return y_.size(); }
+    void copy_samples(float* X, float* y) const {
+        std::lock_guard<std::mutex> lk(mu_);
+        std::copy(X_.begin(), X_.end(), X);
+        std::copy(y_.begin(), y_.end(), y);
+    }
+    // Adam on log-cycles; returns the final epoch's mean squared error.
+    double train(int epochs, float lr);
+    void predict(const float* X, size_t n, float* out) const;
+    // Gradients of the mean squared error for one batch (n <= kMlpB), no update.
+    void gradients(const float* X, const float* y, size_t n, float* grads) const;
+    void get_params(float* out) const;
+    void set_params(const float* in);
+    bool trained() const { return trained_; }
+    // Sum of predicted cycles of a list of operations (one device call).
+    double predict_ops(const std::vector<TileOp>& ops, int m, bool c64) const;
+    int device() const { return device_; }
+
+  private:
+    int device_;
+    bool trained_ = false;
+    std::vector<float> X_, y_;
+    void* params_ = nullptr;  // device: params, adam m, adam v
+    cudaStream_t stream_ = nullptr;
+    mutable std::mutex mu_;
+};
+
+}  // namespace dq

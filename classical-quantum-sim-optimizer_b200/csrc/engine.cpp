@@ -1,7 +1,10 @@
 #include "engine.hpp"
 
 #include <chrono>
+#include <cmath>
 #include <cstring>
+
+#include "cost.hpp"
 
 namespace dq {
 
@@ -188,6 +191,8 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     o.fuse = cfg_.fuse;
     o.seeds = cfg_.seeds;
     o.c64 = cfg_.c64;
+    o.model = cfg_.model;
+    o.chosen_widths = &widths_;
     std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
     for (auto& p : ps) {
         p.op_begin = int(tile_ops_host_.size());
@@ -198,6 +203,37 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
         s.category = 1;
         passes_.push_back(std::move(p));
         steps_.push_back(std::move(s));
+    }
+}
+
+void Executor::record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y) {
+    run(b, nullptr, nullptr);  // uploads the pools; the state it leaves is overwritten below
+    DevMem cyc;
+    size_t most = 1;
+    for (auto& p : passes_) most = std::max(most, p.ops.size());
+    cyc.alloc(most * 8, "cycle counters");
+    std::vector<unsigned long long> host(most);
+    k::init_basis(b);
+    for (size_t si = 0; si < steps_.size(); si++) {
+        const Step& s = steps_[si];
+        if (s.pass < 0) {
+            // Non-pass steps keep the state evolving as in a normal run.
+            continue;
+        }
+        const TilePass& p = passes_[size_t(s.pass)];
+        const int m = int(p.qubits.size());
+        cuda_check(cudaMemsetAsync(cyc.p, 0, p.ops.size() * 8, b.stream), "clear cycle counters");
+        k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()), pool_.as<double2>(), p,
+                     cyc.as<unsigned long long>());
+        cuda_check(cudaMemcpyAsync(host.data(), cyc.p, p.ops.size() * 8, cudaMemcpyDeviceToHost, b.stream), "read");
+        cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+        const double tiles = double(b.W << (b.n - m));
+        for (size_t i = 0; i < p.ops.size(); i++) {
+            float f[kMlpF];
+            tile_op_features(p.ops[i], m, b.c64, f);
+            X.insert(X.end(), f, f + kMlpF);
+            y.push_back(float(std::log(std::max(1.0, double(host[i]) / tiles))));
+        }
     }
 }
 

@@ -108,6 +108,7 @@ struct ExecConfig {
     int seeds = 6;       // planner candidates per pass
     int n = 0;           // qubits of the state the plan runs on
     bool c64 = false;
+    const CostModel* model = nullptr;  // learned fusion-width choice per pass
 };
 
 // A compiled operation list lowered to launch descriptors, with every matrix
@@ -125,6 +126,11 @@ class Executor {
 
     size_t passes() const { return passes_.size(); }
     size_t raw_ops_in_passes() const;
+    const std::vector<int>& chosen_widths() const { return widths_; }
+    size_t tile_ops() const { return tile_ops_host_.size(); }
+    // Runs every step once, timing each tile-local operation of every pass
+    // (clock64 cycles per tile), and appends (features, log cycles) samples.
+    void record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y);
 
   private:
     struct Step {
@@ -148,6 +154,7 @@ class Executor {
     DevMem pool_, tile_ops_;
     bool uploaded_ = false;
     ExecConfig cfg_;
+    std::vector<int> widths_;
     void lower(const Operation& op, std::vector<Condition>& conds);
     void lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end);
 };

@@ -1,6 +1,8 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <cstdio>
+#include <string>
 
 namespace dq {
 
@@ -33,12 +35,34 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
         tmp_.alloc(k::scan_tmp_size(clen) * 8, "scan scratch");
         idx_.alloc(shots_ * 8, "sampled outcomes");
         scalar_.alloc(16, "sampling total");
-        ex_ = std::make_unique<Executor>(ops_, 0, prefix_end_, exec_config(opt_, n_));
-    } else {
-        ex_ = std::make_unique<Executor>(ops_, 0, ops_.size(), exec_config(opt_, n_));
     }
+    const size_t end = (terminal_ && cdf_.p) ? prefix_end_ : ops_.size();
+    ex_ = std::make_unique<Executor>(ops_, 0, end, exec_config(opt_, n_));
     // Upload the matrix pool and warm the kernels once outside any timing.
     run(false);
+    const CostModel* model = sim.cost_model();
+    ExecConfig lc = exec_config(opt_, n_, false, model);
+    if (model && lc.tiled) {
+        // Learned plan vs the greedy fixed-width plan: the faster one is kept,
+        // and a learned plan slower than greedy is rejected and logged.
+        auto learned = std::make_unique<Executor>(ops_, 0, end, lc);
+        greedy_ms_ = std::min(run(false), run(false));
+        std::swap(ex_, learned);
+        run(false);
+        learned_ms_ = std::min(run(false), run(false));
+        std::vector<int> widths = ex_->chosen_widths();
+        rejected_ = learned_ms_ > greedy_ms_;
+        if (rejected_) std::swap(ex_, learned);
+        used_learned_ = !rejected_;
+        std::string w;
+        for (size_t i = 0; i < widths.size(); i++) w += (i ? "," : "") + std::to_string(widths[i]);
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "{\"qubits\": %llu, \"ops\": %llu, \"greedy_ms\": %.4f, \"learned_ms\": %.4f, \"rejected\": %s, ",
+                      (unsigned long long)n_, (unsigned long long)ops_.size(), greedy_ms_, learned_ms_,
+                      rejected_ ? "true" : "false");
+        sim.log_planner(std::string(buf) + "\"widths\": [" + w + "]}");
+    }
 }
 
 double Plan::state_bytes() const { return double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0); }
@@ -132,6 +156,13 @@ void Plan::compare(const Plan& other, double* fidelity, double* max_abs_err) con
     }
     *fidelity = re * re + im * im;
     *max_abs_err = mx;
+}
+
+void Plan::record_costs(std::vector<float>& X, std::vector<float>& y) {
+    std::lock_guard<std::mutex> lk(dev_->mu);
+    dev_->activate();
+    k::Batch bt = st_.view(dev_->stream, 1);
+    ex_->record_costs(bt, X, y);
 }
 
 void Plan::samples(uint64_t* out) const {

@@ -30,6 +30,17 @@ class Plan {
     double state_bytes() const;
     // |<this|other>|^2 and max |a_i - b_i| of the two final states, on the device.
     void compare(const Plan& other, double* fidelity, double* max_abs_err) const;
+    // Learned-vs-greedy planner outcome (zeros when no cost model was attached).
+    void planner(double* learned_ms, double* greedy_ms, int* used_learned, int* rejected) const {
+        *learned_ms = learned_ms_;
+        *greedy_ms = greedy_ms_;
+        *used_learned = used_learned_ ? 1 : 0;
+        *rejected = rejected_ ? 1 : 0;
+    }
+    size_t passes() const { return ex_ ? ex_->passes() : 0; }
+    size_t tile_ops() const { return ex_ ? ex_->tile_ops() : 0; }
+    // Appends per-operation cost samples of one recorded run.
+    void record_costs(std::vector<float>& X, std::vector<float>& y);
 
   private:
     std::shared_ptr<Device> dev_;
@@ -44,6 +55,8 @@ class Plan {
     DevMem cdf_, tmp_, idx_, scalar_;
     double ms_[kcNumClasses] = {}, bytes_[kcNumClasses] = {};
     uint64_t launches_[kcNumClasses] = {};
+    double learned_ms_ = 0, greedy_ms_ = 0;
+    bool used_learned_ = false, rejected_ = false;
 };
 
 }  // namespace dq

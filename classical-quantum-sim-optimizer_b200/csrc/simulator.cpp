@@ -93,8 +93,9 @@ std::string json_double(double v) {
 
 }  // namespace
 
-ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate) {
+ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate, const CostModel* model) {
     ExecConfig c;
+    c.model = model;
     c.c64 = o.precision == Precision::C64;
     c.tiled = !force_per_gate && o.execution != 1;
     c.tile_m = o.tile_qubits > 0 ? o.tile_qubits : (c.c64 ? 13 : 12);

@@ -36,7 +36,7 @@ struct Options {
 };
 
 // Executor configuration for a state of n qubits under these options.
-ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate = false);
+ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate = false, const CostModel* model = nullptr);
 
 struct ShotOutput {
     std::unordered_map<std::string, uint64_t> counts;
@@ -82,12 +82,29 @@ class Simulator {
         if (!dev_) dev_ = std::make_shared<Device>(opt_.device);
         return dev_;
     }
+    // Learned fusion planner (not owned; detach before the model is freed).
+    void set_cost_model(const CostModel* m) { model_ = m; }
+    const CostModel* cost_model() const { return model_; }
+    // Planner decisions: one JSON object per prepared circuit that compared
+    // a learned plan with the greedy one (rejections included).
+    void log_planner(const std::string& line) {
+        std::lock_guard<std::mutex> lk(mu_);
+        planner_log_.push_back(line);
+    }
+    std::string planner_log() {
+        std::lock_guard<std::mutex> lk(mu_);
+        std::string s;
+        for (auto& l : planner_log_) s += l + "\n";
+        return s;
+    }
 
   private:
     Options opt_;
     uint64_t budget_ = 0;
     std::mutex mu_;
     std::shared_ptr<Device> dev_;
+    const CostModel* model_ = nullptr;
+    std::vector<std::string> planner_log_;
     uint64_t next_seed();
     ShotOutput run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots, uint64_t seed,
                          bool profile);

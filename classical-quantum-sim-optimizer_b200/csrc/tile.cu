@@ -5,6 +5,7 @@
 #include <set>
 
 #include "common.hpp"
+#include "cost.hpp"
 #include "tile.hpp"
 
 namespace dq {
@@ -168,6 +169,8 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
         d.type = Operation::Dense;
         d.qubits = bq;
         d.values = acc;
+        d.fused_count = 0;
+        for (size_t mi : members) d.fused_count += ops[mi].fused_count;
         // Keep diagonal structure (cheaper kernels) when the product is diagonal.
         bool diag = true;
         for (int r = 0; r < dim && diag; r++)
@@ -278,6 +281,7 @@ TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::ve
                      std::vector<TileOp>& out) {
     TileOp t;
     std::memset(&t, 0, sizeof t);
+    t.ngates = op.fused_count;
     auto L = [&](uint64_t q) { return local[q]; };
     auto set_ins = [&](std::vector<int> pos) {
         std::sort(pos.begin(), pos.end());
@@ -333,6 +337,7 @@ TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::ve
                     TileOp e;
                     std::memset(&e, 0, sizeof e);
                     e.type = TileOp::kDiagEntry;
+                    e.ngates = op.fused_count;
                     std::vector<int> pos(lq);
                     std::sort(pos.begin(), pos.end());
                     e.nins = int(pos.size());
@@ -431,7 +436,23 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
         std::vector<Operation> pass_ops;
         for (size_t o : taken) pass_ops.push_back(ops[begin + o]);
         p.raw_ops = int(pass_ops.size());
-        std::vector<Operation> fused = fuse_ops(pass_ops, opt.fuse);
+        int width = opt.fuse;
+        if (opt.model) {
+            // The cost model judges each candidate width by its lowered operations.
+            double best = 1e300;
+            for (int w = 1; w <= kTileMaxDense; w++) {
+                std::vector<double2> scratch;
+                std::vector<TileOp> cand;
+                for (auto& op : fuse_ops(pass_ops, w)) lower_tile_op(op, local, scratch, cand);
+                double cost = opt.model->predict_ops(cand, int(p.qubits.size()), opt.c64);
+                if (cost < best) {
+                    best = cost;
+                    width = w;
+                }
+            }
+        }
+        if (opt.chosen_widths) opt.chosen_widths->push_back(width);
+        std::vector<Operation> fused = fuse_ops(pass_ops, width);
         for (auto& op : fused) lower_tile_op(op, local, *pool, p.ops);
         passes.push_back(std::move(p));
     }
@@ -547,10 +568,11 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
     }
 }
 
-template <typename V>
+template <typename V, bool TIMED>
 __global__ void __launch_bounds__(kTileThreads) k_tile(V* __restrict__ s, int n, int m, TileQubits tq,
                                                        const TileOp* __restrict__ ops, int nops,
-                                                       const double2* __restrict__ pool, uint64_t total_tiles) {
+                                                       const double2* __restrict__ pool, uint64_t total_tiles,
+                                                       unsigned long long* __restrict__ cycles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
     const int lb = m < 6 ? m : 6;
@@ -597,9 +619,15 @@ __global__ void __launch_bounds__(kTileThreads) k_tile(V* __restrict__ s, int n,
             }
         }
         __syncthreads();
+        long long t0 = TIMED ? clock64() : 0;
         for (int i = 0; i < nops; i++) {
             tile_apply<V>(tile, ops[i], m, pool);
             __syncthreads();
+            if (TIMED && threadIdx.x == 0) {
+                long long t1 = clock64();
+                atomicAdd(cycles + i, (unsigned long long)(t1 - t0));
+                t0 = t1;
+            }
         }
         for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) g[lo_tab[e & lmask] | hi_tab[e >> lb]] = tile[e];
         __syncthreads();
@@ -617,25 +645,26 @@ int sm_count() {
     return c;
 }
 
-template <typename V>
-void tile_pass_t(const Batch& b, int m, const TileOp* ops, int nops, const double2* pool, const TilePass& hp) {
+template <typename V, bool TIMED>
+void tile_pass_t(const Batch& b, int m, const TileOp* ops, int nops, const double2* pool, const TilePass& hp,
+                 unsigned long long* cycles) {
     TileQubits tq{};
     tq.m = m;
     for (int i = 0; i < m; i++) tq.q[i] = hp.qubits[i];
     const size_t smem = tile_smem_bytes(m, sizeof(V) == 8);
-    static size_t configured[2] = {0, 0};
-    size_t& conf = configured[sizeof(V) == 8 ? 1 : 0];
+    static size_t configured[2][2] = {{0, 0}, {0, 0}};
+    size_t& conf = configured[sizeof(V) == 8 ? 1 : 0][TIMED ? 1 : 0];
     if (smem > conf) {
-        cudaFuncSetAttribute(k_tile<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k_tile<V, TIMED>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         conf = smem;
     }
     const uint64_t total = b.W << (b.n - m);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<V>, kTileThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<V, TIMED>, kTileThreads, smem);
     if (per_sm < 1) per_sm = 1;
     uint64_t grid = std::min<uint64_t>(total, uint64_t(sm_count()) * per_sm);
-    k_tile<V><<<unsigned(grid), kTileThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq, ops, nops, pool,
-                                                                 total);
+    k_tile<V, TIMED><<<unsigned(grid), kTileThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq, ops, nops,
+                                                                        pool, total, cycles);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(kCudaError, std::string("tile pass: ") + cudaGetErrorString(e));
 }
@@ -648,11 +677,18 @@ size_t tile_smem_bytes(int m, bool c64) {
 }
 
 void tile_pass(const Batch& b, const int* /*tile_qubits_dev*/, int m, const TileOp* ops_dev, int nops,
-               const double2* pool_dev, const TilePass& host_pass) {
-    if (b.c64)
-        tile_pass_t<float2>(b, m, ops_dev, nops, pool_dev, host_pass);
-    else
-        tile_pass_t<double2>(b, m, ops_dev, nops, pool_dev, host_pass);
+               const double2* pool_dev, const TilePass& host_pass, unsigned long long* cycles) {
+    if (b.c64) {
+        if (cycles)
+            tile_pass_t<float2, true>(b, m, ops_dev, nops, pool_dev, host_pass, cycles);
+        else
+            tile_pass_t<float2, false>(b, m, ops_dev, nops, pool_dev, host_pass, nullptr);
+    } else {
+        if (cycles)
+            tile_pass_t<double2, true>(b, m, ops_dev, nops, pool_dev, host_pass, cycles);
+        else
+            tile_pass_t<double2, false>(b, m, ops_dev, nops, pool_dev, host_pass, nullptr);
+    }
 }
 
 }  // namespace k

@@ -31,8 +31,11 @@ struct TileOp {
     uint32_t tbit;        // kOne / kX: target bit
     uint32_t lowbit, highbit;  // kSwap
     int mat;              // offset into the pass's double2 matrix pool
+    int ngates;           // operations fused into this one
     uint32_t offs[32];    // kDense: offset of matrix index j
 };
+
+class CostModel;
 
 struct TilePass {
     std::vector<int> qubits;  // ascending global positions of the m tile qubits
@@ -46,6 +49,10 @@ struct TilePlanOptions {
     int fuse = 2;        // widest fused dense operation
     int seeds = 6;       // candidate starts per pass
     bool c64 = false;
+    // With a trained cost model, each pass takes the fusion width (1..3)
+    // whose lowered operations have the smallest predicted cost.
+    const CostModel* model = nullptr;
+    std::vector<int>* chosen_widths = nullptr;  // filled per pass when given
 };
 
 // Widest dense operation a tile pass applies on CUDA cores (register budget).
@@ -66,9 +73,11 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
 std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width);
 
 namespace k {
-// One pass over every tile of every state in the batch.
+// One pass over every tile of every state in the batch.  With `cycles`, thread
+// 0 of each CTA adds the clock64() cycles every operation took on each tile it
+// processed (one slot per operation), for the cost model's training data.
 void tile_pass(const Batch& b, const int* tile_qubits_dev, int m, const TileOp* ops_dev, int nops,
-               const double2* pool_dev, const TilePass& host_pass);
+               const double2* pool_dev, const TilePass& host_pass, unsigned long long* cycles = nullptr);
 size_t tile_smem_bytes(int m, bool c64);
 }  // namespace k
 

@@ -183,6 +183,40 @@ DQ_API int dq_batch_statevector(const dq_batch* b, uint64_t index, double* out, 
 DQ_API int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items);
 DQ_API void dq_batch_free(dq_batch* b);
 
+/* Learned fusion cost model (no counterpart in the reference): a 16-64-64-1
+ * FP32 MLP predicting log device cycles per tile of one tile-local operation
+ * from the features written by the engine (kind, width, tile-local qubit
+ * positions, fused gate count, work per tile, tile size, precision).
+ * Training, gradients and inference run in CUDA kernels of this library.
+ * `record` runs a unitary circuit once with per-operation clock64() timing
+ * and appends its samples.  Attached to a simulator, the model picks each
+ * tile pass's fusion width; a prepared circuit (dq_plan) then times the
+ * learned plan against the greedy fixed-width plan, keeps the faster, and
+ * logs a rejection when the learned plan is slower.  Detach a model before
+ * freeing it. */
+typedef struct dq_cost_model dq_cost_model;
+#define DQ_MLP_FEATURES 16
+#define DQ_MLP_PARAMS 5315 /* 5313 weights and biases + target mean and std */
+DQ_API int dq_cost_model_create(int device, uint64_t seed, dq_cost_model** out);
+DQ_API void dq_cost_model_free(dq_cost_model* m);
+DQ_API int dq_cost_model_add_samples(dq_cost_model* m, const float* features, const float* log_cycles, uint64_t n);
+DQ_API int dq_cost_model_record(dq_cost_model* m, dq_sim* sim, const char* json, size_t json_len, uint64_t* added);
+DQ_API int dq_cost_model_num_samples(const dq_cost_model* m, uint64_t* n);
+DQ_API int dq_cost_model_samples(const dq_cost_model* m, float* features, float* log_cycles, uint64_t n);
+DQ_API int dq_cost_model_train(dq_cost_model* m, int epochs, float lr, double* final_mse);
+DQ_API int dq_cost_model_predict(const dq_cost_model* m, const float* features, uint64_t n, float* log_cycles);
+/* Gradients of the mean squared error over one batch of 1..128 samples (no update). */
+DQ_API int dq_cost_model_gradients(const dq_cost_model* m, const float* features, const float* log_cycles, uint64_t n,
+                                   float* grads);
+DQ_API int dq_cost_model_get_params(const dq_cost_model* m, float* out, uint64_t len);
+DQ_API int dq_cost_model_set_params(dq_cost_model* m, const float* in, uint64_t len);
+DQ_API int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m);
+/* Planner outcome of a prepared circuit built while a model was attached. */
+DQ_API int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int* used_learned, int* rejected);
+DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops);
+/* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
+DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
+
 /* Host-only helpers (no device work): parse, validate and compile a circuit
  * exactly as read_circuit + compile do (simulator.rs:204-211,
  * execution.rs:368-416), returning the operation list as JSON text with
