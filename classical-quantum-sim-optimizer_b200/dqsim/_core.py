@@ -436,6 +436,18 @@ class PreparedCircuit:
         _check(_plan_samples(self._h, out.ctypes.data_as(_P), self.shots))
         return out
 
+    def planner(self):
+        """Learned-vs-greedy outcome of this plan (all zero when no cost model was attached)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        u, r = ctypes.c_int(), ctypes.c_int()
+        _check(_plan_planner(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(u), ctypes.byref(r)))
+        return {"learned_ms": a.value, "greedy_ms": b.value, "used_learned": bool(u.value), "rejected": bool(r.value)}
+
+    def shape(self):
+        p, t = _u64(), _u64()
+        _check(_plan_shape(self._h, ctypes.byref(p), ctypes.byref(t)))
+        return {"passes": p.value, "tile_ops": t.value}
+
     def compare(self, other):
         """(fidelity |<self|other>|^2, max amplitude error) of the two final states."""
         f, e = ctypes.c_double(), ctypes.c_double()
@@ -503,6 +515,120 @@ class BatchedCircuits:
 
 
 BATCH_SEED_STRIDE = 0x9E3779B97F4A7C15
+
+MLP_FEATURES = 16
+MLP_PARAMS = 5315
+_cm_create = _sig("dq_cost_model_create", [ctypes.c_int, _u64, ctypes.POINTER(_P)])
+_cm_free = _sig("dq_cost_model_free", [_P], None)
+_cm_add = _sig("dq_cost_model_add_samples", [_P, _P, _P, _u64])
+_cm_record = _sig("dq_cost_model_record", [_P, _P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_u64)])
+_cm_num = _sig("dq_cost_model_num_samples", [_P, ctypes.POINTER(_u64)])
+_cm_samples = _sig("dq_cost_model_samples", [_P, _P, _P, _u64])
+_cm_train = _sig("dq_cost_model_train", [_P, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_double)])
+_cm_predict = _sig("dq_cost_model_predict", [_P, _P, _u64, _P])
+_cm_grads = _sig("dq_cost_model_gradients", [_P, _P, _P, _u64, _P])
+_cm_get = _sig("dq_cost_model_get_params", [_P, _P, _u64])
+_cm_set = _sig("dq_cost_model_set_params", [_P, _P, _u64])
+_sim_set_cm = _sig("dq_sim_set_cost_model", [_P, _P])
+_plan_planner = _sig("dq_plan_planner", [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
+_plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_sim_log = _sig("dq_sim_planner_log", [_P, ctypes.POINTER(ctypes.c_char_p)])
+
+
+def _f32(a, cols=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if cols is not None and (a.ndim != 2 or a.shape[1] != cols):
+        raise ValueError(f"expected an array of shape (n, {cols})")
+    return a
+
+
+class CostModel:
+    """The planner's learned cost model (dq_cost_model_*): MLP 16-64-64-1, trained on device."""
+
+    def __init__(self, device=0, seed=0):
+        h = _P()
+        _check(_cm_create(int(device), _as_u64(seed, "seed"), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _cm_free(h)
+            self._h = None
+
+    def add_samples(self, features, log_cycles):
+        X = _f32(features, MLP_FEATURES)
+        y = _f32(log_cycles).reshape(-1)
+        if y.shape[0] != X.shape[0]:
+            raise ValueError("features and targets differ in length")
+        _check(_cm_add(self._h, X.ctypes.data_as(_P), y.ctypes.data_as(_P), y.shape[0]))
+
+    def record(self, simulator, circuit):
+        """Run a unitary circuit once with per-operation timing; returns samples added."""
+        text = _circuit_json(circuit)
+        n = _u64()
+        _check(_cm_record(self._h, simulator._h, text, len(text), ctypes.byref(n)))
+        return n.value
+
+    @property
+    def num_samples(self):
+        n = _u64()
+        _check(_cm_num(self._h, ctypes.byref(n)))
+        return n.value
+
+    def samples(self):
+        n = self.num_samples
+        X = np.empty((n, MLP_FEATURES), dtype=np.float32)
+        y = np.empty(n, dtype=np.float32)
+        _check(_cm_samples(self._h, X.ctypes.data_as(_P), y.ctypes.data_as(_P), n))
+        return X, y
+
+    def train(self, epochs=60, lr=2e-3):
+        mse = ctypes.c_double()
+        _check(_cm_train(self._h, int(epochs), float(lr), ctypes.byref(mse)))
+        return mse.value
+
+    def predict(self, features):
+        X = _f32(features, MLP_FEATURES)
+        out = np.empty(X.shape[0], dtype=np.float32)
+        _check(_cm_predict(self._h, X.ctypes.data_as(_P), X.shape[0], out.ctypes.data_as(_P)))
+        return out
+
+    def gradients(self, features, targets):
+        X = _f32(features, MLP_FEATURES)
+        y = _f32(targets).reshape(-1)
+        g = np.empty(MLP_PARAMS - 2, dtype=np.float32)
+        _check(_cm_grads(self._h, X.ctypes.data_as(_P), y.ctypes.data_as(_P), X.shape[0], g.ctypes.data_as(_P)))
+        return g
+
+    @property
+    def params(self):
+        p = np.empty(MLP_PARAMS, dtype=np.float32)
+        _check(_cm_get(self._h, p.ctypes.data_as(_P), MLP_PARAMS))
+        return p
+
+    @params.setter
+    def params(self, value):
+        p = _f32(value).reshape(-1)
+        _check(_cm_set(self._h, p.ctypes.data_as(_P), p.shape[0]))
+
+
+def set_cost_model(simulator, model):
+    """Attach (or with None detach) a trained cost model to a simulator's planner."""
+    _check(_sim_set_cm(simulator._h, None if model is None else model._h))
+    simulator._cost_model = model
+
+
+def planner_log(simulator):
+    out = ctypes.c_char_p()
+    _check(_sim_log(simulator._h, ctypes.byref(out)))
+    try:
+        import json as _json
+
+        return [_json.loads(line) for line in out.value.decode().splitlines() if line.strip()]
+    finally:
+        _string_free(ctypes.cast(out, ctypes.c_void_p))
 
 
 def compile_dump(circuit_json):
