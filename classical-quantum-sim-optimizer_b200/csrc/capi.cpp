@@ -13,6 +13,11 @@
 
 using namespace dq;
 
+namespace dq {
+void measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit, int reset,
+                     const uint64_t* seeds, const uint64_t* draw_index, int* outcomes);
+}
+
 struct dq_plan {
     std::unique_ptr<Plan> impl;
 };
@@ -570,6 +575,13 @@ int dq_sim_planner_log(dq_sim* sim, char** out_text) {
         if (!buf) throw std::bad_alloc();
         std::memcpy(buf, s.c_str(), s.size() + 1);
         *out_text = buf;
+    });
+}
+
+int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit,
+                       int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes) {
+    return guard([&] {
+        measure_noalloc(states, precision, num_states, num_qubits, qubit, reset, seeds, draw_index, outcomes);
     });
 }
 

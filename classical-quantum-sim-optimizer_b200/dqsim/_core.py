@@ -534,6 +534,7 @@ _plan_planner = _sig("dq_plan_planner", [_P, ctypes.POINTER(ctypes.c_double), ct
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
 _plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
 _sim_log = _sig("dq_sim_planner_log", [_P, ctypes.POINTER(ctypes.c_char_p)])
+_measure_noalloc = _sig("dq_measure_noalloc", [_P, ctypes.c_int, _u64, _u64, _u64, ctypes.c_int, _P, _P, _P])
 
 
 def _f32(a, cols=None):
@@ -629,6 +630,22 @@ def planner_log(simulator):
         return [_json.loads(line) for line in out.value.decode().splitlines() if line.strip()]
     finally:
         _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+def measure_noalloc(states_ptr, precision, num_states, num_qubits, qubit, seeds, draw_index, reset=False):
+    """dq_measure_noalloc: measure states already in device memory, allocating nothing on the device.
+
+    states_ptr is a device address (e.g. a CUDA tensor's data_ptr()); returns the outcomes.
+    """
+    prec = PRECISIONS[str(precision).lower()] if not isinstance(precision, int) else precision
+    s = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(-1))
+    d = np.ascontiguousarray(np.asarray(draw_index, dtype=np.uint64).reshape(-1))
+    if s.shape[0] != num_states or d.shape[0] != num_states:
+        raise ValueError("seeds and draw_index need one entry per state")
+    out = np.zeros(num_states, dtype=np.int32)
+    _check(_measure_noalloc(ctypes.c_void_p(int(states_ptr)), prec, num_states, num_qubits, qubit, 1 if reset else 0,
+                            s.ctypes.data_as(_P), d.ctypes.data_as(_P), out.ctypes.data_as(_P)))
+    return out.tolist()
 
 
 def compile_dump(circuit_json):

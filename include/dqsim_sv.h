@@ -217,6 +217,26 @@ DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops)
 /* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
 DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
 
+/* Measure without allocating.  No counterpart in the reference: it serves
+ * callers that cannot call cudaMalloc -- code running while a CUDA stream is
+ * being captured, hosts whose device memory belongs to their own budgeted
+ * allocator, and latency-bound loops that cannot afford the device-wide
+ * synchronisation an allocation may cause.  It measures `qubit` of each of
+ * `num_states` states of 2^num_qubits amplitudes stored back to back at
+ * `states` (the caller's device memory, complex128 or complex64 by
+ * `precision`), drawing from ChaCha8 stream seeds[i] at draw draw_index[i]
+ * (the per-trajectory streams of shots.rs:224), collapses each state in place
+ * (reset != 0 also returns the qubit to |0>) and writes each outcome to host
+ * memory outcomes[i].  It calls no cudaMalloc, cudaFree or allocating
+ * library routine: its scratch is a fixed 256 KiB __device__ array that
+ * every GPU loading this library holds until exit, looked up on the first
+ * call on each device (make that first call before any stream capture).
+ * Requests whose scratch would exceed 256 KiB (about 15 states of 22+
+ * qubits, thousands of small states) fail with DQ_VALUE_ERROR.  All calls
+ * share that array: calls whose GPU work overlaps race on it. */
+DQ_API int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit,
+                              int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes);
+
 /* Host-only helpers (no device work): parse, validate and compile a circuit
  * exactly as read_circuit + compile do (simulator.rs:204-211,
  * execution.rs:368-416), returning the operation list as JSON text with
