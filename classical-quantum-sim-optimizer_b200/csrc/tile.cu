@@ -483,22 +483,79 @@ __device__ __forceinline__ uint32_t expand_local(uint32_t j, const TileOp& op) {
     return j;
 }
 
+// Insertion positions of one operation, held in registers for its whole loop.
+struct Ins {
+    int n;
+    int p[7];
+};
+
+__device__ __forceinline__ Ins load_ins(const TileOp& op) {
+    Ins s;
+    s.n = op.nins;
+#pragma unroll
+    for (int t = 0; t < 7; t++) s.p[t] = op.ins[t];
+    return s;
+}
+
+__device__ __forceinline__ uint32_t expand_ins(uint32_t j, const Ins& s) {
+#pragma unroll
+    for (int t = 0; t < 7; t++) {
+        if (t < s.n) {
+            uint32_t low = (1u << s.p[t]) - 1;
+            j = (j & low) | ((j & ~low) << 1);
+        }
+    }
+    return j;
+}
+
+// 1- and 2-qubit dense matrices: matrix and offsets in registers, rows fully
+// unrolled so the 4 (16) complex products of a group are independent.
+template <typename V, int K>
+__device__ void tile_dense_small(V* __restrict__ tile, const TileOp& op, int m, const double2* __restrict__ pool) {
+    constexpr int D = 1 << K;
+    const uint32_t items = 1u << (m - K);
+    V M[D * D];
+#pragma unroll
+    for (int i = 0; i < D * D; i++) M[i] = dev::from_d2<V>(__ldg(pool + op.mat + i));
+    uint32_t off[D];
+#pragma unroll
+    for (int c = 0; c < D; c++) off[c] = op.offs[c];
+    const Ins ins = load_ins(op);
+    for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
+        const uint32_t base = expand_ins(j, ins);
+        V v[D];
+#pragma unroll
+        for (int c = 0; c < D; c++) v[c] = tile[base | off[c]];
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+            V acc = dev::cmul(M[r * D], v[0]);
+#pragma unroll
+            for (int c = 1; c < D; c++) acc = dev::cadd(acc, dev::cmul(M[r * D + c], v[c]));
+            tile[base | off[r]] = acc;
+        }
+    }
+}
+
 template <typename V, int K>
 __device__ void tile_dense(V* __restrict__ tile, const TileOp& op, int m, const double2* __restrict__ pool) {
     constexpr int D = 1 << K;
     const uint32_t items = 1u << (m - K);
     const double2* mat = pool + op.mat;
+    uint32_t off[D];
+#pragma unroll
+    for (int c = 0; c < D; c++) off[c] = op.offs[c];
+    const Ins ins = load_ins(op);
     for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
-        const uint32_t base = expand_local(j, op);
+        const uint32_t base = expand_ins(j, ins);
         V v[D];
 #pragma unroll
-        for (int c = 0; c < D; c++) v[c] = tile[base | op.offs[c]];
+        for (int c = 0; c < D; c++) v[c] = tile[base | off[c]];
 #pragma unroll 1
         for (int r = 0; r < D; r++) {
             V acc = dev::czero<V>();
 #pragma unroll
             for (int c = 0; c < D; c++) acc = dev::cadd(acc, dev::cmul(dev::from_d2<V>(__ldg(mat + r * D + c)), v[c]));
-            tile[base | op.offs[r]] = acc;
+            tile[base | op.offs[r]] = acc;  // row offset from the (cached) descriptor: no dynamic register index
         }
     }
 }
@@ -508,7 +565,9 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
     switch (op.type) {
         case TileOp::kOne:
         case TileOp::kX: {
-            const uint32_t items = 1u << (m - op.nins);
+            const Ins ins = load_ins(op);
+            const uint32_t items = 1u << (m - ins.n);
+            const uint32_t fixed = op.fixed, tbit = op.tbit;
             const bool is_x = op.type == TileOp::kX;
             V u00 = dev::czero<V>(), u01 = u00, u10 = u00, u11 = u00;
             if (!is_x) {
@@ -518,7 +577,7 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
                 u11 = dev::from_d2<V>(__ldg(pool + op.mat + 3));
             }
             for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
-                const uint32_t i0 = expand_local(j, op) | op.fixed, i1 = i0 | op.tbit;
+                const uint32_t i0 = expand_ins(j, ins) | fixed, i1 = i0 | tbit;
                 V a = tile[i0], b = tile[i1];
                 if (is_x) {
                     tile[i0] = b;
@@ -531,10 +590,12 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
             break;
         }
         case TileOp::kDiagEntry: {
-            const uint32_t items = 1u << (m - op.nins);
+            const Ins ins = load_ins(op);
+            const uint32_t items = 1u << (m - ins.n);
+            const uint32_t fixed = op.fixed;
             const V v = dev::from_d2<V>(__ldg(pool + op.mat));
             for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
-                const uint32_t i = expand_local(j, op) | op.fixed;
+                const uint32_t i = expand_ins(j, ins) | fixed;
                 tile[i] = dev::cmul(tile[i], v);
             }
             break;
@@ -549,19 +610,21 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
             break;
         }
         case TileOp::kSwap: {
-            const uint32_t items = 1u << (m - op.nins);
+            const Ins ins = load_ins(op);
+            const uint32_t items = 1u << (m - ins.n);
+            const uint32_t fixed = op.fixed, lo = op.lowbit, hi = op.highbit;
             for (uint32_t j = threadIdx.x; j < items; j += blockDim.x) {
-                const uint32_t i = expand_local(j, op) | op.fixed;
-                V a = tile[i | op.lowbit];
-                tile[i | op.lowbit] = tile[i | op.highbit];
-                tile[i | op.highbit] = a;
+                const uint32_t i = expand_ins(j, ins) | fixed;
+                V a = tile[i | lo];
+                tile[i | lo] = tile[i | hi];
+                tile[i | hi] = a;
             }
             break;
         }
         case TileOp::kDense:
             switch (op.k) {
-                case 1: tile_dense<V, 1>(tile, op, m, pool); break;
-                case 2: tile_dense<V, 2>(tile, op, m, pool); break;
+                case 1: tile_dense_small<V, 1>(tile, op, m, pool); break;
+                case 2: tile_dense_small<V, 2>(tile, op, m, pool); break;
                 case 3: tile_dense<V, 3>(tile, op, m, pool); break;
             }
             break;
@@ -569,7 +632,7 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
 }
 
 template <typename V, bool TIMED>
-__global__ void __launch_bounds__(kTileThreads) k_tile(V* __restrict__ s, int n, int m, TileQubits tq,
+__global__ void __launch_bounds__(kTileThreads, 2) k_tile(V* __restrict__ s, int n, int m, TileQubits tq,
                                                        const TileOp* __restrict__ ops, int nops,
                                                        const double2* __restrict__ pool, uint64_t total_tiles,
                                                        unsigned long long* __restrict__ cycles) {
