@@ -558,11 +558,12 @@ int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int
     });
 }
 
-int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops) {
+int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops, uint64_t* fused_blocks) {
     return guard([&] {
         need(p, "plan");
         if (passes) *passes = p->impl->passes();
         if (tile_ops) *tile_ops = p->impl->tile_ops();
+        if (fused_blocks) *fused_blocks = p->impl->fused_blocks();
     });
 }
 
@@ -645,6 +646,58 @@ int dq_tile_plan_dump(const char* json, size_t len, int tile_qubits, int fusion_
         if (!out) throw std::bad_alloc();
         std::memcpy(out, s.c_str(), s.size() + 1);
         *out_text = out;
+    });
+}
+
+int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
+    return guard([&] {
+        need(json, "json");
+        need(out_text, "out_text");
+        uint64_t n = 0, ncb = 0;
+        auto ops = compile_json(json, len, &n, &ncb);
+        for (auto& op : ops)
+            if (!op.is_unitary()) fail(kValueError, "circuit has non-unitary operations");
+        if (n < uint64_t(kFusedM)) fail(kValueError, "fused passes need at least 12 qubits");
+        TilePlanOptions o;
+        o.m = kFusedM;
+        o.keep_raw = true;
+        std::vector<double2> pool;
+        auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
+        std::vector<FusedBlock> blocks;
+        std::vector<float> upool;
+        std::string s = "{\"n\":" + std::to_string(n) + ",\"passes\":[";
+        char buf[48];
+        for (size_t pi = 0; pi < passes.size(); pi++) {
+            FusedPass fp = build_fused_pass(passes[pi].raw, passes[pi].qubits, blocks, upool);
+            s += pi ? ",{" : "{";
+            s += "\"raw\":" + std::to_string(fp.raw_ops) + ",\"qubits\":[";
+            for (size_t i = 0; i < fp.qubits.size(); i++) s += (i ? "," : "") + std::to_string(fp.qubits[i]);
+            s += "],\"in_lo\":[";
+            for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.in_lo[i]);
+            s += "],\"in_hi\":[";
+            for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.in_hi[i]);
+            s += "],\"blocks\":[";
+            for (int bi = 0; bi < fp.nblocks; bi++) {
+                const FusedBlock& b = blocks[size_t(fp.first_block + bi)];
+                s += bi ? ",{" : "{";
+                s += "\"u_off\":" + std::to_string(b.u_off) + ",\"last\":" + std::to_string(b.last) + ",\"next_b\":[";
+                for (int i = 0; i < 32; i++) s += (i ? "," : "") + std::to_string(b.next_b[i]);
+                s += "],\"next_c\":[";
+                for (int i = 0; i < kFusedCols; i++) s += (i ? "," : "") + std::to_string(b.next_c[i]);
+                s += "]}";
+            }
+            s += "]}";
+        }
+        s += "],\"upool\":[";
+        for (size_t i = 0; i < upool.size(); i++) {
+            std::snprintf(buf, sizeof buf, "%s%.9g", i ? "," : "", upool[i]);
+            s += buf;
+        }
+        s += "]}";
+        char* outp = static_cast<char*>(std::malloc(s.size() + 1));
+        if (!outp) throw std::bad_alloc();
+        std::memcpy(outp, s.c_str(), s.size() + 1);
+        *out_text = outp;
     });
 }
 

@@ -146,7 +146,7 @@ double Executor::step_bytes(size_t i, const k::Batch& b) const {
     const Step& s = steps_[i];
     const double S = b.c64 ? 8.0 : 16.0;
     const double full = S * double(uint64_t(1) << b.n) * double(b.W);
-    if (s.pass >= 0) return 2.0 * full;
+    if (s.pass >= 0 || s.fused >= 0) return 2.0 * full;
     switch (s.type) {
         case Operation::One:
         case Operation::X: return 2.0 * full / double(uint64_t(1) << s.controls.size());
@@ -193,6 +193,20 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     o.c64 = cfg_.c64;
     o.model = cfg_.model;
     o.chosen_widths = &widths_;
+    if (cfg_.fused && cfg_.c64 && cfg_.n >= kFusedM) {
+        o.m = kFusedM;
+        o.keep_raw = true;
+        std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
+        for (auto& p : ps) {
+            Step s;
+            s.fused = int(fused_.size());
+            s.type = Operation::Dense;
+            s.category = 1;
+            fused_.push_back(build_fused_pass(p.raw, p.qubits, fused_blocks_host_, upool_host_));
+            steps_.push_back(std::move(s));
+        }
+        return;
+    }
     std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
     for (auto& p : ps) {
         p.op_begin = int(tile_ops_host_.size());
@@ -320,9 +334,20 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
                                        cudaMemcpyHostToDevice, b.stream),
                        "upload tile operations");
         }
+        if (!fused_blocks_host_.empty()) {
+            fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
+            upool_.alloc(upool_host_.size() * sizeof(float), "fused block gate images");
+            cuda_check(cudaMemcpyAsync(fused_blocks_.p, fused_blocks_host_.data(),
+                                       fused_blocks_host_.size() * sizeof(FusedBlock), cudaMemcpyHostToDevice, b.stream),
+                       "upload fused blocks");
+            cuda_check(cudaMemcpyAsync(upool_.p, upool_host_.data(), upool_host_.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, b.stream),
+                       "upload gate images");
+        }
         uploaded_ = true;
     }
     std::vector<uint64_t> host_cbits;
+    bool norm_pending = false;  // a fused pass left a norm the next fused pass divides out
     for (size_t si = 0; si < steps_.size(); si++) {
         const Step& s = steps_[si];
         if (profile && s.cond.n) {
@@ -345,6 +370,29 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
             if (!ok) continue;
         }
         auto t0 = std::chrono::steady_clock::now();
+        if (s.fused >= 0) {
+            const FusedPass& p = fused_[size_t(s.fused)];
+            const size_t tiles = size_t(b.W) << (b.n - kFusedM);
+            norm_tiles_.ensure(tiles * 8, "fused tile norms");
+            norm_states_.ensure(size_t(b.W) * 8, "fused state norms");
+            if (rec) rec->begin(kcFused, step_bytes(si, b));
+            k::fused_pass(b, p, fused_blocks_.as<FusedBlock>(), upool_.as<float>(), b.err,
+                          norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>());
+            k::fused_state_norm(b, norm_tiles_.as<double>(), norm_states_.as<double>());
+            norm_pending = true;
+            const bool last_fused = si + 1 == steps_.size() || steps_[si + 1].fused < 0;
+            if (last_fused) {
+                k::fused_renormalize(b, norm_states_.as<double>());
+                norm_pending = false;
+            }
+            if (rec) rec->end();
+            if (profile) {
+                cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+                profile->nq_calls++;
+                profile->nq_time += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            }
+            continue;
+        }
         if (s.pass >= 0) {
             const TilePass& p = passes_[size_t(s.pass)];
             if (rec) rec->begin(kcTile, step_bytes(si, b));

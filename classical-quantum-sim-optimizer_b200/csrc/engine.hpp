@@ -109,6 +109,7 @@ struct ExecConfig {
     int n = 0;           // qubits of the state the plan runs on
     bool c64 = false;
     const CostModel* model = nullptr;  // learned fusion-width choice per pass
+    bool fused = false;  // complex64: 5-qubit blocks on tcgen05 (12-qubit tiles)
 };
 
 // A compiled operation list lowered to launch descriptors, with every matrix
@@ -124,7 +125,8 @@ class Executor {
     // Algorithmic bytes one step moves for a batch (the roofline numerator).
     double step_bytes(size_t i, const k::Batch& b) const;
 
-    size_t passes() const { return passes_.size(); }
+    size_t passes() const { return passes_.size() + fused_.size(); }
+    size_t fused_blocks() const { return fused_blocks_host_.size(); }
     size_t raw_ops_in_passes() const;
     const std::vector<int>& chosen_widths() const { return widths_; }
     size_t tile_ops() const { return tile_ops_host_.size(); }
@@ -134,7 +136,8 @@ class Executor {
 
   private:
     struct Step {
-        int pass = -1;  // >= 0: a tile pass (index into passes_)
+        int pass = -1;   // >= 0: a tile pass (index into passes_)
+        int fused = -1;  // >= 0: a tensor-core fused pass (index into fused_)
         Operation::Type type;
         int target = 0, a = 0, b = 0;
         std::vector<k::Ctl> controls;
@@ -151,7 +154,10 @@ class Executor {
     std::vector<double2> pool_host_;
     std::vector<TilePass> passes_;
     std::vector<TileOp> tile_ops_host_;
-    DevMem pool_, tile_ops_;
+    std::vector<FusedPass> fused_;
+    std::vector<FusedBlock> fused_blocks_host_;
+    std::vector<float> upool_host_;
+    DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_;
     bool uploaded_ = false;
     ExecConfig cfg_;
     std::vector<int> widths_;

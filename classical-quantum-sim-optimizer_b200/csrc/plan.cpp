@@ -108,6 +108,7 @@ double Plan::run(bool record) {
     if (record) rec.collect(ms_, launches_, bytes_);
     int flag = 0;
     cuda_check(cudaMemcpy(&flag, st_.err.p, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+    if (flag == 3) fail(kRuntimeError, "a tensor-core pass gave up on a bounded wait");
     if (flag) fail(kRuntimeError, "Cannot measure or sample a state with nonfinite or zero norm");
     return double(ms);
 }

@@ -39,6 +39,7 @@ class Plan {
     }
     size_t passes() const { return ex_ ? ex_->passes() : 0; }
     size_t tile_ops() const { return ex_ ? ex_->tile_ops() : 0; }
+    size_t fused_blocks() const { return ex_ ? ex_->fused_blocks() : 0; }
     // Appends per-operation cost samples of one recorded run.
     void record_costs(std::vector<float>& X, std::vector<float>& y);
 

@@ -45,6 +45,7 @@ void check_err_flag(const StateBatch& st, cudaStream_t s) {
     int flag = 0;
     cuda_check(cudaMemcpyAsync(&flag, st.err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "read error flag");
     cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+    if (flag == 3) fail(kRuntimeError, "a tensor-core pass gave up on a bounded wait");
     if (flag) fail(kRuntimeError, "Cannot measure a state with nonfinite or zero norm");
 }
 
@@ -100,6 +101,7 @@ ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate, const 
     c.tiled = !force_per_gate && o.execution != 1;
     c.tile_m = o.tile_qubits > 0 ? o.tile_qubits : (c.c64 ? 13 : 12);
     c.fuse = o.fusion_width > 0 ? o.fusion_width : 2;
+    c.fused = c.c64 && c.tiled && o.fusion_width == 5;
     c.n = int(n);
     return c;
 }

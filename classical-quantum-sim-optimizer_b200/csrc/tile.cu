@@ -191,6 +191,135 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
 }
 
 // ---------------------------------------------------------------------------
+// Fused tensor-core blocks
+// ---------------------------------------------------------------------------
+namespace {
+
+// Round to TF32 (10 explicit mantissa bits), to nearest with ties away from
+// zero, as cvt.rna.tf32.f32 does on the device.
+float tf32_rna(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// Float offset of (row, k) in the canonical K-major, no-swizzle operand layout
+// with 64 K-elements per row: 8-row x 16-byte core matrices, the K chunks of a
+// row group 128 B apart, row groups 2048 B apart.
+inline size_t canon(int row, int k) { return size_t(row / 8) * 512 + size_t(k / 4) * 32 + size_t(row % 8) * 4 + k % 4; }
+
+}  // namespace
+
+FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
+                           std::vector<FusedBlock>& blocks, std::vector<float>& upool) {
+    FusedPass fp;
+    fp.qubits = tile_qubits;
+    fp.raw_ops = int(pass_ops.size());
+    fp.first_block = int(blocks.size());
+    const int m = int(tile_qubits.size());
+    if (m != kFusedM) fail(kValueError, "fused passes hold exactly 12 tile qubits");
+    std::vector<int> local(64, -1);
+    for (int i = 0; i < m; i++) local[tile_qubits[i]] = i;
+    // Block list: 5-qubit fusion, each block as (local qubits MSB-first, 32x32 matrix).
+    struct Blk {
+        int q[5];
+        std::vector<cplx> u;
+    };
+    std::vector<Blk> blk;
+    for (const Operation& op : fuse_ops(pass_ops, 5)) {
+        std::vector<uint64_t> oq;
+        std::vector<cplx> om;
+        op_matrix(op, oq, om);
+        std::vector<uint64_t> bq = oq;
+        for (int i = 0; i < m && bq.size() < 5; i++) {
+            uint64_t g = uint64_t(tile_qubits[i]);
+            if (std::find(bq.begin(), bq.end(), g) == bq.end()) bq.push_back(g);
+        }
+        std::vector<cplx> acc(32 * 32, cplx(0));
+        for (int i = 0; i < 32; i++) acc[size_t(i) * 32 + i] = cplx(1);
+        left_multiply(bq, acc, oq, om);
+        Blk b;
+        for (int t = 0; t < 5; t++) b.q[t] = local[bq[t]];
+        b.u = std::move(acc);
+        blk.push_back(std::move(b));
+    }
+    if (blk.empty()) {  // a pass of nothing but identities: one identity block
+        Blk b;
+        for (int t = 0; t < 5; t++) b.q[t] = 4 - t;
+        b.u.assign(32 * 32, cplx(0));
+        for (int i = 0; i < 32; i++) b.u[size_t(i) * 32 + i] = cplx(1);
+        blk.push_back(std::move(b));
+    }
+    // Layout of block j: packed = (pext(l, other_j) << 5) | basis_j(l), basis MSB = q[0].
+    auto others = [&](const Blk& b) {
+        std::vector<int> o;
+        for (int i = 0; i < m; i++)
+            if (std::find(b.q, b.q + 5, i) == b.q + 5) o.push_back(i);
+        return o;
+    };
+    auto layout = [&](const Blk& b, const std::vector<int>& oth, uint32_t l) {
+        uint32_t basis = 0, col = 0;
+        for (int t = 0; t < 5; t++) basis = (basis << 1) | ((l >> b.q[t]) & 1u);
+        for (size_t t = 0; t < oth.size(); t++) col |= ((l >> oth[t]) & 1u) << t;
+        return uint16_t((col << 5) | basis);
+    };
+    auto dep_basis = [&](const Blk& b, uint32_t basis) {
+        uint32_t l = 0;
+        for (int t = 0; t < 5; t++) l |= ((basis >> (4 - t)) & 1u) << b.q[t];
+        return l;
+    };
+    auto dep_col = [&](const std::vector<int>& oth, uint32_t col) {
+        uint32_t l = 0;
+        for (size_t t = 0; t < oth.size(); t++) l |= ((col >> t) & 1u) << oth[t];
+        return l;
+    };
+    std::vector<std::vector<int>> oth(blk.size());
+    for (size_t j = 0; j < blk.size(); j++) oth[j] = others(blk[j]);
+    for (int e = 0; e < 64; e++) {
+        fp.in_lo[e] = layout(blk[0], oth[0], uint32_t(e));
+        fp.in_hi[e] = layout(blk[0], oth[0], uint32_t(e) << 6);
+    }
+    for (size_t j = 0; j < blk.size(); j++) {
+        FusedBlock d;
+        std::memset(&d, 0, sizeof d);
+        d.u_off = uint32_t(upool.size());
+        d.last = j + 1 == blk.size() ? 1u : 0u;
+        for (uint32_t bb = 0; bb < 32; bb++) {
+            uint32_t l = dep_basis(blk[j], bb);
+            d.next_b[bb] = d.last ? uint16_t(l) : layout(blk[j + 1], oth[j + 1], l);
+        }
+        for (uint32_t c = 0; c < uint32_t(kFusedCols); c++) {
+            uint32_t l = dep_col(oth[j], c);
+            d.next_c[c] = d.last ? uint16_t(l) : layout(blk[j + 1], oth[j + 1], l);
+        }
+        // Real 64x64 form [[Re, -Im], [Im, Re]] with rows 2b'+ri' and columns 2b+ri,
+        // stored as the B operand (N = 64 output rows, K = 64 inputs, K-major).
+        std::vector<float> img(kFusedUFloats, 0.f);
+        for (int bo = 0; bo < 32; bo++)
+            for (int bi = 0; bi < 32; bi++) {
+                const cplx v = blk[j].u[size_t(bo) * 32 + bi];
+                const double e[2][2] = {{v.re, -v.im}, {v.im, v.re}};
+                for (int ro = 0; ro < 2; ro++)
+                    for (int ri = 0; ri < 2; ri++) {
+                        float f = float(e[ro][ri]);
+                        float hi = tf32_rna(f);
+                        float lo = tf32_rna(f - hi);
+                        size_t o = canon(2 * bo + ro, 2 * bi + ri);
+                        img[o] = hi;
+                        img[4096 + o] = lo;
+                    }
+            }
+        upool.insert(upool.end(), img.begin(), img.end());
+        blocks.push_back(d);
+    }
+    fp.nblocks = int(blk.size());
+    return fp;
+}
+
+// ---------------------------------------------------------------------------
 // Pass planner
 // ---------------------------------------------------------------------------
 namespace {
@@ -436,6 +565,11 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
         std::vector<Operation> pass_ops;
         for (size_t o : taken) pass_ops.push_back(ops[begin + o]);
         p.raw_ops = int(pass_ops.size());
+        if (opt.keep_raw) {
+            p.raw = std::move(pass_ops);
+            passes.push_back(std::move(p));
+            continue;
+        }
         int width = opt.fuse;
         if (opt.model) {
             // The cost model judges each candidate width by its lowered operations.

@@ -42,6 +42,7 @@ struct TilePass {
     std::vector<TileOp> ops;
     int op_begin = 0;         // index into the device op array
     int raw_ops = 0;          // unfused operations covered (for statistics)
+    std::vector<Operation> raw;  // filled when TilePlanOptions::keep_raw
 };
 
 struct TilePlanOptions {
@@ -53,6 +54,9 @@ struct TilePlanOptions {
     // whose lowered operations have the smallest predicted cost.
     const CostModel* model = nullptr;
     std::vector<int>* chosen_widths = nullptr;  // filled per pass when given
+    // Keep each pass's raw operations (for fused tensor-core blocks) instead
+    // of lowering them to tile-local operations.
+    bool keep_raw = false;
 };
 
 // Widest dense operation a tile pass applies on CUDA cores (register budget).
@@ -71,6 +75,51 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
 // Greedy dependency-respecting fusion of a topologically ordered op list into
 // dense operations of at most `width` qubits (width 1 leaves gates alone).
 std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width);
+
+// ---------------------------------------------------------------------------
+// Tensor-core fused blocks (complex64): a pass of 12 tile qubits whose
+// operations are fused into 32x32 complex blocks, each applied as one
+// 128 x 64 x 192 TF32 contraction (3xTF32 split) on tcgen05.
+// ---------------------------------------------------------------------------
+constexpr int kFusedM = 12;            // tile qubits of a fused pass
+constexpr int kFusedCols = 1 << (kFusedM - 5);
+constexpr int kFusedUFloats = 2 * 64 * 64;  // U_hi and U_lo images of one block
+
+// Device descriptor of one block.  Packed tile positions are (column << 5) | basis.
+struct alignas(16) FusedBlock {
+    uint32_t u_off;          // float offset of the block's U_hi/U_lo image in the pool
+    uint32_t last;           // 1: outputs go to natural tile order
+    uint32_t pad[2];
+    uint16_t next_b[32];     // output basis -> packed position for the next block (or natural index)
+    uint16_t next_c[128];    // output column -> packed position part
+};
+
+struct FusedPass {
+    std::vector<int> qubits;   // 12 ascending global positions
+    int first_block = 0, nblocks = 0;
+    uint16_t in_lo[64], in_hi[64];  // natural local index -> packed position of block 0
+    int raw_ops = 0;
+};
+
+// Fuses a pass's operations into 5-qubit blocks and appends their descriptors
+// and TF32 hi/lo gate images (canonical K-major operand layout).
+FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
+                           std::vector<FusedBlock>& blocks, std::vector<float>& upool);
+
+namespace k {
+// One fused pass over every tile of every state (complex64 only).  err: device
+// flag set to 3 when a bounded wait on an mbarrier runs out.
+// in_norm (per state, nullable): squared norm left by the previous fused pass,
+// divided out on load; tile_norm (W * 2^(n-12) doubles) receives each output
+// tile's FP64 squared norm.
+void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const float* upool_dev,
+                int* err_dev, const double* in_norm, double* tile_norm);
+// norm[st] = fixed-order sum of state st's tile norms.
+void fused_state_norm(const Batch& b, const double* tile_norm, double* norm);
+// Divides every state by the square root of its norm (FP64 scale).
+void fused_renormalize(const Batch& b, const double* norm);
+size_t fused_smem_bytes();
+}  // namespace k
 
 namespace k {
 // One pass over every tile of every state in the batch.  With `cycles`, thread

@@ -444,9 +444,9 @@ class PreparedCircuit:
         return {"learned_ms": a.value, "greedy_ms": b.value, "used_learned": bool(u.value), "rejected": bool(r.value)}
 
     def shape(self):
-        p, t = _u64(), _u64()
-        _check(_plan_shape(self._h, ctypes.byref(p), ctypes.byref(t)))
-        return {"passes": p.value, "tile_ops": t.value}
+        p, t, f = _u64(), _u64(), _u64()
+        _check(_plan_shape(self._h, ctypes.byref(p), ctypes.byref(t), ctypes.byref(f)))
+        return {"passes": p.value, "tile_ops": t.value, "fused_blocks": f.value}
 
     def compare(self, other):
         """(fidelity |<self|other>|^2, max amplitude error) of the two final states."""
@@ -532,7 +532,7 @@ _cm_set = _sig("dq_cost_model_set_params", [_P, _P, _u64])
 _sim_set_cm = _sig("dq_sim_set_cost_model", [_P, _P])
 _plan_planner = _sig("dq_plan_planner", [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
-_plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
 _sim_log = _sig("dq_sim_planner_log", [_P, ctypes.POINTER(ctypes.c_char_p)])
 _measure_noalloc = _sig("dq_measure_noalloc", [_P, ctypes.c_int, _u64, _u64, _u64, ctypes.c_int, _P, _P, _P])
 
@@ -672,6 +672,22 @@ def tile_plan_dump(circuit_json, tile_qubits=12, fusion_width=2):
     text = circuit_json.encode("utf-8") if isinstance(circuit_json, str) else circuit_json
     out = ctypes.c_char_p()
     _check(_tile_plan_dump(text, len(text), int(tile_qubits), int(fusion_width), ctypes.byref(out)))
+    try:
+        return _json.loads(out.value.decode("utf-8"))
+    finally:
+        _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+_fused_plan_dump = _sig("dq_fused_plan_dump", [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p)])
+
+
+def fused_plan_dump(circuit_json):
+    """Host-only: the tensor-core fused plan of a unitary circuit (for tests and inspection)."""
+    import json as _json
+
+    text = circuit_json.encode("utf-8") if isinstance(circuit_json, str) else circuit_json
+    out = ctypes.c_char_p()
+    _check(_fused_plan_dump(text, len(text), ctypes.byref(out)))
     try:
         return _json.loads(out.value.decode("utf-8"))
     finally:

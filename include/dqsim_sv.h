@@ -213,7 +213,8 @@ DQ_API int dq_cost_model_set_params(dq_cost_model* m, const float* in, uint64_t 
 DQ_API int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m);
 /* Planner outcome of a prepared circuit built while a model was attached. */
 DQ_API int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int* used_learned, int* rejected);
-DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops);
+/* Passes, CUDA-core tile operations and tensor-core fused blocks of the kept plan. */
+DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops, uint64_t* fused_blocks);
 /* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
 DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
 
@@ -246,6 +247,9 @@ DQ_API int dq_compile_dump(const char* json, size_t json_len, char** out_text);
  * (tile qubits, tile-local operations, matrix pool) as JSON text.  No
  * counterpart in the reference; it exposes the planner for inspection. */
 DQ_API int dq_tile_plan_dump(const char* json, size_t json_len, int tile_qubits, int fusion_width, char** out_text);
+/* Host-only: the tensor-core fused plan (12-qubit passes of 32x32 blocks: layout
+ * tables and TF32 hi/lo gate images) as JSON text.  No counterpart in the reference. */
+DQ_API int dq_fused_plan_dump(const char* json, size_t json_len, char** out_text);
 DQ_API void dq_string_free(char* s);
 
 #ifdef __cplusplus

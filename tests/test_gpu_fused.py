@@ -1,0 +1,66 @@
+"""The complex64 fused form on tcgen05 tensor cores (fusion_width=5) against the
+FP64 oracle: state fidelity >= 1 - 1e-6 and max amplitude error <= 1e-5."""
+
+import numpy as np
+import pytest
+
+from helpers import Circuit, assert_distribution, brickwork, conditional, hea, inst, qft, random_circuit
+from oracle import oracle as o
+
+import dqsim
+from dqsim import _core
+
+pytestmark = pytest.mark.gpu
+
+
+def fused(**kw):
+    return dqsim.StatevectorSimulator(precision="complex64", fusion_width=5, max_memory_mb=1 << 16, **kw)
+
+
+def check(circuit):
+    got = fused(seed=3).simulate(circuit).statevector
+    want = o.OracleSimulator(seed=3, max_memory_mb=1 << 16).simulate(circuit).statevector
+    fid = abs(np.vdot(got, want)) ** 2
+    err = float(np.max(np.abs(got - want)))
+    assert fid >= 1 - 1e-6, fid
+    assert err <= 1e-5, err
+    return fid, err
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: brickwork(12, 3, seed=1, measure=False),
+    lambda: brickwork(14, 10, seed=2, measure=False),
+    lambda: qft(16, seed=4),
+    lambda: hea(18, 8, seed=5),
+    lambda: brickwork(20, 20, seed=0, measure=False),
+])
+def test_fused_matches_oracle(maker):
+    check(maker())
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_fused_random_circuits(seed):
+    check(Circuit(15, random_circuit(seed, 15, 200)))
+
+
+def test_fused_trajectories_and_sampling():
+    ins = brickwork(14, 4, seed=7, measure=False).data["instructions"]
+    ins += [inst("measure", qubit=0, cbit=0), inst("reset", qubit=13), conditional(inst("x", qubit=13), 1),
+            inst("measure", qubit=13, cbit=1)]
+    ins += brickwork(14, 2, seed=8, measure=False).data["instructions"] + [inst("measure", qubit=5, cbit=2)]
+    c = Circuit(14, ins, 3)
+    counts = fused(seed=4).simulate_shots(c, 4000)
+    want = o.OracleSimulator(seed=4).simulate_shots(c, 4000)
+    assert sum(counts.values()) == 4000
+    assert all(k[1] == k[2] for k in counts)  # the reset qubit copies the first outcome
+    # same ChaCha8 streams; complex64 probabilities differ by ~1e-7, so almost every shot agrees
+    tvd = sum(abs(counts.get(k, 0) - want.get(k, 0)) for k in set(counts) | set(want)) / 2 / 4000
+    assert tvd < 0.01, (counts, want)
+    plan = _core.PreparedCircuit(fused(seed=1), brickwork(22, 12, seed=3, measure=True), shots=5000)
+    plan.run()
+    assert plan.shape()["passes"] > 0
+    ref = _core.PreparedCircuit(dqsim.StatevectorSimulator(seed=1, max_memory_mb=1 << 16),
+                                brickwork(22, 12, seed=3, measure=True), shots=5000)
+    ref.run()
+    fid, err = plan.compare(ref)
+    assert fid >= 1 - 1e-6 and err <= 1e-5
