@@ -408,12 +408,21 @@ BatchRun::BatchRun(Simulator& sim, const std::vector<std::string>& texts, uint64
     cuda_check(cudaMemcpyAsync(circ_off_.p, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, s), "upload");
     cuda_check(cudaMemcpyAsync(seeds_.p, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, s), "upload");
     const size_t smem = (S << max_m_);
-    if (c64_)
+    // Largest carveout: the occupancy query that sizes the persistent grid must
+    // match what the launch gets, since every CTA has to be resident at once.
+    if (c64_) {
         cuda_check(cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "smem attribute");
-    else
+        cuda_check(cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        int(cudaSharedmemCarveoutMaxShared)),
+                   "carveout attribute");
+    } else {
         cuda_check(cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        int(cudaSharedmemCarveoutMaxShared)),
+                   "carveout attribute");
+    }
     dev_->sync();
 }
 

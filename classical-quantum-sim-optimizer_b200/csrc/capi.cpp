@@ -676,6 +676,10 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.in_lo[i]);
             s += "],\"in_hi\":[";
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.in_hi[i]);
+            s += "],\"out_lo\":[";
+            for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_lo[i]);
+            s += "],\"out_hi\":[";
+            for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_hi[i]);
             s += "],\"blocks\":[";
             for (int bi = 0; bi < fp.nblocks; bi++) {
                 const FusedBlock& b = blocks[size_t(fp.first_block + bi)];

@@ -9,10 +9,14 @@
 // thread issues 24 tcgen05.mma.kind::tf32 instructions (M=128, N=64, K=8):
 // A_hi*B_hi + A_hi*B_lo + A_lo*B_hi accumulate into a 128 x 64 FP32 tile in
 // tensor memory.  The readback (tcgen05.ld, one TMEM lane per tile column)
-// writes every output amplitude straight into the layout the next block needs,
-// or, after the last block, into natural order for the store to HBM.
+// writes every output amplitude straight into the layout the next block needs
+// (128-byte swizzled, bit orders chosen on the host to spread each half-warp's
+// stores over all banks), or, after the last block, into a swizzled
+// natural-order stage for the store to HBM.  The next block's gate image and
+// layout tables are fetched while the current block is read back.
 // Every wait on an mbarrier is bounded; on expiry the CTA records an error,
 // waits (bounded) for its own copy and MMAs, frees its tensor memory and stops.
+#include <algorithm>
 #include <cstdio>
 
 #include "common.hpp"
@@ -26,17 +30,21 @@ constexpr int kThreads = 256;
 constexpr uint32_t kTmemCols = 64;
 constexpr uint32_t kXBytes = 32768;      // one operand copy of the tile (4096 complex64)
 constexpr uint32_t kUBytes = 32768;      // U_hi + U_lo images
+constexpr uint32_t kDescBytes = 320;     // next_b[32] + next_c[128] (u16) of one block
 constexpr uint32_t kOffX0 = 0, kOffX1 = kXBytes, kOffU = 2 * kXBytes;
 constexpr uint32_t kOffTabs = kOffU + kUBytes;           // lo_tab[64], hi_tab[64] (u64)
-constexpr uint32_t kOffDesc = kOffTabs + 128 * 8;        // next_b[32], next_c[128] (u16)
-constexpr uint32_t kOffBar = kOffDesc + 160 * 2 + 16;    // two mbarriers, 8-byte aligned
+constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
+constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // two block-table buffers
+constexpr uint32_t kOffBar = kOffDesc + 2 * kDescBytes;  // two mbarriers, 8-byte aligned
 constexpr uint32_t kSmemBytes = kOffBar + 64;
 constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
 constexpr long long kWaitCycles = 4000000000LL;          // ... or this many SM cycles
+static_assert(kOffDesc % 16 == 0 && kDescBytes % 16 == 0, "bulk copies need 16-byte alignment");
+static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
 
 struct FusedQubits {
     int q[kFusedM];
-    uint16_t in_lo[64], in_hi[64];
+    uint16_t io[4][64];  // in_lo, in_hi, out_lo, out_hi
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -45,13 +53,26 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 
 // K-major, no-swizzle shared-memory matrix descriptor (sm_100 format, version 1):
 // leading byte offset 128 (the two 16-byte K chunks of one MMA), stride byte
-// offset 2048 (consecutive 8-row core-matrix groups).
+// offset 2048 (consecutive 8-row core-matrix groups).  Used for the gate image.
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
     uint64_t d = 0;
     d |= uint64_t((saddr & 0x3FFFFu) >> 4);
     d |= uint64_t(128u >> 4) << 16;
     d |= uint64_t(2048u >> 4) << 32;
     d |= uint64_t(1) << 46;
+    return d;
+}
+
+// K-major, 128-byte-swizzled descriptor (layout type 2): 8-row x 128-byte
+// atoms, 1024 bytes between 8-row groups; the leading offset is unused.  The
+// start address steps 32 bytes per K = 8 slice inside an atom.  Used for the tile.
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr & 0x3FFFFu) >> 4);
+    d |= uint64_t(1) << 16;
+    d |= uint64_t(1024u >> 4) << 32;
+    d |= uint64_t(1) << 46;
+    d |= uint64_t(2) << 61;
     return d;
 }
 
@@ -84,21 +105,33 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
 __device__ __forceinline__ float tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
 }
 
-// Byte offset of complex amplitude (column, basis) in the A operand layout.
-__device__ __forceinline__ uint32_t a_off(uint32_t col, uint32_t basis) {
-    return (col >> 3) * 2048u + (basis >> 1) * 128u + (col & 7u) * 16u + (basis & 1u) * 8u;
-}
-
+// TF32 hi part rounded to nearest; the lo remainder is left for the tensor
+// core to truncate (its error is below 2^-22 of the value).
 __device__ __forceinline__ void put_split(unsigned char* sm, uint32_t off, float re, float im) {
     const float hr = tf32(re), hi = tf32(im);
     *reinterpret_cast<float2*>(sm + kOffX0 + off) = make_float2(hr, hi);
-    *reinterpret_cast<float2*>(sm + kOffX1 + off) = make_float2(tf32(re - hr), tf32(im - hi));
+    *reinterpret_cast<float2*>(sm + kOffX1 + off) = make_float2(re - hr, im - hi);
+}
+
+// Gate image and layout tables of one block, one transaction count on bar.
+__device__ __forceinline__ void fetch_block(unsigned char* sm, const FusedBlock* blk, const float* upool, uint32_t buf,
+                                            uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kUBytes + kDescBytes)
+                 : "memory");
+    bulk_g2s(smem_addr(sm + kOffU), upool + blk->u_off, kUBytes, bar);
+    bulk_g2s(smem_addr(sm + kOffDesc + buf * kDescBytes), blk->next_b, kDescBytes, bar);
 }
 
 __global__ void __launch_bounds__(kThreads, 2)
@@ -111,24 +144,26 @@ __global__ void __launch_bounds__(kThreads, 2)
     __shared__ double s_wsum[kThreads / 32];
     uint64_t* lo_tab = reinterpret_cast<uint64_t*>(sm + kOffTabs);
     uint64_t* hi_tab = lo_tab + 64;
-    uint16_t* nb = reinterpret_cast<uint16_t*>(sm + kOffDesc);
-    uint16_t* nc = nb + 32;
+    uint16_t* io = reinterpret_cast<uint16_t*>(sm + kOffIO);  // in_lo | in_hi | out_lo | out_hi
     const uint32_t bar_u = smem_addr(sm + kOffBar), bar_m = bar_u + 8;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    for (int e = tid; e < 64; e += kThreads) {
+    if (tid < 64) {
         uint64_t a = 0, b = 0;
         for (int t = 0; t < 6; t++) {
-            if ((e >> t) & 1) {
+            if ((tid >> t) & 1) {
                 a |= uint64_t(1) << fq.q[t];
                 b |= uint64_t(1) << fq.q[6 + t];
             }
         }
-        lo_tab[e] = a;
-        hi_tab[e] = b;
+        lo_tab[tid] = a;
+        hi_tab[tid] = b;
     }
+    io[tid] = fq.io[tid >> 6][tid & 63];
     if (tid == 0) {
-        s_abort = 0;
+        // The swizzled operand needs 1024-byte aligned atoms.
+        s_abort = (smem_addr(sm) & 1023u) != 0;
+        if (s_abort) atomicExch(err, 3);
         mbar_init(bar_u, 1);
         mbar_init(bar_m, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -142,10 +177,18 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
+    const uint64_t desc_x0 = make_desc_sw128(smem_addr(sm + kOffX0)), desc_x1 = make_desc_sw128(smem_addr(sm + kOffX1));
+    const uint64_t desc_u0 = make_desc(smem_addr(sm + kOffU)), desc_u1 = make_desc(smem_addr(sm + kOffU) + 16384u);
     uint32_t phase_u = 0, phase_m = 0;
     uint32_t pending_u = 0, pending_m = 0;  // issued and not yet awaited (thread 0)
+    uint32_t seq = 0;                       // blocks processed: selects the table buffer
+    if (tid == 0 && uint64_t(blockIdx.x) < total_tiles) {
+        fetch_block(sm, blocks, upool, 0, bar_u);
+        pending_u = 1;
+    }
 
     const int rest = n - kFusedM;
+    const uint32_t row = uint32_t(tid >> 6);  // this thread's elements: l = (tid & 63) | (row + 4k) << 6
     for (uint64_t t = blockIdx.x; t < total_tiles && !s_abort; t += gridDim.x) {
         const uint64_t st = t >> rest;
         uint64_t tidx = t & ((uint64_t(1) << rest) - 1);
@@ -157,28 +200,20 @@ __global__ void __launch_bounds__(kThreads, 2)
         // FP64 renormalisation of the previous pass (tensor-core accumulation
         // rounds toward zero, so unitary blocks shrink the norm slightly).
         const double scale = in_norm ? 1.0 / sqrt(in_norm[st]) : 1.0;
-        // Tile -> A operand of block 0, split into TF32 hi / lo.
-        for (uint32_t e = tid; e < 4096u; e += kThreads) {
-            float2 v = g[lo_tab[e & 63] | hi_tab[e >> 6]];
-            uint32_t p = uint32_t(fq.in_lo[e & 63]) | uint32_t(fq.in_hi[e >> 6]);
-            put_split(sm, a_off(p >> 5, p & 31), float(double(v.x) * scale), float(double(v.y) * scale));
+        const uint64_t glo = lo_tab[tid & 63];
+        {
+            // Tile -> A operand of block 0, split into TF32 hi / lo (loads first, all in flight).
+            float2 v[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = __ldcs(g + (glo | hi_tab[row + 4 * k]));
+            const uint32_t plo = io[tid & 63];
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+                put_split(sm, plo ^ io[64 + row + 4 * k], float(double(v[k].x) * scale), float(double(v[k].y) * scale));
         }
         double norm_acc = 0.0;
         for (int j = 0; j < nblocks; j++) {
-            const FusedBlock& blk = blocks[j];
-            if (tid == 0) {
-                // U image of this block (the previous block's MMAs are complete).
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_u), "r"(kUBytes)
-                             : "memory");
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        smem_addr(sm + kOffU)),
-                    "l"(upool + blk.u_off), "r"(kUBytes), "r"(bar_u)
-                    : "memory");
-                pending_u = 1;
-            }
-            if (tid < 32) nb[tid] = blk.next_b[tid];
-            if (tid < 128) nc[tid] = blk.next_c[tid];
+            const uint32_t buf = seq & 1u;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (tid == 0) {
@@ -190,20 +225,17 @@ __global__ void __launch_bounds__(kThreads, 2)
                     atomicExch(err, 3);
                 } else {
                     asm volatile("tcgen05.fence::after_thread_sync;");
-                    const uint32_t ax0 = smem_addr(sm + kOffX0), ax1 = smem_addr(sm + kOffX1);
-                    const uint32_t bu0 = smem_addr(sm + kOffU), bu1 = bu0 + 16384u;
-#pragma unroll 1
+                    // Descriptors advance by (byte offset >> 4) in their start-address field.
+#pragma unroll
                     for (int q = 0; q < 24; q++) {
                         const int part = q >> 3, ks = q & 7;
-                        const uint32_t a = (part == 2 ? ax1 : ax0) + uint32_t(ks) * 256u;
-                        const uint32_t bb = (part == 1 ? bu1 : bu0) + uint32_t(ks) * 256u;
-                        const uint64_t ad = make_desc(a), bd = make_desc(bb);
-                        const uint32_t acc = q > 0 ? 1u : 0u;
+                        const uint64_t ad = (part == 2 ? desc_x1 : desc_x0) + uint64_t((ks >> 2) * 1024 + (ks & 3) * 2);
+                        const uint64_t bd = (part == 1 ? desc_u1 : desc_u0) + uint64_t(ks * 16);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
                             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                            "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+                            "l"(ad), "l"(bd), "r"(kIdesc), "r"(q > 0 ? 1u : 0u));
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                         bar_m)
@@ -215,6 +247,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                     if (!ok) {
                         s_abort = 1;
                         atomicExch(err, 3);
+                    } else {
+                        // The gate image is free again: fetch the next block's while this one is read back.
+                        const int next = j + 1 < nblocks ? j + 1 : (t + gridDim.x < total_tiles ? 0 : -1);
+                        if (next >= 0) {
+                            fetch_block(sm, blocks + next, upool, buf ^ 1u, bar_u);
+                            pending_u = 1;
+                        }
                     }
                 }
             }
@@ -223,6 +262,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             asm volatile("tcgen05.fence::after_thread_sync;");
             // Readback: warp w reads TMEM lanes 32*(w%4).. (tile columns) and
             // output columns 32*(w/4).. (16 complex outputs per thread).
+            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + buf * kDescBytes);
+            const uint16_t* nc = nb + 32;
             const uint32_t col = uint32_t((warp & 3) * 32 + lane);
             const uint32_t half = uint32_t(warp >> 2);
             uint32_t r[32];
@@ -238,28 +279,37 @@ __global__ void __launch_bounds__(kThreads, 2)
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             const uint32_t cpart = nc[col];
-            if (!blk.last) {
+            uint32_t nbw[8];  // this half's 16 destination parts, two per word
+            {
+                const uint4 w0 = *reinterpret_cast<const uint4*>(nb + half * 16);
+                const uint4 w1 = *reinterpret_cast<const uint4*>(nb + half * 16 + 8);
+                nbw[0] = w0.x, nbw[1] = w0.y, nbw[2] = w0.z, nbw[3] = w0.w;
+                nbw[4] = w1.x, nbw[5] = w1.y, nbw[6] = w1.z, nbw[7] = w1.w;
+            }
+            if (j + 1 < nblocks) {
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
-                    const uint32_t p = cpart | nb[half * 16 + i];
-                    put_split(sm, a_off(p >> 5, p & 31), __uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+                    const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
+                    put_split(sm, off, __uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
                 }
             } else {
-                float2* stage = reinterpret_cast<float2*>(sm + kOffX0);
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
-                    const uint32_t l = cpart | nb[half * 16 + i];
+                    const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
                     const float re = __uint_as_float(r[2 * i]), im = __uint_as_float(r[2 * i + 1]);
-                    stage[l] = make_float2(re, im);
+                    *reinterpret_cast<float2*>(sm + kOffX0 + off) = make_float2(re, im);
                     norm_acc += double(re) * re + double(im) * im;
                 }
             }
+            seq++;
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();
         }
         if (s_abort) break;
-        const float2* stage = reinterpret_cast<const float2*>(sm + kOffX0);
-        for (uint32_t e = tid; e < 4096u; e += kThreads) g[lo_tab[e & 63] | hi_tab[e >> 6]] = stage[e];
+        const uint32_t olo = io[128 + (tid & 63)];
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            g[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(sm + kOffX0 + (olo ^ io[192 + row + 4 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) s_wsum[warp] = norm_acc;
@@ -271,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         __syncthreads();
     }
-    // On an aborted wait, give the copy and the MMAs in flight a bounded chance to land.
+    // On an aborted wait, give the copies and the MMAs in flight a bounded chance to land.
     if (tid == 0) {
         if (pending_u) mbar_wait(bar_u, phase_u & 1);
         if (pending_m) mbar_wait(bar_m, phase_m & 1);
@@ -339,18 +389,35 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     FusedQubits fq;
     for (int i = 0; i < kFusedM; i++) fq.q[i] = p.qubits[i];
     for (int e = 0; e < 64; e++) {
-        fq.in_lo[e] = p.in_lo[e];
-        fq.in_hi[e] = p.in_hi[e];
+        fq.io[0][e] = p.in_lo[e];
+        fq.io[1][e] = p.in_hi[e];
+        fq.io[2][e] = p.out_lo[e];
+        fq.io[3][e] = p.out_hi[e];
     }
-    static bool configured = false;
-    if (!configured) {
+    // Two CTAs per SM need the largest shared-memory carveout.  Residency is
+    // computed from the kernel's registers and shared memory (the grid-stride
+    // loop is correct for any grid; a grid below residency leaves SMs half idle).
+    static int per_sm_of[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& per_sm = per_sm_of[dev & 63];
+    if (per_sm == 0) {
         cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
-        if (e != cudaSuccess) fail(kCudaError, std::string("fused pass smem: ") + cudaGetErrorString(e));
-        configured = true;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fused, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     int(cudaSharedmemCarveoutMaxShared));
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_fused);
+        int smem_sm = 0, reserved = 0, regs_sm = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        if (e != cudaSuccess) fail(kCudaError, std::string("fused pass setup: ") + cudaGetErrorString(e));
+        const size_t per_cta = kSmemBytes + fa.sharedSizeBytes + size_t(reserved);
+        const int by_smem = int(size_t(smem_sm) / per_cta);
+        const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kThreads) : 2;
+        per_sm = std::max(1, std::min({2, by_smem, by_regs}));
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused, kThreads, kSmemBytes);
-    if (per_sm < 1) per_sm = 1;
     const uint64_t total = b.W << (b.n - kFusedM);
     const uint64_t grid = std::min<uint64_t>(total, uint64_t(sm_count()) * uint64_t(per_sm));
     k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq,

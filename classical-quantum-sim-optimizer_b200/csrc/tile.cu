@@ -206,6 +206,16 @@ float tf32_rna(float v) {
     return r;
 }
 
+}  // namespace
+
+uint32_t fused_operand_offset(uint32_t packed) {
+    const uint32_t col = packed >> 5, basis = packed & 31u;
+    return (basis >> 4) * 16384u + (col >> 3) * 1024u + (col & 7u) * 128u + ((((basis >> 1) & 7u) ^ (col & 7u)) << 4) +
+           (basis & 1u) * 8u;
+}
+
+namespace {
+
 // Float offset of (row, k) in the canonical K-major, no-swizzle operand layout
 // with 64 K-elements per row: 8-row x 16-byte core matrices, the K chunks of a
 // row group 128 B apart, row groups 2048 B apart.
@@ -254,12 +264,6 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         blk.push_back(std::move(b));
     }
     // Layout of block j: packed = (pext(l, other_j) << 5) | basis_j(l), basis MSB = q[0].
-    auto others = [&](const Blk& b) {
-        std::vector<int> o;
-        for (int i = 0; i < m; i++)
-            if (std::find(b.q, b.q + 5, i) == b.q + 5) o.push_back(i);
-        return o;
-    };
     auto layout = [&](const Blk& b, const std::vector<int>& oth, uint32_t l) {
         uint32_t basis = 0, col = 0;
         for (int t = 0; t < 5; t++) basis = (basis << 1) | ((l >> b.q[t]) & 1u);
@@ -276,11 +280,137 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         for (size_t t = 0; t < oth.size(); t++) l |= ((col >> t) & 1u) << oth[t];
         return l;
     };
-    std::vector<std::vector<int>> oth(blk.size());
-    for (size_t j = 0; j < blk.size(); j++) oth[j] = others(blk[j]);
+    // Bank-aware layouts.  The operand is stored 128-byte swizzled, so the
+    // bank slot of an 8-byte store (one of 16) has bits (b0, b1^c0, b2^c1,
+    // b3^c2) of the block's basis (b) and column (c) index.  Shared memory
+    // serves a warp's 8-byte stores one half-warp at a time, and across a
+    // half-warp the readback of block j-1 varies the four qubits of its column
+    // bits 0..3 (its TMEM lanes; local qubits 0..3 for the tile load).  Block
+    // j's basis and column bit order is chosen greedily so that those four
+    // qubits reach four independent slot bits (one wavefront per half-warp):
+    // one lane qubit of the block at basis bit 0, lane qubits outside it at
+    // column bits 0..2, the rest at the remaining basis bits 1..3.  Free
+    // column bits 0..3 then take a qubit of block j+1 first, so that the next
+    // readback also has a lane qubit there.
+    const size_t J = blk.size();
+    std::vector<std::vector<int>> oth(J);
+    uint32_t lanes = 0xFu;  // qubits varying across a half-warp of the incoming stores
+    for (size_t j = 0; j < J; j++) {
+        Blk& bj = blk[j];
+        uint32_t bmask = 0, nmask = 0;
+        for (int t = 0; t < 5; t++) bmask |= 1u << bj.q[t];
+        if (j + 1 < J)
+            for (int t = 0; t < 5; t++) nmask |= 1u << blk[j + 1].q[t];
+        int bpos[5] = {-1, -1, -1, -1, -1};  // qubit at basis bit k
+        int cpos[7] = {-1, -1, -1, -1, -1, -1, -1};
+        uint32_t used = 0;
+        std::vector<int> lb, lc;
+        for (int i = 0; i < m; i++)
+            if ((lanes >> i) & 1u) ((bmask >> i) & 1u ? lb : lc).push_back(i);
+        uint32_t slots = 0;  // slot bits already reached (bit k: slot bit k)
+        if (!lb.empty()) {
+            bpos[0] = lb[0];
+            used |= 1u << lb[0];
+            slots |= 1u;
+        }
+        for (size_t t = 0; t < lc.size() && t < 3; t++) {
+            cpos[t] = lc[t];
+            used |= 1u << lc[t];
+            slots |= 2u << t;
+        }
+        if (lc.size() > 3) {
+            cpos[3] = lc[3];
+            used |= 1u << lc[3];
+        }
+        for (size_t t = 1; t < lb.size(); t++)
+            for (int k = 1; k < 4; k++)
+                if (bpos[k] < 0 && !((slots >> k) & 1u)) {
+                    bpos[k] = lb[t];
+                    used |= 1u << lb[t];
+                    slots |= 1u << k;
+                    break;
+                }
+        for (size_t t = 1; t < lb.size(); t++)  // lane qubits of the block that reached no new slot
+            if (!((used >> lb[t]) & 1u))
+                for (int k = 1; k < 5; k++)
+                    if (bpos[k] < 0) {
+                        bpos[k] = lb[t];
+                        used |= 1u << lb[t];
+                        break;
+                    }
+        for (int t = 0; t < 5; t++)
+            if (!((used >> bj.q[t]) & 1u))
+                for (int k = 0; k < 5; k++)
+                    if (bpos[k] < 0) {
+                        bpos[k] = bj.q[t];
+                        used |= 1u << bj.q[t];
+                        break;
+                    }
+        // Column bits: lane qubits placed above; then one qubit of the next
+        // block among bits 0..3 (if none is there yet), then the rest ascending.
+        bool next_lane = false;
+        for (int k = 0; k < 4; k++)
+            if (cpos[k] >= 0 && ((nmask >> cpos[k]) & 1u)) next_lane = true;
+        std::vector<int> rest;
+        for (int i = 0; i < m; i++)
+            if (!((bmask >> i) & 1u) && !((used >> i) & 1u)) rest.push_back(i);
+        if (!next_lane)
+            std::stable_sort(rest.begin(), rest.end(),
+                             [&](int x, int y) { return ((nmask >> x) & 1u) > ((nmask >> y) & 1u); });
+        size_t ri = 0;
+        for (int k = 0; k < 7; k++)
+            if (cpos[k] < 0) cpos[k] = rest[ri++];
+        // Basis order q[t] = qubit at basis bit 4-t; permute the matrix to match.
+        int old_bit[12];
+        for (int t = 0; t < 5; t++) old_bit[bj.q[t]] = 4 - t;
+        int perm[5];  // new basis bit k <- old basis bit perm[k]
+        for (int k = 0; k < 5; k++) perm[k] = old_bit[bpos[k]];
+        auto old_index = [&](int x) {
+            int o = 0;
+            for (int k = 0; k < 5; k++) o |= ((x >> k) & 1) << perm[k];
+            return o;
+        };
+        std::vector<cplx> nu(32 * 32);
+        for (int r = 0; r < 32; r++)
+            for (int c = 0; c < 32; c++) nu[size_t(r) * 32 + c] = bj.u[size_t(old_index(r)) * 32 + old_index(c)];
+        bj.u = std::move(nu);
+        for (int t = 0; t < 5; t++) bj.q[t] = bpos[4 - t];
+        oth[j].assign(cpos, cpos + 7);
+        lanes = 0;
+        for (int k = 0; k < 4; k++) lanes |= 1u << cpos[k];
+    }
+    // Stage after the last block: natural index l lives at slot s(l) = l ^ h(l),
+    // h copying lane qubits above bit 3 onto the bank bits 0..3 that the last
+    // block's lanes leave constant (s is linear and invertible; a warp reading
+    // consecutive l still covers every bank).
+    uint32_t hsrc[4] = {0, 0, 0, 0}, hdst[4] = {0, 0, 0, 0};
+    int hn = 0;
+    {
+        std::vector<uint32_t> free_bits, high;
+        for (uint32_t b = 0; b < 4; b++)
+            if (!((lanes >> b) & 1u)) free_bits.push_back(b);
+        for (uint32_t b = 4; b < 12; b++)
+            if ((lanes >> b) & 1u) high.push_back(b);
+        for (; hn < int(std::min(free_bits.size(), high.size())); hn++) {
+            hsrc[hn] = high[size_t(hn)];
+            hdst[hn] = free_bits[size_t(hn)];
+        }
+    }
+    // Tables hold shared-memory byte offsets.  Both maps below are linear over
+    // GF(2) in the local index, so parts of an index combine by XOR.
+    auto stage_off = [&](uint32_t l) {
+        uint32_t s = l;
+        for (int i = 0; i < hn; i++) s ^= ((l >> hsrc[i]) & 1u) << hdst[i];
+        return uint16_t(s * 8u);
+    };
+    auto operand_off = [&](const Blk& b, const std::vector<int>& oth, uint32_t l) {
+        return uint16_t(fused_operand_offset(layout(b, oth, l)));
+    };
     for (int e = 0; e < 64; e++) {
-        fp.in_lo[e] = layout(blk[0], oth[0], uint32_t(e));
-        fp.in_hi[e] = layout(blk[0], oth[0], uint32_t(e) << 6);
+        fp.in_lo[e] = operand_off(blk[0], oth[0], uint32_t(e));
+        fp.in_hi[e] = operand_off(blk[0], oth[0], uint32_t(e) << 6);
+        fp.out_lo[e] = stage_off(uint32_t(e));
+        fp.out_hi[e] = stage_off(uint32_t(e) << 6);
     }
     for (size_t j = 0; j < blk.size(); j++) {
         FusedBlock d;
@@ -289,11 +419,11 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         d.last = j + 1 == blk.size() ? 1u : 0u;
         for (uint32_t bb = 0; bb < 32; bb++) {
             uint32_t l = dep_basis(blk[j], bb);
-            d.next_b[bb] = d.last ? uint16_t(l) : layout(blk[j + 1], oth[j + 1], l);
+            d.next_b[bb] = d.last ? stage_off(l) : operand_off(blk[j + 1], oth[j + 1], l);
         }
         for (uint32_t c = 0; c < uint32_t(kFusedCols); c++) {
             uint32_t l = dep_col(oth[j], c);
-            d.next_c[c] = d.last ? uint16_t(l) : layout(blk[j + 1], oth[j + 1], l);
+            d.next_c[c] = d.last ? stage_off(l) : operand_off(blk[j + 1], oth[j + 1], l);
         }
         // Real 64x64 form [[Re, -Im], [Im, Re]] with rows 2b'+ri' and columns 2b+ri,
         // stored as the B operand (N = 64 output rows, K = 64 inputs, K-major).
@@ -853,6 +983,9 @@ void tile_pass_t(const Batch& b, int m, const TileOp* ops, int nops, const doubl
     size_t& conf = configured[sizeof(V) == 8 ? 1 : 0][TIMED ? 1 : 0];
     if (smem > conf) {
         cudaFuncSetAttribute(k_tile<V, TIMED>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        // Largest carveout, so the occupancy below is what the launch gets.
+        cudaFuncSetAttribute(k_tile<V, TIMED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxShared));
         conf = smem;
     }
     const uint64_t total = b.W << (b.n - m);

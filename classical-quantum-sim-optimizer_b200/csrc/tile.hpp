@@ -85,19 +85,26 @@ constexpr int kFusedM = 12;            // tile qubits of a fused pass
 constexpr int kFusedCols = 1 << (kFusedM - 5);
 constexpr int kFusedUFloats = 2 * 64 * 64;  // U_hi and U_lo images of one block
 
-// Device descriptor of one block.  Packed tile positions are (column << 5) | basis.
+// Byte offset in a block's tile operand (128-byte swizzled, K-major; K element
+// 2*basis + re/im) of packed position (column << 5) | basis.  Linear over GF(2).
+uint32_t fused_operand_offset(uint32_t packed);
+
+// Device descriptor of one block.  An output at (column, basis) of this block
+// goes to byte offset next_c[column] ^ next_b[basis]: in the next block's tile
+// operand, or after the last block in the swizzled natural-order stage.
 struct alignas(16) FusedBlock {
     uint32_t u_off;          // float offset of the block's U_hi/U_lo image in the pool
-    uint32_t last;           // 1: outputs go to natural tile order
+    uint32_t last;           // 1: outputs go to the stage
     uint32_t pad[2];
-    uint16_t next_b[32];     // output basis -> packed position for the next block (or natural index)
-    uint16_t next_c[128];    // output column -> packed position part
+    uint16_t next_b[32];     // output basis -> destination offset part
+    uint16_t next_c[128];    // output column -> destination offset part
 };
 
 struct FusedPass {
     std::vector<int> qubits;   // 12 ascending global positions
     int first_block = 0, nblocks = 0;
-    uint16_t in_lo[64], in_hi[64];  // natural local index -> packed position of block 0
+    uint16_t in_lo[64], in_hi[64];    // natural local index l -> operand offset of block 0 (lo ^ hi)
+    uint16_t out_lo[64], out_hi[64];  // natural local index l -> stage offset (lo ^ hi)
     int raw_ops = 0;
 };
 

@@ -42,6 +42,17 @@ def block_matrix(upool, off):
     return real[0::2, 0::2] + 1j * real[1::2, 0::2]
 
 
+def operand_offset(packed):
+    """Byte offset of packed (column << 5) | basis in the 128-byte swizzled tile operand."""
+    col, basis = packed >> 5, packed & 31
+    return ((basis >> 4) * 16384 + (col >> 3) * 1024 + (col & 7) * 128 + ((((basis >> 1) & 7) ^ (col & 7)) << 4)
+            + (basis & 1) * 8)
+
+
+PACKED = np.arange(4096)
+SLOT_OF_PACKED = operand_offset(PACKED) // 8  # operand slot holding packed position p
+
+
 def emulate(plan):
     n = plan["n"]
     upool = np.asarray(plan["upool"], dtype=np.float32)
@@ -53,20 +64,19 @@ def emulate(plan):
         other = [q for q in range(n) if q not in T]
         idx = deposit(np.arange(1 << (n - 12)), other)[:, None] | deposit(local, T)[None, :]
         tiles = state[idx]
-        packed = np.asarray(p["in_lo"])[local & 63] | np.asarray(p["in_hi"])[local >> 6]
-        X = np.zeros((tiles.shape[0], 128, 32), dtype=np.complex128)
-        X[:, packed >> 5, packed & 31] = tiles
+        # shared memory as 4096 eight-byte slots; tables hold byte offsets combined by XOR
+        off = np.asarray(p["in_lo"])[local & 63] ^ np.asarray(p["in_hi"])[local >> 6]
+        slots = np.zeros_like(tiles)
+        slots[:, off // 8] = tiles
         for blk in p["blocks"]:
+            X = slots[:, SLOT_OF_PACKED].reshape(-1, 128, 32)
             U = block_matrix(upool, blk["u_off"])
             Y = X @ U.T
-            P = np.asarray(blk["next_c"])[:, None] | np.asarray(blk["next_b"])[None, :]
-            if blk["last"]:
-                out = np.zeros_like(tiles)
-                out[:, P] = Y
-                tiles = out
-            else:
-                X = np.zeros_like(X)
-                X[:, P >> 5, P & 31] = Y
+            off = np.asarray(blk["next_c"])[:, None] ^ np.asarray(blk["next_b"])[None, :]
+            slots = np.zeros_like(tiles)
+            slots[:, off // 8] = Y
+        out = np.asarray(p["out_lo"])[local & 63] ^ np.asarray(p["out_hi"])[local >> 6]
+        tiles = slots[:, out // 8]
         state[idx] = tiles
     return state
 
