@@ -1,22 +1,31 @@
 // Fused 5-qubit blocks as tcgen05 tensor-core contractions (complex64 state).
 //
-// A CTA owns one 2^12-amplitude tile at a time.  For block j (a 32x32 complex
-// matrix U on 5 tile qubits) the tile is held in shared memory as the A
-// operand of D = A * B: 128 rows (the tile's 128 "columns", i.e. values of the
-// other 7 tile qubits) by K = 64 real inputs (re/im of the 32 basis states),
-// split into TF32 hi and lo parts.  B is the block's real 64x64 form of U
-// (hi and lo), brought in by one cp.async.bulk (TMA) copy per block.  One
-// thread issues 24 tcgen05.mma.kind::tf32 instructions (M=128, N=64, K=8):
-// A_hi*B_hi + A_hi*B_lo + A_lo*B_hi accumulate into a 128 x 64 FP32 tile in
-// tensor memory.  The readback (tcgen05.ld, one TMEM lane per tile column)
-// writes every output amplitude straight into the layout the next block needs
-// (128-byte swizzled, bit orders chosen on the host to spread each half-warp's
-// stores over all banks), or, after the last block, into a swizzled
-// natural-order stage for the store to HBM.  The next block's gate image and
-// layout tables are fetched while the current block is read back.
-// Every wait on an mbarrier is bounded; on expiry the CTA records an error,
-// waits (bounded) for its own copy and MMAs, frees its tensor memory and stops.
+// A tile is 2^12 amplitudes.  For block j (a 32x32 complex matrix U on 5 tile
+// qubits) the tile is held in shared memory as the A operand of D = A * B: 128
+// rows (the tile's 128 "columns", i.e. values of the other 7 tile qubits) by
+// K = 64 real inputs (re/im of the 32 basis states), split into TF32 hi and lo
+// parts.  B is the block's real 64x64 form of U (hi and lo), brought in by a
+// cp.async.bulk (TMA) copy.  24 tcgen05.mma.kind::tf32 instructions (M=128,
+// N=64, K=8) accumulate A_hi*B_hi + A_hi*B_lo + A_lo*B_hi into a 128 x 64 FP32
+// tile in tensor memory.  The readback (tcgen05.ld, one TMEM lane per tile
+// column) writes every output amplitude straight into the layout the next
+// block needs (128-byte swizzled, bit orders chosen on the host to spread each
+// half-warp's stores over all banks), or, after the last block, into a
+// swizzled natural-order stage for the store to HBM.
+//
+// One CTA per SM, persistent over pairs of tiles, with two groups of 8 warps.
+// Group g owns tile 2*pair + g, one 64-column TMEM accumulator and its own
+// operand buffers; one thread of the group issues its MMAs, so one tile's
+// MMAs run while the other tile is read back.  The two tiles walk the same
+// block sequence and share the gate images (two buffers, fetched two blocks
+// ahead by whichever group finishes its MMAs on a buffer last).  Hand-offs
+// are mbarriers (copies, MMA completion) and per-group named barriers; every
+// mbarrier wait is bounded, and a group stops only by a group-wide vote, so
+// no thread is left waiting on a named barrier.  On expiry the CTA records an
+// error, waits (bounded) for its own copies and MMAs, frees its tensor memory
+// and stops.
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 
 #include "common.hpp"
@@ -26,21 +35,31 @@ namespace dq {
 namespace k {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr uint32_t kTmemCols = 64;
-constexpr uint32_t kXBytes = 32768;      // one operand copy of the tile (4096 complex64)
-constexpr uint32_t kUBytes = 32768;      // U_hi + U_lo images
-constexpr uint32_t kDescBytes = 320;     // next_b[32] + next_c[128] (u16) of one block
-constexpr uint32_t kOffX0 = 0, kOffX1 = kXBytes, kOffU = 2 * kXBytes;
-constexpr uint32_t kOffTabs = kOffU + kUBytes;           // lo_tab[64], hi_tab[64] (u64)
-constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
-constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // two block-table buffers
-constexpr uint32_t kOffBar = kOffDesc + 2 * kDescBytes;  // two mbarriers, 8-byte aligned
-constexpr uint32_t kSmemBytes = kOffBar + 64;
-constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
-constexpr long long kWaitCycles = 4000000000LL;          // ... or this many SM cycles
+constexpr int kGroupThreads = 256;                        // one readback group (8 warps)
+constexpr int kThreads = 2 * kGroupThreads;               // two groups
+constexpr uint32_t kTmemCols = 128;                       // one 64-column accumulator per group
+constexpr uint32_t kXBytes = 32768;                       // one operand copy of a tile (4096 complex64)
+constexpr uint32_t kUBytes = 32768;                       // U_hi + U_lo images of one block
+constexpr uint32_t kDescBytes = 320;                      // next_b[32] + next_c[128] (u16) of one block
+constexpr uint32_t kOffU = 4 * kXBytes;                   // group g: X_hi at g*64K, X_lo at g*64K + 32K
+constexpr uint32_t kOffTabs = kOffU + 2 * kUBytes;        // lo_tab[64], hi_tab[64] (u64)
+constexpr uint32_t kOffIO = kOffTabs + 128 * 8;           // in_lo, in_hi, out_lo, out_hi [64] (u16)
+constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;        // three block-table buffers
+constexpr uint32_t kOffBar = kOffDesc + 3 * kDescBytes;   // mbarriers, 8-byte aligned
+constexpr uint32_t kOffWsum = kOffBar + 16 * 8;           // per-group warp sums (double)
+constexpr uint32_t kSmemBytes = kOffWsum + 2 * 8 * 8;
+constexpr uint64_t kSpinLimit = uint64_t(1) << 26;        // polls of an mbarrier before giving up
+constexpr long long kWaitCycles = 4000000000LL;           // ... or this many SM cycles
 static_assert(kOffDesc % 16 == 0 && kDescBytes % 16 == 0, "bulk copies need 16-byte alignment");
+static_assert(kOffBar % 8 == 0 && kOffWsum % 8 == 0, "mbarrier alignment");
 static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
+
+// mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
+constexpr uint32_t kBarUFull = 0;  // [2] gate image of buffer b landed (expect_tx)
+constexpr uint32_t kBarTFull = 2;  // [3] block tables of buffer b landed (expect_tx)
+constexpr uint32_t kBarMma = 5;    // [2] MMAs of group g's tile complete (tcgen05.commit)
+constexpr uint32_t kBarDrain = 7;  // [2] group g's MMAs in flight complete (abort path)
+constexpr uint32_t kNumBars = 9;
 
 struct FusedQubits {
     int q[kFusedM];
@@ -105,10 +124,37 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(bar)
                  : "memory");
+}
+
+// Barrier over one readback group (named barrier 1 + g, 256 threads).
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory");
+}
+
+// Barrier over one readback group that also ANDs a predicate across it.
+__device__ __forceinline__ bool group_all(bool v, int g) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(uint32_t(v)), "r"(1 + g), "r"(kGroupThreads)
+        : "memory");
+    return r != 0;
 }
 
 __device__ __forceinline__ float tf32(float x) {
@@ -119,34 +165,43 @@ __device__ __forceinline__ float tf32(float x) {
 
 // TF32 hi part rounded to nearest; the lo remainder is left for the tensor
 // core to truncate (its error is below 2^-22 of the value).
-__device__ __forceinline__ void put_split(unsigned char* sm, uint32_t off, float re, float im) {
+__device__ __forceinline__ void put_split(unsigned char* x, uint32_t off, float re, float im) {
     const float hr = tf32(re), hi = tf32(im);
-    *reinterpret_cast<float2*>(sm + kOffX0 + off) = make_float2(hr, hi);
-    *reinterpret_cast<float2*>(sm + kOffX1 + off) = make_float2(re - hr, im - hi);
+    *reinterpret_cast<float2*>(x + off) = make_float2(hr, hi);
+    *reinterpret_cast<float2*>(x + kXBytes + off) = make_float2(re - hr, im - hi);
 }
 
-// Gate image and layout tables of one block, one transaction count on bar.
-__device__ __forceinline__ void fetch_block(unsigned char* sm, const FusedBlock* blk, const float* upool, uint32_t buf,
-                                            uint32_t bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kUBytes + kDescBytes)
-                 : "memory");
-    bulk_g2s(smem_addr(sm + kOffU), upool + blk->u_off, kUBytes, bar);
-    bulk_g2s(smem_addr(sm + kOffDesc + buf * kDescBytes), blk->next_b, kDescBytes, bar);
-}
-
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 1)
     k_fused(float2* __restrict__ s, int n, FusedQubits fq, const FusedBlock* __restrict__ blocks, int nblocks,
             const float* __restrict__ upool, uint64_t total_tiles, int* __restrict__ err,
             const double* __restrict__ in_norm, double* __restrict__ tile_norm) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
-    __shared__ double s_wsum[kThreads / 32];
+    __shared__ unsigned s_ucnt[2];          // per gate-image buffer: groups whose MMAs on it completed
+    __shared__ unsigned long long s_fetched;  // steps whose copies were issued
     uint64_t* lo_tab = reinterpret_cast<uint64_t*>(sm + kOffTabs);
     uint64_t* hi_tab = lo_tab + 64;
     uint16_t* io = reinterpret_cast<uint16_t*>(sm + kOffIO);  // in_lo | in_hi | out_lo | out_hi
-    const uint32_t bar_u = smem_addr(sm + kOffBar), bar_m = bar_u + 8;
+    double* wsum = reinterpret_cast<double*>(sm + kOffWsum);
+    const uint32_t bars = smem_addr(sm + kOffBar);
+    auto bar = [bars](uint32_t slot) { return bars + 8u * slot; };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t npairs = (total_tiles + 1) / 2;
+    uint64_t my_pairs = 0;
+    if (blockIdx.x < npairs) my_pairs = (npairs - 1 - blockIdx.x) / gridDim.x + 1;
+    const uint64_t steps = my_pairs * uint64_t(nblocks);
+    const uint32_t u0 = smem_addr(sm + kOffU);
+    // Copies of step st: its block's gate image into buffer st % 2 and its
+    // tables into buffer st % 3.
+    auto fetch = [&](uint64_t st) {
+        const FusedBlock* blk = blocks + int(st % uint64_t(nblocks));
+        const uint32_t ub = uint32_t(st & 1), tb = uint32_t(st % 3);
+        mbar_expect(bar(kBarUFull + ub), kUBytes);
+        bulk_g2s(u0 + ub * kUBytes, upool + blk->u_off, kUBytes, bar(kBarUFull + ub));
+        mbar_expect(bar(kBarTFull + tb), kDescBytes);
+        bulk_g2s(smem_addr(sm + kOffDesc + tb * kDescBytes), blk->next_b, kDescBytes, bar(kBarTFull + tb));
+    };
 
     if (tid < 64) {
         uint64_t a = 0, b = 0;
@@ -159,14 +214,18 @@ __global__ void __launch_bounds__(kThreads, 2)
         lo_tab[tid] = a;
         hi_tab[tid] = b;
     }
-    io[tid] = fq.io[tid >> 6][tid & 63];
+    if (tid < 256) io[tid] = fq.io[tid >> 6][tid & 63];
     if (tid == 0) {
         // The swizzled operand needs 1024-byte aligned atoms.
         s_abort = (smem_addr(sm) & 1023u) != 0;
         if (s_abort) atomicExch(err, 3);
-        mbar_init(bar_u, 1);
-        mbar_init(bar_m, 1);
+        s_ucnt[0] = s_ucnt[1] = 0;
+        for (uint32_t i = 0; i < kNumBars; i++) mbar_init(bar(i), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        uint64_t f = 0;
+        if (!s_abort)
+            for (; f < 2 && f < steps; f++) fetch(f);
+        s_fetched = f;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
@@ -177,108 +236,92 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
-    const uint64_t desc_x0 = make_desc_sw128(smem_addr(sm + kOffX0)), desc_x1 = make_desc_sw128(smem_addr(sm + kOffX1));
-    const uint64_t desc_u0 = make_desc(smem_addr(sm + kOffU)), desc_u1 = make_desc(smem_addr(sm + kOffU) + 16384u);
-    uint32_t phase_u = 0, phase_m = 0;
-    uint32_t pending_u = 0, pending_m = 0;  // issued and not yet awaited (thread 0)
-    uint32_t seq = 0;                       // blocks processed: selects the table buffer
-    if (tid == 0 && uint64_t(blockIdx.x) < total_tiles) {
-        fetch_block(sm, blocks, upool, 0, bar_u);
-        pending_u = 1;
-    }
 
+    // Readback group g: tiles 2*pair + g.
+    const int g = warp >> 3, gw = warp & 7, gt = tid & (kGroupThreads - 1);
+    unsigned char* x = sm + uint32_t(g) * 2u * kXBytes;
+    const uint32_t row = uint32_t(gt >> 6);  // elements l = (gt & 63) | (row + 4k) << 6
+    const uint64_t glo = lo_tab[gt & 63];
+    const uint32_t plo = io[gt & 63], olo = io[128 + (gt & 63)];
+    const uint32_t col = uint32_t((gw & 3) * 32 + lane);
+    const uint32_t half = uint32_t(gw >> 2);
+    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 64u * uint32_t(g) + half * 32u;
+    const uint64_t desc_x = make_desc_sw128(smem_addr(x));
     const int rest = n - kFusedM;
-    const uint32_t row = uint32_t(tid >> 6);  // this thread's elements: l = (tid & 63) | (row + 4k) << 6
-    for (uint64_t t = blockIdx.x; t < total_tiles && !s_abort; t += gridDim.x) {
-        const uint64_t st = t >> rest;
+    uint32_t mma_cnt = 0;
+    uint64_t st = 0;
+    bool ok = !s_abort;
+    for (uint64_t pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
+        const uint64_t t = 2 * pair + uint64_t(g);
+        if (t >= total_tiles) break;  // only the last pair of the grid can be odd
+        const bool partner = 2 * pair + uint64_t(g ^ 1) < total_tiles;
+        const uint64_t stt = t >> rest;
         uint64_t tidx = t & ((uint64_t(1) << rest) - 1);
         for (int b = 0; b < kFusedM; b++) {
             uint64_t low = (uint64_t(1) << fq.q[b]) - 1;
             tidx = (tidx & low) | ((tidx & ~low) << 1);
         }
-        float2* __restrict__ g = s + ((st << n) | tidx);
+        float2* __restrict__ gp = s + ((stt << n) | tidx);
         // FP64 renormalisation of the previous pass (tensor-core accumulation
         // rounds toward zero, so unitary blocks shrink the norm slightly).
-        const double scale = in_norm ? 1.0 / sqrt(in_norm[st]) : 1.0;
-        const uint64_t glo = lo_tab[tid & 63];
+        const double scale = in_norm ? 1.0 / sqrt(in_norm[stt]) : 1.0;
         {
-            // Tile -> A operand of block 0, split into TF32 hi / lo (loads first, all in flight).
             float2 v[16];
 #pragma unroll
-            for (int k = 0; k < 16; k++) v[k] = __ldcs(g + (glo | hi_tab[row + 4 * k]));
-            const uint32_t plo = io[tid & 63];
+            for (int k = 0; k < 16; k++) v[k] = gp[glo | hi_tab[row + 4 * k]];
 #pragma unroll
             for (int k = 0; k < 16; k++)
-                put_split(sm, plo ^ io[64 + row + 4 * k], float(double(v[k].x) * scale), float(double(v[k].y) * scale));
+                put_split(x, plo ^ io[64 + row + 4 * k], float(double(v[k].x) * scale), float(double(v[k].y) * scale));
         }
         double norm_acc = 0.0;
-        for (int j = 0; j < nblocks; j++) {
-            const uint32_t buf = seq & 1u;
+        for (int j = 0; j < nblocks; j++, st++) {
+            // Operand of step st written: one thread issues its MMAs.
+            asm volatile("tcgen05.fence::before_thread_sync;");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (tid == 0) {
-                bool ok = mbar_wait(bar_u, phase_u & 1);
-                phase_u++;
-                pending_u = 0;
-                if (!ok) {
-                    s_abort = 1;
-                    atomicExch(err, 3);
-                } else {
+            group_sync(g);
+            bool w = true;
+            const uint32_t ub = uint32_t(st & 1);
+            if (gt == 0) {
+                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st >> 1) & 1u);
+                if (w) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
+                    const uint64_t desc_u = make_desc(u0 + ub * kUBytes);
                     // Descriptors advance by (byte offset >> 4) in their start-address field.
 #pragma unroll
                     for (int q = 0; q < 24; q++) {
                         const int part = q >> 3, ks = q & 7;
-                        const uint64_t ad = (part == 2 ? desc_x1 : desc_x0) + uint64_t((ks >> 2) * 1024 + (ks & 3) * 2);
-                        const uint64_t bd = (part == 1 ? desc_u1 : desc_u0) + uint64_t(ks * 16);
+                        const uint64_t ad = desc_x + (part == 2 ? uint64_t(kXBytes >> 4) : 0) +
+                                            uint64_t((ks >> 2) * 1024 + (ks & 3) * 2);
+                        const uint64_t bd = desc_u + (part == 1 ? uint64_t(16384 >> 4) : 0) + uint64_t(ks * 16);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 64u * g),
                             "l"(ad), "l"(bd), "r"(kIdesc), "r"(q > 0 ? 1u : 0u));
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                        bar_m)
+                        bar(kBarMma + g))
                                  : "memory");
-                    pending_m = 1;
-                    ok = mbar_wait(bar_m, phase_m & 1);
-                    phase_m++;
-                    pending_m = 0;
-                    if (!ok) {
-                        s_abort = 1;
-                        atomicExch(err, 3);
-                    } else {
-                        // The gate image is free again: fetch the next block's while this one is read back.
-                        const int next = j + 1 < nblocks ? j + 1 : (t + gridDim.x < total_tiles ? 0 : -1);
-                        if (next >= 0) {
-                            fetch_block(sm, blocks + next, upool, buf ^ 1u, bar_u);
-                            pending_u = 1;
-                        }
-                    }
                 }
             }
-            __syncthreads();
-            if (s_abort) break;
+            w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u);
+            mma_cnt++;
+            w = w && mbar_wait(bar(kBarTFull + uint32_t(st % 3)), uint32_t(st / 3) & 1u);
+            if (!group_all(w, g)) {
+                ok = false;
+                break;
+            }
+            if (gt == 0 && st + 2 < steps) {
+                // The gate-image buffer is free once both tiles' MMAs on it completed:
+                // the second group to get here fetches step st + 2 into it.
+                if (!partner || (atomicAdd(&s_ucnt[ub], 1u) & 1u)) {
+                    fetch(st + 2);
+                    atomicMax(&s_fetched, st + 3);
+                }
+            }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // Readback: warp w reads TMEM lanes 32*(w%4).. (tile columns) and
-            // output columns 32*(w/4).. (16 complex outputs per thread).
-            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + buf * kDescBytes);
-            const uint16_t* nc = nb + 32;
-            const uint32_t col = uint32_t((warp & 3) * 32 + lane);
-            const uint32_t half = uint32_t(warp >> 2);
-            uint32_t r[32];
-            const uint32_t taddr = tmem + ((uint32_t(warp & 3) * 32u) << 16) + half * 32u;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const uint32_t cpart = nc[col];
+            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % 3) * kDescBytes);
+            const uint32_t cpart = nb[32 + col];
             uint32_t nbw[8];  // this half's 16 destination parts, two per word
             {
                 const uint4 w0 = *reinterpret_cast<const uint4*>(nb + half * 16);
@@ -286,49 +329,77 @@ __global__ void __launch_bounds__(kThreads, 2)
                 nbw[0] = w0.x, nbw[1] = w0.y, nbw[2] = w0.z, nbw[3] = w0.w;
                 nbw[4] = w1.x, nbw[5] = w1.y, nbw[6] = w1.z, nbw[7] = w1.w;
             }
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (j + 1 < nblocks) {
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                    put_split(sm, off, __uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+                    put_split(x, off, __uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
                 }
             } else {
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
                     const float re = __uint_as_float(r[2 * i]), im = __uint_as_float(r[2 * i + 1]);
-                    *reinterpret_cast<float2*>(sm + kOffX0 + off) = make_float2(re, im);
+                    *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
                     norm_acc += double(re) * re + double(im) * im;
                 }
             }
-            seq++;
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
         }
-        if (s_abort) break;
-        const uint32_t olo = io[128 + (tid & 63)];
+        if (!ok) break;
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        group_sync(g);  // stage complete
 #pragma unroll
         for (int k = 0; k < 16; k++)
-            g[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(sm + kOffX0 + (olo ^ io[192 + row + 4 * k]));
+            gp[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + row + 4 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
-        if (lane == 0) s_wsum[warp] = norm_acc;
-        __syncthreads();
-        if (tid == 0) {
+        if (lane == 0) wsum[g * 8 + gw] = norm_acc;
+        group_sync(g);
+        if (gt == 0) {
             double tsum = 0.0;
-            for (int w = 0; w < kThreads / 32; w++) tsum += s_wsum[w];
+            for (int w2 = 0; w2 < 8; w2++) tsum += wsum[g * 8 + w2];
             tile_norm[t] = tsum;
         }
-        __syncthreads();
+        group_sync(g);  // stage and sums read before the next tile overwrites them
     }
-    // On an aborted wait, give the copies and the MMAs in flight a bounded chance to land.
-    if (tid == 0) {
-        if (pending_u) mbar_wait(bar_u, phase_u & 1);
-        if (pending_m) mbar_wait(bar_m, phase_m & 1);
+    if (!ok && gt == 0) {
+        s_abort = 1;
+        atomicExch(err, 3);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    if (gt == 0 && s_abort) {
+        // Bounded drain of this CTA's own copies and MMAs still in flight
+        // (each issuing thread commits and waits for its own MMAs).
+        if (g == 0) {
+            const uint64_t fetched = s_fetched;
+            for (uint64_t f = fetched > 3 ? fetched - 3 : 0; f < fetched; f++) {
+                if (f + 2 >= fetched) mbar_wait(bar(kBarUFull + uint32_t(f & 1)), uint32_t(f >> 1) & 1u);
+                mbar_wait(bar(kBarTFull + uint32_t(f % 3)), uint32_t(f / 3) & 1u);
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            bar(kBarDrain + g))
+                     : "memory");
+        mbar_wait(bar(kBarDrain + g), 0);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
 int sm_count() {
@@ -386,6 +457,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
                 const double* in_norm, double* tile_norm) {
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
     if (b.n < kFusedM || int(p.qubits.size()) != kFusedM) fail(kValueError, "fused passes need 12 tile qubits");
+    if (p.nblocks < 1) fail(kValueError, "fused pass without blocks");
     FusedQubits fq;
     for (int i = 0; i < kFusedM; i++) fq.q[i] = p.qubits[i];
     for (int e = 0; e < 64; e++) {
@@ -394,32 +466,20 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
         fq.io[2][e] = p.out_lo[e];
         fq.io[3][e] = p.out_hi[e];
     }
-    // Two CTAs per SM need the largest shared-memory carveout.  Residency is
-    // computed from the kernel's registers and shared memory (the grid-stride
-    // loop is correct for any grid; a grid below residency leaves SMs half idle).
-    static int per_sm_of[64] = {};
+    static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    int& per_sm = per_sm_of[dev & 63];
-    if (per_sm == 0) {
+    if (!configured[dev & 63]) {
         cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_fused, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      int(cudaSharedmemCarveoutMaxShared));
-        cudaFuncAttributes fa{};
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_fused);
-        int smem_sm = 0, reserved = 0, regs_sm = 0;
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
         if (e != cudaSuccess) fail(kCudaError, std::string("fused pass setup: ") + cudaGetErrorString(e));
-        const size_t per_cta = kSmemBytes + fa.sharedSizeBytes + size_t(reserved);
-        const int by_smem = int(size_t(smem_sm) / per_cta);
-        const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kThreads) : 2;
-        per_sm = std::max(1, std::min({2, by_smem, by_regs}));
+        configured[dev & 63] = true;
     }
+    // One CTA per SM, persistent over pairs of tiles.
     const uint64_t total = b.W << (b.n - kFusedM);
-    const uint64_t grid = std::min<uint64_t>(total, uint64_t(sm_count()) * uint64_t(per_sm));
+    const uint64_t grid = std::min<uint64_t>((total + 1) / 2, uint64_t(sm_count()));
     k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq,
                                                                blocks_dev + p.first_block, p.nblocks, upool_dev, total,
                                                                err, in_norm, tile_norm);
