@@ -664,7 +664,7 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
         std::vector<double2> pool;
         auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
         std::vector<FusedBlock> blocks;
-        std::vector<float> upool;
+        std::vector<uint16_t> upool;
         std::string s = "{\"n\":" + std::to_string(n) + ",\"passes\":[";
         char buf[48];
         for (size_t pi = 0; pi < passes.size(); pi++) {
@@ -694,7 +694,7 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
         }
         s += "],\"upool\":[";
         for (size_t i = 0; i < upool.size(); i++) {
-            std::snprintf(buf, sizeof buf, "%s%.9g", i ? "," : "", upool[i]);
+            std::snprintf(buf, sizeof buf, "%s%u", i ? "," : "", unsigned(upool[i]));
             s += buf;
         }
         s += "]}";

@@ -336,11 +336,11 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
         }
         if (!fused_blocks_host_.empty()) {
             fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
-            upool_.alloc(upool_host_.size() * sizeof(float), "fused block gate images");
+            upool_.alloc(upool_host_.size() * sizeof(uint16_t), "fused block gate images");
             cuda_check(cudaMemcpyAsync(fused_blocks_.p, fused_blocks_host_.data(),
                                        fused_blocks_host_.size() * sizeof(FusedBlock), cudaMemcpyHostToDevice, b.stream),
                        "upload fused blocks");
-            cuda_check(cudaMemcpyAsync(upool_.p, upool_host_.data(), upool_host_.size() * sizeof(float),
+            cuda_check(cudaMemcpyAsync(upool_.p, upool_host_.data(), upool_host_.size() * sizeof(uint16_t),
                                        cudaMemcpyHostToDevice, b.stream),
                        "upload gate images");
         }
@@ -376,7 +376,7 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
             norm_tiles_.ensure(tiles * 8, "fused tile norms");
             norm_states_.ensure(size_t(b.W) * 8, "fused state norms");
             if (rec) rec->begin(kcFused, step_bytes(si, b));
-            k::fused_pass(b, p, fused_blocks_.as<FusedBlock>(), upool_.as<float>(), b.err,
+            k::fused_pass(b, p, fused_blocks_.as<FusedBlock>(), upool_.as<uint16_t>(), b.err,
                           norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>());
             k::fused_state_norm(b, norm_tiles_.as<double>(), norm_states_.as<double>());
             norm_pending = true;

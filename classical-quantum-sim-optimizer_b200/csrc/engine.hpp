@@ -156,7 +156,7 @@ class Executor {
     std::vector<TileOp> tile_ops_host_;
     std::vector<FusedPass> fused_;
     std::vector<FusedBlock> fused_blocks_host_;
-    std::vector<float> upool_host_;
+    std::vector<uint16_t> upool_host_;
     DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_;
     bool uploaded_ = false;
     ExecConfig cfg_;

@@ -3,27 +3,33 @@
 // A tile is 2^12 amplitudes.  For block j (a 32x32 complex matrix U on 5 tile
 // qubits) the tile is held in shared memory as the A operand of D = A * B: 128
 // rows (the tile's 128 "columns", i.e. values of the other 7 tile qubits) by
-// K = 64 real inputs (re/im of the 32 basis states), split into TF32 hi and lo
-// parts.  B is the block's real 64x64 form of U (hi and lo), brought in by a
-// cp.async.bulk (TMA) copy.  24 tcgen05.mma.kind::tf32 instructions (M=128,
-// N=64, K=8) accumulate A_hi*B_hi + A_hi*B_lo + A_lo*B_hi into a 128 x 64 FP32
-// tile in tensor memory.  The readback (tcgen05.ld, one TMEM lane per tile
-// column) writes every output amplitude straight into the layout the next
-// block needs (128-byte swizzled, bit orders chosen on the host to spread each
-// half-warp's stores over all banks), or, after the last block, into a
-// swizzled natural-order stage for the store to HBM.
+// K = 64 real inputs (re/im of the 32 basis states), split into f16 hi and lo
+// parts after scaling the tile by a power of two (its norm is kept in
+// [2^13, 2^14), so every amplitude and every block output stays in f16 range;
+// blocks are unitary).  B is the block's real 64x64 form of U (f16 hi and lo),
+// brought in by a cp.async.bulk (TMA) copy.  12 tcgen05.mma.kind::f16
+// instructions (M=128, N=64, K=16) accumulate A_hi*B_hi + A_hi*B_lo +
+// A_lo*B_hi into a 128 x 64 FP32 tile in tensor memory.  The readback
+// (tcgen05.ld, one TMEM lane per tile column) writes every output amplitude
+// straight into the layout the next block needs (128-byte swizzled, bit orders
+// chosen on the host so that each warp's stores hit every bank once), or,
+// after the last block, unscaled into a swizzled natural-order FP32 stage for
+// the store to HBM.
 //
 // One CTA per SM, persistent over pairs of tiles, with two groups of 8 warps.
-// Group g owns tile 2*pair + g, one 64-column TMEM accumulator and its own
-// operand buffers; one thread of the group issues its MMAs, so one tile's
-// MMAs run while the other tile is read back.  The two tiles walk the same
-// block sequence and share the gate images (two buffers, fetched two blocks
-// ahead by whichever group finishes its MMAs on a buffer last).  Hand-offs
-// are mbarriers (copies, MMA completion) and per-group named barriers; every
-// mbarrier wait is bounded, and a group stops only by a group-wide vote, so
-// no thread is left waiting on a named barrier.  On expiry the CTA records an
-// error, waits (bounded) for its own copies and MMAs, frees its tensor memory
-// and stops.
+// Group g owns tile 2*pair + g, one 64-column TMEM accumulator, its operand
+// buffers and a buffer into which its next tile is prefetched (cp.async)
+// while the current one runs; one thread of the group issues its MMAs, so one
+// tile's MMAs run while the other tile is read back.  The two tiles walk the
+// same block sequence and share the gate images (two buffers, fetched two
+// blocks ahead by whichever group finishes its MMAs on a buffer last).
+// Hand-offs are mbarriers (copies, MMA completion) and per-group named
+// barriers; every mbarrier wait is bounded, and a group stops only by a
+// group-wide vote, so no thread is left waiting on a named barrier.  On expiry
+// the CTA records an error, waits (bounded) for its own copies and MMAs, frees
+// its tensor memory and stops.
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cstddef>
 #include <cstdio>
@@ -35,24 +41,27 @@ namespace dq {
 namespace k {
 namespace {
 
-constexpr int kGroupThreads = 256;                        // one readback group (8 warps)
-constexpr int kThreads = 2 * kGroupThreads;               // two groups
-constexpr uint32_t kTmemCols = 128;                       // one 64-column accumulator per group
-constexpr uint32_t kXBytes = 32768;                       // one operand copy of a tile (4096 complex64)
-constexpr uint32_t kUBytes = 32768;                       // U_hi + U_lo images of one block
-constexpr uint32_t kDescBytes = 320;                      // next_b[32] + next_c[128] (u16) of one block
-constexpr uint32_t kOffU = 4 * kXBytes;                   // group g: X_hi at g*64K, X_lo at g*64K + 32K
-constexpr uint32_t kOffTabs = kOffU + 2 * kUBytes;        // lo_tab[64], hi_tab[64] (u64)
-constexpr uint32_t kOffIO = kOffTabs + 128 * 8;           // in_lo, in_hi, out_lo, out_hi [64] (u16)
-constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;        // three block-table buffers
-constexpr uint32_t kOffBar = kOffDesc + 3 * kDescBytes;   // mbarriers, 8-byte aligned
-constexpr uint32_t kOffWsum = kOffBar + 16 * 8;           // per-group warp sums (double)
+constexpr int kGroupThreads = 256;                       // one group (8 warps)
+constexpr int kThreads = 2 * kGroupThreads;              // two groups
+constexpr uint32_t kTmemCols = 128;                      // one 64-column accumulator per group
+constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part of a tile (4096 x 4 B)
+constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
+constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
+constexpr uint32_t kDescBytes = 320;                     // next_b[32] + next_c[128] (u16) of one block
+constexpr uint32_t kOffRaw = 2 * kTileBytes;             // group g: operand at g*32K, prefetch at 64K + g*32K
+constexpr uint32_t kOffU = kOffRaw + 2 * kTileBytes;     // two gate-image buffers
+constexpr uint32_t kOffTabs = kOffU + 2 * kUBytes;       // lo_tab[64], hi_tab[64] (u64)
+constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
+constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // three block-table buffers
+constexpr uint32_t kOffBar = kOffDesc + 3 * kDescBytes;  // mbarriers, 8-byte aligned
+constexpr uint32_t kOffWsum = kOffBar + 16 * 8;          // per-group warp sums (double)
 constexpr uint32_t kSmemBytes = kOffWsum + 2 * 8 * 8;
-constexpr uint64_t kSpinLimit = uint64_t(1) << 26;        // polls of an mbarrier before giving up
-constexpr long long kWaitCycles = 4000000000LL;           // ... or this many SM cycles
+constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
+constexpr long long kWaitCycles = 4000000000LL;          // ... or this many SM cycles
 static_assert(kOffDesc % 16 == 0 && kDescBytes % 16 == 0, "bulk copies need 16-byte alignment");
-static_assert(kOffBar % 8 == 0 && kOffWsum % 8 == 0, "mbarrier alignment");
+static_assert(kOffU % 1024 == 0 && kOffBar % 8 == 0 && kOffWsum % 8 == 0, "operand and mbarrier alignment");
 static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
+static_assert(kUBytes == kFusedUHalves * 2, "gate image size");
 
 // mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
 constexpr uint32_t kBarUFull = 0;  // [2] gate image of buffer b landed (expect_tx)
@@ -70,21 +79,10 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// K-major, no-swizzle shared-memory matrix descriptor (sm_100 format, version 1):
-// leading byte offset 128 (the two 16-byte K chunks of one MMA), stride byte
-// offset 2048 (consecutive 8-row core-matrix groups).  Used for the gate image.
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= uint64_t((saddr & 0x3FFFFu) >> 4);
-    d |= uint64_t(128u >> 4) << 16;
-    d |= uint64_t(2048u >> 4) << 32;
-    d |= uint64_t(1) << 46;
-    return d;
-}
-
-// K-major, 128-byte-swizzled descriptor (layout type 2): 8-row x 128-byte
-// atoms, 1024 bytes between 8-row groups; the leading offset is unused.  The
-// start address steps 32 bytes per K = 8 slice inside an atom.  Used for the tile.
+// K-major, 128-byte-swizzled shared-memory matrix descriptor (sm_100 format,
+// version 1, layout type 2): 8-row x 128-byte atoms, 1024 bytes between 8-row
+// groups; the leading offset is unused.  A row holds all 64 f16 K elements, so
+// the start address steps 32 bytes per K = 16 slice.
 __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
     uint64_t d = 0;
     d |= uint64_t((saddr & 0x3FFFFu) >> 4);
@@ -95,8 +93,8 @@ __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
     return d;
 }
 
-// kind::tf32 instruction descriptor: D FP32, A/B TF32, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16 instruction descriptor: D FP32, A/B F16, both K-major, N = 64, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
@@ -124,10 +122,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
 __device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -138,12 +132,12 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 
-// Barrier over one readback group (named barrier 1 + g, 256 threads).
+// Barrier over one group (named barrier 1 + g, 256 threads).
 __device__ __forceinline__ void group_sync(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory");
 }
 
-// Barrier over one readback group that also ANDs a predicate across it.
+// Barrier over one group that also ANDs a predicate across it.
 __device__ __forceinline__ bool group_all(bool v, int g) {
     uint32_t r;
     asm volatile(
@@ -157,28 +151,34 @@ __device__ __forceinline__ bool group_all(bool v, int g) {
     return r != 0;
 }
 
-__device__ __forceinline__ float tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+// f16 hi part rounded to nearest, lo = f16 of the remainder.
+__device__ __forceinline__ void put_split(unsigned char* x, uint32_t off, float re, float im) {
+    const __half2 h = __floats2half2_rn(re, im);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
+    *reinterpret_cast<__half2*>(x + off) = h;
+    *reinterpret_cast<__half2*>(x + kPartBytes + off) = l;
 }
 
-// TF32 hi part rounded to nearest; the lo remainder is left for the tensor
-// core to truncate (its error is below 2^-22 of the value).
-__device__ __forceinline__ void put_split(unsigned char* x, uint32_t off, float re, float im) {
-    const float hr = tf32(re), hi = tf32(im);
-    *reinterpret_cast<float2*>(x + off) = make_float2(hr, hi);
-    *reinterpret_cast<float2*>(x + kXBytes + off) = make_float2(re - hr, im - hi);
+// Global position of the first amplitude of tile t (its local index 0).
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, int n, const FusedQubits& fq) {
+    const int rest = n - kFusedM;
+    uint64_t tidx = t & ((uint64_t(1) << rest) - 1);
+    for (int b = 0; b < kFusedM; b++) {
+        const uint64_t low = (uint64_t(1) << fq.q[b]) - 1;
+        tidx = (tidx & low) | ((tidx & ~low) << 1);
+    }
+    return ((t >> rest) << n) | tidx;
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
     k_fused(float2* __restrict__ s, int n, FusedQubits fq, const FusedBlock* __restrict__ blocks, int nblocks,
-            const float* __restrict__ upool, uint64_t total_tiles, int* __restrict__ err,
+            const uint16_t* __restrict__ upool, uint64_t total_tiles, int* __restrict__ err,
             const double* __restrict__ in_norm, double* __restrict__ tile_norm) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
-    __shared__ unsigned s_ucnt[2];          // per gate-image buffer: groups whose MMAs on it completed
+    __shared__ unsigned s_ucnt[2];            // per gate-image buffer: groups whose MMAs on it completed
     __shared__ unsigned long long s_fetched;  // steps whose copies were issued
     uint64_t* lo_tab = reinterpret_cast<uint64_t*>(sm + kOffTabs);
     uint64_t* hi_tab = lo_tab + 64;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (tid < 256) io[tid] = fq.io[tid >> 6][tid & 63];
     if (tid == 0) {
-        // The swizzled operand needs 1024-byte aligned atoms.
+        // The swizzled operands need 1024-byte aligned atoms.
         s_abort = (smem_addr(sm) & 1023u) != 0;
         if (s_abort) atomicExch(err, 3);
         s_ucnt[0] = s_ucnt[1] = 0;
@@ -237,42 +237,62 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
 
-    // Readback group g: tiles 2*pair + g.
     const int g = warp >> 3, gw = warp & 7, gt = tid & (kGroupThreads - 1);
-    unsigned char* x = sm + uint32_t(g) * 2u * kXBytes;
-    const uint32_t row = uint32_t(gt >> 6);  // elements l = (gt & 63) | (row + 4k) << 6
+    unsigned char* x = sm + uint32_t(g) * kTileBytes;
+    unsigned char* raw = sm + kOffRaw + uint32_t(g) * kTileBytes;
+    const uint32_t row = uint32_t(gt >> 6);  // this thread's elements: l = (gt & 63) | (row + 4k) << 6
     const uint64_t glo = lo_tab[gt & 63];
     const uint32_t plo = io[gt & 63], olo = io[128 + (gt & 63)];
     const uint32_t col = uint32_t((gw & 3) * 32 + lane);
     const uint32_t half = uint32_t(gw >> 2);
     const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 64u * uint32_t(g) + half * 32u;
     const uint64_t desc_x = make_desc_sw128(smem_addr(x));
-    const int rest = n - kFusedM;
+    // Prefetch of tile t into this group's raw buffer, natural local order.
+    auto prefetch = [&](uint64_t t) {
+        const float2* src = s + tile_base(t, n, fq);
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(raw + (gt + 256u * k) * 8u)),
+                         "l"(src + (glo | hi_tab[row + 4 * k]))
+                         : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     uint32_t mma_cnt = 0;
     uint64_t st = 0;
     bool ok = !s_abort;
+    if (ok && uint64_t(blockIdx.x) * 2 + uint64_t(g) < total_tiles) prefetch(uint64_t(blockIdx.x) * 2 + uint64_t(g));
     for (uint64_t pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
         const uint64_t t = 2 * pair + uint64_t(g);
         if (t >= total_tiles) break;  // only the last pair of the grid can be odd
         const bool partner = 2 * pair + uint64_t(g ^ 1) < total_tiles;
-        const uint64_t stt = t >> rest;
-        uint64_t tidx = t & ((uint64_t(1) << rest) - 1);
-        for (int b = 0; b < kFusedM; b++) {
-            uint64_t low = (uint64_t(1) << fq.q[b]) - 1;
-            tidx = (tidx & low) | ((tidx & ~low) << 1);
-        }
-        float2* __restrict__ gp = s + ((stt << n) | tidx);
+        const uint64_t base = tile_base(t, n, fq);
         // FP64 renormalisation of the previous pass (tensor-core accumulation
         // rounds toward zero, so unitary blocks shrink the norm slightly).
-        const double scale = in_norm ? 1.0 / sqrt(in_norm[stt]) : 1.0;
-        {
-            float2 v[16];
+        const double scale = in_norm ? 1.0 / sqrt(in_norm[base >> n]) : 1.0;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        group_sync(g);
+        float2 v[16];
+        float part = 0.f;
 #pragma unroll
-            for (int k = 0; k < 16; k++) v[k] = gp[glo | hi_tab[row + 4 * k]];
-#pragma unroll
-            for (int k = 0; k < 16; k++)
-                put_split(x, plo ^ io[64 + row + 4 * k], float(double(v[k].x) * scale), float(double(v[k].y) * scale));
+        for (int k = 0; k < 16; k++) {
+            const float2 r = *reinterpret_cast<const float2*>(raw + (gt + 256u * k) * 8u);
+            v[k] = make_float2(float(double(r.x) * scale), float(double(r.y) * scale));
+            part += v[k].x * v[k].x + v[k].y * v[k].y;
         }
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) wsum[g * 8 + gw] = double(part);
+        group_sync(g);  // raw read and partial norms written
+        if (pair + gridDim.x < npairs && 2 * (pair + gridDim.x) + uint64_t(g) < total_tiles)
+            prefetch(2 * (pair + gridDim.x) + uint64_t(g));
+        // Power-of-two scale putting the tile norm in [2^13, 2^14).
+        float m2 = 0.f;
+        for (int w2 = 0; w2 < 8; w2++) m2 += float(wsum[g * 8 + w2]);
+        int em = -100;
+        if (m2 > 1e-30f) em = ((__float_as_int(sqrtf(m2)) >> 23) & 0xFF) - 127;
+        const int e = min(max(13 - em, -120), 120);
+        const float sc = __int_as_float((127 + e) << 23), inv_sc = __int_as_float((127 - e) << 23);
+#pragma unroll
+        for (int k = 0; k < 16; k++) put_split(x, plo ^ io[64 + row + 4 * k], v[k].x * sc, v[k].y * sc);
         double norm_acc = 0.0;
         for (int j = 0; j < nblocks; j++, st++) {
             // Operand of step st written: one thread issues its MMAs.
@@ -285,28 +305,28 @@ __global__ void __launch_bounds__(kThreads, 1)
                 w = mbar_wait(bar(kBarUFull + ub), uint32_t(st >> 1) & 1u);
                 if (w) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
-                    const uint64_t desc_u = make_desc(u0 + ub * kUBytes);
+                    const uint64_t desc_u = make_desc_sw128(u0 + ub * kUBytes);
                     // Descriptors advance by (byte offset >> 4) in their start-address field.
 #pragma unroll
-                    for (int q = 0; q < 24; q++) {
-                        const int part = q >> 3, ks = q & 7;
-                        const uint64_t ad = desc_x + (part == 2 ? uint64_t(kXBytes >> 4) : 0) +
-                                            uint64_t((ks >> 2) * 1024 + (ks & 3) * 2);
-                        const uint64_t bd = desc_u + (part == 1 ? uint64_t(16384 >> 4) : 0) + uint64_t(ks * 16);
+                    for (int q = 0; q < 12; q++) {
+                        const int part3 = q >> 2, ks = q & 3;
+                        const uint64_t ad = desc_x + (part3 == 2 ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
+                        const uint64_t bd = desc_u + (part3 == 1 ? uint64_t((kUBytes / 2) >> 4) : 0) + uint64_t(ks * 2);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 64u * g),
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 64u * g),
                             "l"(ad), "l"(bd), "r"(kIdesc), "r"(q > 0 ? 1u : 0u));
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                         bar(kBarMma + g))
                                  : "memory");
                 }
+                // The rest of the group waits in the vote below, not on the mbarriers.
+                w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u);
+                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % 3)), uint32_t(st / 3) & 1u);
             }
-            w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u);
             mma_cnt++;
-            w = w && mbar_wait(bar(kBarTFull + uint32_t(st % 3)), uint32_t(st / 3) & 1u);
             if (!group_all(w, g)) {
                 ok = false;
                 break;
@@ -351,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                    const float re = __uint_as_float(r[2 * i]), im = __uint_as_float(r[2 * i + 1]);
+                    const float re = __uint_as_float(r[2 * i]) * inv_sc, im = __uint_as_float(r[2 * i + 1]) * inv_sc;
                     *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
                     norm_acc += double(re) * re + double(im) * im;
                 }
@@ -360,11 +380,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         asm volatile("tcgen05.fence::before_thread_sync;");
         group_sync(g);  // stage complete
+        float2* __restrict__ gp = s + base;
 #pragma unroll
         for (int k = 0; k < 16; k++)
             gp[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + row + 4 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
+        group_sync(g);  // stage read; the scale partials are consumed
         if (lane == 0) wsum[g * 8 + gw] = norm_acc;
         group_sync(g);
         if (gt == 0) {
@@ -372,8 +394,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int w2 = 0; w2 < 8; w2++) tsum += wsum[g * 8 + w2];
             tile_norm[t] = tsum;
         }
-        group_sync(g);  // stage and sums read before the next tile overwrites them
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     if (!ok && gt == 0) {
         s_abort = 1;
         atomicExch(err, 3);
@@ -453,7 +475,7 @@ void fused_renormalize(const Batch& b, const double* norm) {
     if (e != cudaSuccess) fail(kCudaError, std::string("renormalize: ") + cudaGetErrorString(e));
 }
 
-void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const float* upool_dev, int* err,
+void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev, int* err,
                 const double* in_norm, double* tile_norm) {
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
     if (b.n < kFusedM || int(p.qubits.size()) != kFusedM) fail(kValueError, "fused passes need 12 tile qubits");

@@ -195,36 +195,59 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
 // ---------------------------------------------------------------------------
 namespace {
 
-// Round to TF32 (10 explicit mantissa bits), to nearest with ties away from
-// zero, as cvt.rna.tf32.f32 does on the device.
-float tf32_rna(float v) {
+// IEEE binary16 bits of v, rounded to nearest even (|v| below 65504).
+uint16_t f16_rn(float v) {
     uint32_t u;
     std::memcpy(&u, &v, 4);
-    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
-    float r;
-    std::memcpy(&r, &u, 4);
-    return r;
+    const uint16_t sign = uint16_t((u >> 16) & 0x8000u);
+    const int e = int((u >> 23) & 0xFFu) - 127;
+    const uint32_t m = (u & 0x7FFFFFu) | 0x800000u;  // 24-bit significand (normal inputs)
+    if ((u & 0x7FFFFFFFu) == 0 || e < -25) return sign;
+    if (e > 15) return uint16_t(sign | 0x7C00u);
+    uint32_t q, rem, half;
+    if (e < -14) {  // subnormal result: units of 2^-24
+        const int shift = -(e + 1);
+        q = m >> shift;
+        rem = m & ((1u << shift) - 1u);
+        half = 1u << (shift - 1);
+    } else {  // normal: exponent field e + 15, 10 fraction bits
+        q = (uint32_t(e + 15) << 10) | ((m & 0x7FFFFFu) >> 13);
+        rem = m & 0x1FFFu;
+        half = 0x1000u;
+    }
+    if (rem > half || (rem == half && (q & 1u))) q++;  // a carry moves into the exponent correctly
+    return uint16_t(sign | q);
+}
+
+float f16_value(uint16_t h) {
+    const int e = (h >> 10) & 0x1F;
+    const float m = float(h & 0x3FF);
+    const float v = e ? std::ldexp(1024.0f + m, e - 25) : std::ldexp(m, -24);
+    return (h & 0x8000u) ? -v : v;
 }
 
 }  // namespace
 
 uint32_t fused_operand_offset(uint32_t packed) {
     const uint32_t col = packed >> 5, basis = packed & 31u;
-    return (basis >> 4) * 16384u + (col >> 3) * 1024u + (col & 7u) * 128u + ((((basis >> 1) & 7u) ^ (col & 7u)) << 4) +
-           (basis & 1u) * 8u;
+    return (col >> 3) * 1024u + (col & 7u) * 128u + (((basis >> 2) ^ (col & 7u)) << 4) + (basis & 3u) * 4u;
 }
 
 namespace {
 
-// Float offset of (row, k) in the canonical K-major, no-swizzle operand layout
-// with 64 K-elements per row: 8-row x 16-byte core matrices, the K chunks of a
-// row group 128 B apart, row groups 2048 B apart.
-inline size_t canon(int row, int k) { return size_t(row / 8) * 512 + size_t(k / 4) * 32 + size_t(row % 8) * 4 + k % 4; }
+// Half-word offset of (row, k) in a K-major, 128-byte-swizzled operand with 64
+// 16-bit K elements per row: row r at (r / 8) * 1024 + (r % 8) * 128 bytes, its
+// 16-byte chunk index XORed with r % 8.
+inline size_t sw128_half(int row, int k) {
+    const size_t byte = size_t(row / 8) * 1024 + size_t(row % 8) * 128 + size_t(((k * 2) >> 4) ^ (row % 8)) * 16 +
+                        size_t((k * 2) & 15);
+    return byte / 2;
+}
 
 }  // namespace
 
 FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
-                           std::vector<FusedBlock>& blocks, std::vector<float>& upool) {
+                           std::vector<FusedBlock>& blocks, std::vector<uint16_t>& upool) {
     FusedPass fp;
     fp.qubits = tile_qubits;
     fp.raw_ops = int(pass_ops.size());
@@ -280,21 +303,20 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         for (size_t t = 0; t < oth.size(); t++) l |= ((col >> t) & 1u) << oth[t];
         return l;
     };
-    // Bank-aware layouts.  The operand is stored 128-byte swizzled, so the
-    // bank slot of an 8-byte store (one of 16) has bits (b0, b1^c0, b2^c1,
-    // b3^c2) of the block's basis (b) and column (c) index.  Shared memory
-    // serves a warp's 8-byte stores one half-warp at a time, and across a
-    // half-warp the readback of block j-1 varies the four qubits of its column
-    // bits 0..3 (its TMEM lanes; local qubits 0..3 for the tile load).  Block
-    // j's basis and column bit order is chosen greedily so that those four
-    // qubits reach four independent slot bits (one wavefront per half-warp):
-    // one lane qubit of the block at basis bit 0, lane qubits outside it at
-    // column bits 0..2, the rest at the remaining basis bits 1..3.  Free
-    // column bits 0..3 then take a qubit of block j+1 first, so that the next
-    // readback also has a lane qubit there.
+    // Bank-aware layouts.  The operand is stored 128-byte swizzled with 4-byte
+    // complex entries (f16 re, im), so the bank of a store has bits (b0, b1,
+    // b2^c0, b3^c1, b4^c2) of the block's basis (b) and column (c) index.
+    // Across a warp, the readback of block j-1 varies the five qubits of its
+    // column bits 0..4 (its TMEM lanes; local qubits 0..4 for the tile load).
+    // Block j's basis and column bit order is chosen greedily so that those
+    // five qubits reach five independent bank bits (one wavefront per warp):
+    // lane qubits of the block at basis bits 0 and 1, lane qubits outside it
+    // at column bits 0..2, the rest at basis bits 2..4.  Free column bits 0..4
+    // then take qubits of block j+1 first (two of them are needed at its basis
+    // bits 0 and 1).
     const size_t J = blk.size();
     std::vector<std::vector<int>> oth(J);
-    uint32_t lanes = 0xFu;  // qubits varying across a half-warp of the incoming stores
+    uint32_t lanes = 0x1Fu;  // qubits varying across a warp of the incoming stores
     for (size_t j = 0; j < J; j++) {
         Blk& bj = blk[j];
         uint32_t bmask = 0, nmask = 0;
@@ -303,41 +325,37 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
             for (int t = 0; t < 5; t++) nmask |= 1u << blk[j + 1].q[t];
         int bpos[5] = {-1, -1, -1, -1, -1};  // qubit at basis bit k
         int cpos[7] = {-1, -1, -1, -1, -1, -1, -1};
-        uint32_t used = 0;
+        uint32_t used = 0, reached = 0;  // reached bit k: bank bit k varies
         std::vector<int> lb, lc;
         for (int i = 0; i < m; i++)
             if ((lanes >> i) & 1u) ((bmask >> i) & 1u ? lb : lc).push_back(i);
-        uint32_t slots = 0;  // slot bits already reached (bit k: slot bit k)
-        if (!lb.empty()) {
-            bpos[0] = lb[0];
-            used |= 1u << lb[0];
-            slots |= 1u;
+        size_t bi = 0;
+        for (int k = 0; k < 2 && bi < lb.size(); k++, bi++) {
+            bpos[k] = lb[bi];
+            used |= 1u << lb[bi];
+            reached |= 1u << k;
         }
-        for (size_t t = 0; t < lc.size() && t < 3; t++) {
-            cpos[t] = lc[t];
-            used |= 1u << lc[t];
-            slots |= 2u << t;
+        size_t ci = 0;
+        for (int k = 0; k < 3 && ci < lc.size(); k++, ci++) {
+            cpos[k] = lc[ci];
+            used |= 1u << lc[ci];
+            reached |= 4u << k;
         }
-        if (lc.size() > 3) {
-            cpos[3] = lc[3];
-            used |= 1u << lc[3];
+        for (int k = 3; ci < lc.size(); k++, ci++) {  // more lane qubits than bank bits left: no bank
+            cpos[k] = lc[ci];
+            used |= 1u << lc[ci];
         }
-        for (size_t t = 1; t < lb.size(); t++)
-            for (int k = 1; k < 4; k++)
-                if (bpos[k] < 0 && !((slots >> k) & 1u)) {
-                    bpos[k] = lb[t];
-                    used |= 1u << lb[t];
-                    slots |= 1u << k;
-                    break;
-                }
-        for (size_t t = 1; t < lb.size(); t++)  // lane qubits of the block that reached no new slot
-            if (!((used >> lb[t]) & 1u))
-                for (int k = 1; k < 5; k++)
-                    if (bpos[k] < 0) {
-                        bpos[k] = lb[t];
-                        used |= 1u << lb[t];
-                        break;
-                    }
+        for (; bi < lb.size(); bi++) {
+            int k = 2;
+            while (k < 5 && (bpos[k] >= 0 || ((reached >> k) & 1u))) k++;
+            if (k == 5) {
+                k = 2;
+                while (bpos[k] >= 0) k++;
+            }
+            bpos[k] = lb[bi];
+            used |= 1u << lb[bi];
+            reached |= 1u << k;
+        }
         for (int t = 0; t < 5; t++)
             if (!((used >> bj.q[t]) & 1u))
                 for (int k = 0; k < 5; k++)
@@ -346,17 +364,13 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
                         used |= 1u << bj.q[t];
                         break;
                     }
-        // Column bits: lane qubits placed above; then one qubit of the next
-        // block among bits 0..3 (if none is there yet), then the rest ascending.
-        bool next_lane = false;
-        for (int k = 0; k < 4; k++)
-            if (cpos[k] >= 0 && ((nmask >> cpos[k]) & 1u)) next_lane = true;
+        // Column bits: lane qubits placed above, then qubits of the next block
+        // (they become its basis bits), then the rest ascending.
         std::vector<int> rest;
         for (int i = 0; i < m; i++)
             if (!((bmask >> i) & 1u) && !((used >> i) & 1u)) rest.push_back(i);
-        if (!next_lane)
-            std::stable_sort(rest.begin(), rest.end(),
-                             [&](int x, int y) { return ((nmask >> x) & 1u) > ((nmask >> y) & 1u); });
+        std::stable_sort(rest.begin(), rest.end(),
+                         [&](int x, int y) { return ((nmask >> x) & 1u) > ((nmask >> y) & 1u); });
         size_t ri = 0;
         for (int k = 0; k < 7; k++)
             if (cpos[k] < 0) cpos[k] = rest[ri++];
@@ -377,8 +391,11 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         for (int t = 0; t < 5; t++) bj.q[t] = bpos[4 - t];
         oth[j].assign(cpos, cpos + 7);
         lanes = 0;
-        for (int k = 0; k < 4; k++) lanes |= 1u << cpos[k];
+        for (int k = 0; k < 5; k++) lanes |= 1u << cpos[k];
     }
+    // The last block's readback stores 8-byte FP32 entries, one half-warp at a
+    // time: its column bits 0..3 vary across a half-warp.
+    lanes &= ~(1u << oth[J - 1][4]);
     // Stage after the last block: natural index l lives at slot s(l) = l ^ h(l),
     // h copying lane qubits above bit 3 onto the bank bits 0..3 that the last
     // block's lanes leave constant (s is linear and invertible; a warp reading
@@ -426,20 +443,20 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
             d.next_c[c] = d.last ? stage_off(l) : operand_off(blk[j + 1], oth[j + 1], l);
         }
         // Real 64x64 form [[Re, -Im], [Im, Re]] with rows 2b'+ri' and columns 2b+ri,
-        // stored as the B operand (N = 64 output rows, K = 64 inputs, K-major).
-        std::vector<float> img(kFusedUFloats, 0.f);
+        // stored as the B operand (N = 64 output rows, K = 64 inputs, K-major,
+        // 128-byte swizzled) in f16 hi and lo parts.
+        std::vector<uint16_t> img(kFusedUHalves, 0);
         for (int bo = 0; bo < 32; bo++)
             for (int bi = 0; bi < 32; bi++) {
                 const cplx v = blk[j].u[size_t(bo) * 32 + bi];
                 const double e[2][2] = {{v.re, -v.im}, {v.im, v.re}};
                 for (int ro = 0; ro < 2; ro++)
                     for (int ri = 0; ri < 2; ri++) {
-                        float f = float(e[ro][ri]);
-                        float hi = tf32_rna(f);
-                        float lo = tf32_rna(f - hi);
-                        size_t o = canon(2 * bo + ro, 2 * bi + ri);
+                        const uint16_t hi = f16_rn(float(e[ro][ri]));
+                        const uint16_t lo = f16_rn(float(e[ro][ri] - double(f16_value(hi))));
+                        const size_t o = sw128_half(2 * bo + ro, 2 * bi + ri);
                         img[o] = hi;
-                        img[4096 + o] = lo;
+                        img[kFusedUHalves / 2 + o] = lo;
                     }
             }
         upool.insert(upool.end(), img.begin(), img.end());

@@ -79,21 +79,23 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width);
 // ---------------------------------------------------------------------------
 // Tensor-core fused blocks (complex64): a pass of 12 tile qubits whose
 // operations are fused into 32x32 complex blocks, each applied as one
-// 128 x 64 x 192 TF32 contraction (3xTF32 split) on tcgen05.
+// 128 x 64 x 192 FP16 contraction (three products of f16 hi/lo parts, FP32
+// accumulation, tiles scaled by a power of two) on tcgen05.
 // ---------------------------------------------------------------------------
 constexpr int kFusedM = 12;            // tile qubits of a fused pass
 constexpr int kFusedCols = 1 << (kFusedM - 5);
-constexpr int kFusedUFloats = 2 * 64 * 64;  // U_hi and U_lo images of one block
+constexpr int kFusedUHalves = 2 * 64 * 64;  // U_hi and U_lo images of one block (f16)
 
-// Byte offset in a block's tile operand (128-byte swizzled, K-major; K element
-// 2*basis + re/im) of packed position (column << 5) | basis.  Linear over GF(2).
+// Byte offset in a block's tile operand (f16, K-major, 128-byte swizzled; K
+// element 2*basis + re/im) of packed position (column << 5) | basis.  Linear
+// over GF(2).
 uint32_t fused_operand_offset(uint32_t packed);
 
 // Device descriptor of one block.  An output at (column, basis) of this block
 // goes to byte offset next_c[column] ^ next_b[basis]: in the next block's tile
 // operand, or after the last block in the swizzled natural-order stage.
 struct alignas(16) FusedBlock {
-    uint32_t u_off;          // float offset of the block's U_hi/U_lo image in the pool
+    uint32_t u_off;          // f16 offset of the block's U_hi/U_lo image in the pool
     uint32_t last;           // 1: outputs go to the stage
     uint32_t pad[2];
     uint16_t next_b[32];     // output basis -> destination offset part
@@ -109,9 +111,9 @@ struct FusedPass {
 };
 
 // Fuses a pass's operations into 5-qubit blocks and appends their descriptors
-// and TF32 hi/lo gate images (canonical K-major operand layout).
+// and f16 hi/lo gate images (K-major, 128-byte swizzled operand layout).
 FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
-                           std::vector<FusedBlock>& blocks, std::vector<float>& upool);
+                           std::vector<FusedBlock>& blocks, std::vector<uint16_t>& upool);
 
 namespace k {
 // One fused pass over every tile of every state (complex64 only).  err: device
@@ -119,7 +121,7 @@ namespace k {
 // in_norm (per state, nullable): squared norm left by the previous fused pass,
 // divided out on load; tile_norm (W * 2^(n-12) doubles) receives each output
 // tile's FP64 squared norm.
-void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const float* upool_dev,
+void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev,
                 int* err_dev, const double* in_norm, double* tile_norm);
 // norm[st] = fixed-order sum of state st's tile norms.
 void fused_state_norm(const Batch& b, const double* tile_norm, double* norm);

@@ -18,13 +18,15 @@ from oracle import oracle as o
 from dqsim import _core
 
 
-def canon(row, k):
-    return (row // 8) * 512 + (k // 4) * 32 + (row % 8) * 4 + k % 4
+def sw128_half(row, k):
+    """Half-word index of (row, k) in a K-major, 128-byte swizzled f16 operand (64 K per row)."""
+    byte = (row // 8) * 1024 + (row % 8) * 128 + (((k * 2) >> 4) ^ (row % 8)) * 16 + ((k * 2) & 15)
+    return byte // 2
 
 
 ROWS = np.arange(64)[:, None]
 KS = np.arange(64)[None, :]
-CANON = canon(ROWS, KS)
+SW128 = sw128_half(ROWS, KS)
 
 
 def deposit(v, positions):
@@ -36,26 +38,26 @@ def deposit(v, positions):
 
 
 def block_matrix(upool, off):
-    hi = upool[off:off + 4096][CANON]
-    lo = upool[off + 4096:off + 8192][CANON]
-    real = hi.astype(np.float64) + lo.astype(np.float64)
+    """The block's 32x32 complex matrix from its f16 hi/lo gate image."""
+    hi = upool[off:off + 4096][SW128].astype(np.float64)
+    lo = upool[off + 4096:off + 8192][SW128].astype(np.float64)
+    real = hi + lo
     return real[0::2, 0::2] + 1j * real[1::2, 0::2]
 
 
 def operand_offset(packed):
-    """Byte offset of packed (column << 5) | basis in the 128-byte swizzled tile operand."""
+    """Byte offset of packed (column << 5) | basis in the f16, 128-byte swizzled tile operand."""
     col, basis = packed >> 5, packed & 31
-    return ((basis >> 4) * 16384 + (col >> 3) * 1024 + (col & 7) * 128 + ((((basis >> 1) & 7) ^ (col & 7)) << 4)
-            + (basis & 1) * 8)
+    return (col >> 3) * 1024 + (col & 7) * 128 + (((basis >> 2) ^ (col & 7)) << 4) + (basis & 3) * 4
 
 
 PACKED = np.arange(4096)
-SLOT_OF_PACKED = operand_offset(PACKED) // 8  # operand slot holding packed position p
+SLOT_OF_PACKED = operand_offset(PACKED) // 4  # 4-byte operand slot holding packed position p
 
 
 def emulate(plan):
     n = plan["n"]
-    upool = np.asarray(plan["upool"], dtype=np.float32)
+    upool = np.asarray(plan["upool"], dtype=np.uint16).view(np.float16)
     state = np.zeros(1 << n, dtype=np.complex128)
     state[0] = 1.0
     local = np.arange(4096)
@@ -64,17 +66,17 @@ def emulate(plan):
         other = [q for q in range(n) if q not in T]
         idx = deposit(np.arange(1 << (n - 12)), other)[:, None] | deposit(local, T)[None, :]
         tiles = state[idx]
-        # shared memory as 4096 eight-byte slots; tables hold byte offsets combined by XOR
+        # tables hold byte offsets combined by XOR: 4-byte operand entries, 8-byte stage entries
         off = np.asarray(p["in_lo"])[local & 63] ^ np.asarray(p["in_hi"])[local >> 6]
         slots = np.zeros_like(tiles)
-        slots[:, off // 8] = tiles
+        slots[:, off // 4] = tiles
         for blk in p["blocks"]:
             X = slots[:, SLOT_OF_PACKED].reshape(-1, 128, 32)
             U = block_matrix(upool, blk["u_off"])
             Y = X @ U.T
             off = np.asarray(blk["next_c"])[:, None] ^ np.asarray(blk["next_b"])[None, :]
             slots = np.zeros_like(tiles)
-            slots[:, off // 8] = Y
+            slots[:, off // (8 if blk["last"] else 4)] = Y
         out = np.asarray(p["out_lo"])[local & 63] ^ np.asarray(p["out_hi"])[local >> 6]
         tiles = slots[:, out // 8]
         state[idx] = tiles
@@ -105,14 +107,20 @@ def test_fused_plan_random_circuits(seed):
     check(Circuit(13, ins))
 
 
-def test_gate_images_are_tf32_hi_lo_pairs():
+def test_gate_images_are_f16_hi_lo_pairs():
     plan = _core.fused_plan_dump(brickwork(13, 4, seed=1, measure=False).model_dump_json())
-    up = np.asarray(plan["upool"], dtype=np.float32)
-    bits = up.view(np.uint32)
+    up = np.asarray(plan["upool"], dtype=np.uint16).view(np.float16)
     for blk in plan["passes"][0]["blocks"]:
-        hi = bits[blk["u_off"]:blk["u_off"] + 4096]
-        assert np.all((hi & 0x1FFF) == 0)  # 10 explicit mantissa bits
+        hi = up[blk["u_off"]:blk["u_off"] + 4096]
+        lo = up[blk["u_off"] + 4096:blk["u_off"] + 8192]
+        # lo is at most half an f16 unit of hi: it carries the next 11 bits
+        assert np.all(np.abs(lo.astype(np.float64)) <= np.abs(hi.astype(np.float64)) * 2.0 ** -11 + 2.0 ** -24)
     assert plan["passes"][0]["blocks"][-1]["last"] == 1
+
+
+def test_operand_offsets_are_a_bijection():
+    offs = operand_offset(PACKED)
+    assert len(set(offs.tolist())) == 4096 and offs.max() < 16384 and np.all(offs % 4 == 0)
 
 
 def test_fused_block_counts_for_30q_brickwork():
