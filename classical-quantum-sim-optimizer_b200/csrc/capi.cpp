@@ -661,6 +661,7 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
         TilePlanOptions o;
         o.m = kFusedM;
         o.keep_raw = true;
+        o.pinned_low = kFusedPinned;
         std::vector<double2> pool;
         auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
         std::vector<FusedBlock> blocks;

@@ -196,6 +196,7 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     if (cfg_.fused && cfg_.c64 && cfg_.n >= kFusedM) {
         o.m = kFusedM;
         o.keep_raw = true;
+        o.pinned_low = kFusedPinned;
         std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
         for (auto& p : ps) {
             Step s;

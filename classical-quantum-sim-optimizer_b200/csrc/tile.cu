@@ -518,9 +518,11 @@ size_t closure(const Dag& g, PlanState& s, const std::vector<char>& inT, std::ve
 }
 
 // Grow T from a seed op and absorb; returns (ops, T) without committing.
-size_t grow(const Dag& g, PlanState s, size_t seed, int m, int n, std::vector<char>& inT, std::vector<size_t>* taken) {
+size_t grow(const Dag& g, PlanState s, size_t seed, int m, int n, int pinned, std::vector<char>& inT,
+            std::vector<size_t>* taken) {
     inT.assign(n, 0);
     int size = 0;
+    for (int q = 0; q < pinned && q < n; q++, size++) inT[q] = 1;
     for (auto q : g.qs[seed])
         if (!inT[q]) {
             inT[q] = 1;
@@ -667,7 +669,8 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
     // A pass holds every qubit of each of its operations.
     int widest = 1;
     for (size_t i = begin; i < end; i++) widest = std::max(widest, int(ops[i].touched().size()));
-    const int m = std::min(std::max(opt.m, widest), n);
+    const int pinned = std::min(std::max(opt.pinned_low, 0), n);
+    const int m = std::min(std::max(opt.m, widest + pinned), n);
     Dag g;
     g.qs.resize(N);
     g.per_qubit.assign(n, {});
@@ -686,7 +689,7 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
         size_t best_seed = seeds[0], best_count = 0;
         for (size_t sd : seeds) {
             std::vector<char> inT;
-            size_t c = grow(g, s, sd, m, n, inT, nullptr);
+            size_t c = grow(g, s, sd, m, n, pinned, inT, nullptr);
             if (c > best_count) {
                 best_count = c;
                 best_seed = sd;
@@ -694,7 +697,7 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
         }
         std::vector<char> inT;
         std::vector<size_t> taken;
-        grow(g, s, best_seed, m, n, inT, &taken);
+        grow(g, s, best_seed, m, n, pinned, inT, &taken);
         for (size_t o : taken) take(g, s, o);
         // pad T to m qubits with the lowest free qubits (longer contiguous rows)
         int size = 0;

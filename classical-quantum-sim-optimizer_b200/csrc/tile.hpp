@@ -57,6 +57,9 @@ struct TilePlanOptions {
     // Keep each pass's raw operations (for fused tensor-core blocks) instead
     // of lowering them to tile-local operations.
     bool keep_raw = false;
+    // Qubits 0..pinned_low-1 belong to every tile, so each thread's run of
+    // amplitudes in HBM is 2^pinned_low elements long (whole 32-byte sectors).
+    int pinned_low = 0;
 };
 
 // Widest dense operation a tile pass applies on CUDA cores (register budget).
@@ -83,6 +86,7 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width);
 // accumulation, tiles scaled by a power of two) on tcgen05.
 // ---------------------------------------------------------------------------
 constexpr int kFusedM = 12;            // tile qubits of a fused pass
+constexpr int kFusedPinned = 2;        // low qubits in every fused tile (32-byte runs of complex64)
 constexpr int kFusedCols = 1 << (kFusedM - 5);
 constexpr int kFusedUHalves = 2 * 64 * 64;  // U_hi and U_lo images of one block (f16)
 
