@@ -49,11 +49,13 @@ constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also 
 constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
 constexpr uint32_t kDescBytes = 320;                     // next_b[32] + next_c[128] (u16) of one block
 constexpr uint32_t kOffRaw = 2 * kTileBytes;             // group g: operand at g*32K, prefetch at 64K + g*32K
-constexpr uint32_t kOffU = kOffRaw + 2 * kTileBytes;     // two gate-image buffers
-constexpr uint32_t kOffTabs = kOffU + 2 * kUBytes;       // lo_tab[64], hi_tab[64] (u64)
+constexpr uint32_t kUBufs = 3;                           // gate images in flight (fetched kUBufs blocks ahead)
+constexpr uint32_t kTBufs = kUBufs + 1;                  // block tables (also read during the readback)
+constexpr uint32_t kOffU = kOffRaw + 2 * kTileBytes;     // gate-image buffers
+constexpr uint32_t kOffTabs = kOffU + kUBufs * kUBytes;  // lo_tab[64], hi_tab[64] (u64)
 constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
-constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // three block-table buffers
-constexpr uint32_t kOffBar = kOffDesc + 3 * kDescBytes;  // mbarriers, 8-byte aligned
+constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // block-table buffers
+constexpr uint32_t kOffBar = kOffDesc + kTBufs * kDescBytes;  // mbarriers, 8-byte aligned
 constexpr uint32_t kOffWsum = kOffBar + 16 * 8;          // per-group warp sums (double)
 constexpr uint32_t kSmemBytes = kOffWsum + 2 * 8 * 8;
 constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
@@ -64,11 +66,12 @@ static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0
 static_assert(kUBytes == kFusedUHalves * 2, "gate image size");
 
 // mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
-constexpr uint32_t kBarUFull = 0;  // [2] gate image of buffer b landed (expect_tx)
-constexpr uint32_t kBarTFull = 2;  // [3] block tables of buffer b landed (expect_tx)
-constexpr uint32_t kBarMma = 5;    // [2] MMAs of group g's tile complete (tcgen05.commit)
-constexpr uint32_t kBarDrain = 7;  // [2] group g's MMAs in flight complete (abort path)
-constexpr uint32_t kNumBars = 9;
+constexpr uint32_t kBarUFull = 0;                  // [kUBufs] gate image of buffer b landed (expect_tx)
+constexpr uint32_t kBarTFull = kBarUFull + kUBufs;  // [kTBufs] block tables of buffer b landed (expect_tx)
+constexpr uint32_t kBarMma = kBarTFull + kTBufs;    // [2] MMAs of group g's tile complete (tcgen05.commit)
+constexpr uint32_t kBarDrain = kBarMma + 2;         // [2] group g's MMAs in flight complete (abort path)
+constexpr uint32_t kNumBars = kBarDrain + 2;
+static_assert(kNumBars <= 16, "mbarrier slots");
 
 struct FusedQubits {
     int q[kFusedM];
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
-    __shared__ unsigned s_ucnt[2];            // per gate-image buffer: groups whose MMAs on it completed
+    __shared__ unsigned s_ucnt[kUBufs];       // per gate-image buffer: groups whose MMAs on it completed
     __shared__ unsigned long long s_fetched;  // steps whose copies were issued
     uint64_t* lo_tab = reinterpret_cast<uint64_t*>(sm + kOffTabs);
     uint64_t* hi_tab = lo_tab + 64;
@@ -192,11 +195,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (blockIdx.x < npairs) my_pairs = (npairs - 1 - blockIdx.x) / gridDim.x + 1;
     const uint64_t steps = my_pairs * uint64_t(nblocks);
     const uint32_t u0 = smem_addr(sm + kOffU);
-    // Copies of step st: its block's gate image into buffer st % 2 and its
-    // tables into buffer st % 3.
+    // Copies of step st: its block's gate image into buffer st % kUBufs and
+    // its tables into buffer st % kTBufs.
     auto fetch = [&](uint64_t st) {
         const FusedBlock* blk = blocks + int(st % uint64_t(nblocks));
-        const uint32_t ub = uint32_t(st & 1), tb = uint32_t(st % 3);
+        const uint32_t ub = uint32_t(st % kUBufs), tb = uint32_t(st % kTBufs);
         mbar_expect(bar(kBarUFull + ub), kUBytes);
         bulk_g2s(u0 + ub * kUBytes, upool + blk->u_off, kUBytes, bar(kBarUFull + ub));
         mbar_expect(bar(kBarTFull + tb), kDescBytes);
@@ -219,12 +222,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         // The swizzled operands need 1024-byte aligned atoms.
         s_abort = (smem_addr(sm) & 1023u) != 0;
         if (s_abort) atomicExch(err, 3);
-        s_ucnt[0] = s_ucnt[1] = 0;
+        for (uint32_t i = 0; i < kUBufs; i++) s_ucnt[i] = 0;
         for (uint32_t i = 0; i < kNumBars; i++) mbar_init(bar(i), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         uint64_t f = 0;
         if (!s_abort)
-            for (; f < 2 && f < steps; f++) fetch(f);
+            for (; f < kUBufs && f < steps; f++) fetch(f);
         s_fetched = f;
     }
     if (warp == 0) {
@@ -247,14 +250,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t half = uint32_t(gw >> 2);
     const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 64u * uint32_t(g) + half * 32u;
     const uint64_t desc_x = make_desc_sw128(smem_addr(x));
-    // Prefetch of tile t into this group's raw buffer, natural local order.
+    // Prefetch of tile t into this group's raw buffer, natural local order, 16
+    // bytes per copy (local qubit 0 is global qubit 0: pairs are adjacent).
+    const uint64_t pair_lo = lo_tab[(2 * gt) & 63];
     auto prefetch = [&](uint64_t t) {
         const float2* src = s + tile_base(t, n, fq);
 #pragma unroll
-        for (int k = 0; k < 16; k++)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(raw + (gt + 256u * k) * 8u)),
-                         "l"(src + (glo | hi_tab[row + 4 * k]))
+        for (int k = 0; k < 8; k++) {
+            const uint32_t e = 2u * gt + 512u * k;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(raw + e * 8u)),
+                         "l"(src + (pair_lo | hi_tab[e >> 6]))
                          : "memory");
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     uint32_t mma_cnt = 0;
@@ -300,9 +307,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             group_sync(g);
             bool w = true;
-            const uint32_t ub = uint32_t(st & 1);
+            const uint32_t ub = uint32_t(st % kUBufs);
             if (gt == 0) {
-                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st >> 1) & 1u);
+                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u);
                 if (w) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
                     const uint64_t desc_u = make_desc_sw128(u0 + ub * kUBytes);
@@ -324,23 +331,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 // The rest of the group waits in the vote below, not on the mbarriers.
                 w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u);
-                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % 3)), uint32_t(st / 3) & 1u);
+                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)), uint32_t(st / kTBufs) & 1u);
             }
             mma_cnt++;
             if (!group_all(w, g)) {
                 ok = false;
                 break;
             }
-            if (gt == 0 && st + 2 < steps) {
+            if (gt == 0 && st + kUBufs < steps) {
                 // The gate-image buffer is free once both tiles' MMAs on it completed:
-                // the second group to get here fetches step st + 2 into it.
+                // the second group to get here fetches step st + kUBufs into it.
                 if (!partner || (atomicAdd(&s_ucnt[ub], 1u) & 1u)) {
-                    fetch(st + 2);
-                    atomicMax(&s_fetched, st + 3);
+                    fetch(st + kUBufs);
+                    atomicMax(&s_fetched, st + kUBufs + 1);
                 }
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % 3) * kDescBytes);
+            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % kTBufs) * kDescBytes);
             const uint32_t cpart = nb[32 + col];
             uint32_t nbw[8];  // this half's 16 destination parts, two per word
             {
@@ -407,9 +414,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         // (each issuing thread commits and waits for its own MMAs).
         if (g == 0) {
             const uint64_t fetched = s_fetched;
-            for (uint64_t f = fetched > 3 ? fetched - 3 : 0; f < fetched; f++) {
-                if (f + 2 >= fetched) mbar_wait(bar(kBarUFull + uint32_t(f & 1)), uint32_t(f >> 1) & 1u);
-                mbar_wait(bar(kBarTFull + uint32_t(f % 3)), uint32_t(f / 3) & 1u);
+            for (uint64_t f = fetched > kTBufs ? fetched - kTBufs : 0; f < fetched; f++) {
+                if (f + kUBufs >= fetched) mbar_wait(bar(kBarUFull + uint32_t(f % kUBufs)), uint32_t(f / kUBufs) & 1u);
+                mbar_wait(bar(kBarTFull + uint32_t(f % kTBufs)), uint32_t(f / kTBufs) & 1u);
             }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -480,6 +487,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
     if (b.n < kFusedM || int(p.qubits.size()) != kFusedM) fail(kValueError, "fused passes need 12 tile qubits");
     if (p.nblocks < 1) fail(kValueError, "fused pass without blocks");
+    if (p.qubits[0] != 0 || p.qubits[1] != 1) fail(kValueError, "fused passes hold global qubits 0 and 1");
     FusedQubits fq;
     for (int i = 0; i < kFusedM; i++) fq.q[i] = p.qubits[i];
     for (int e = 0; e < 64; e++) {
