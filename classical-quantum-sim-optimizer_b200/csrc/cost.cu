@@ -204,6 +204,27 @@ void tile_op_features(const TileOp& op, int m, bool c64, float* out) {
     out[15] = float(count) / 5.f;
 }
 
+void fused_block_features(int gates, uint32_t local_mask, int nblocks, float* out) {
+    for (int i = 0; i < F; i++) out[i] = 0.f;
+    int lo = 31, hi = 0;
+    for (int b = 0; b < 32; b++)
+        if ((local_mask >> b) & 1u) {
+            lo = std::min(lo, b);
+            hi = std::max(hi, b);
+        }
+    if (local_mask == 0) lo = hi = 0;
+    out[6] = 1.f;  // width 5: only tensor-core blocks have it
+    out[7] = 1.f / float(std::max(1, nblocks));
+    out[8] = float(std::max(1, gates)) / 16.f;
+    out[9] = float(lo) / 14.f;
+    out[10] = float(hi) / 14.f;
+    out[11] = lo < 3 ? 1.f : 0.f;
+    out[12] = float(kFusedM - 5) / 14.f;
+    out[13] = float(kFusedM) / 14.f;
+    out[14] = 1.f;
+    out[15] = 1.f;
+}
+
 CostModel::CostModel(int device, uint64_t seed) : device_(device) {
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -338,6 +359,17 @@ double CostModel::predict_ops(const std::vector<TileOp>& ops, int m, bool c64) c
     std::vector<float> X(ops.size() * F), y(ops.size());
     for (size_t i = 0; i < ops.size(); i++) tile_op_features(ops[i], m, c64, X.data() + i * F);
     predict(X.data(), ops.size(), y.data());
+    double total = 0;
+    for (float v : y) total += std::exp(double(v));
+    return total;
+}
+
+double CostModel::predict_fused(const FusedPass& p) const {
+    const size_t nb = p.block_gates.size();
+    if (nb == 0) return 0.0;
+    std::vector<float> X(nb * F), y(nb);
+    for (size_t i = 0; i < nb; i++) fused_block_features(p.block_gates[i], p.block_masks[i], int(nb), X.data() + i * F);
+    predict(X.data(), nb, y.data());
     double total = 0;
     for (float v : y) total += std::exp(double(v));
     return total;

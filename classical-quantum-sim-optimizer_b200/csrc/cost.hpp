@@ -1,14 +1,20 @@
 // Learned cost model for the fusion planner.
 //
-// A 16 -> 64 -> 64 -> 1 MLP (ReLU, FP32) predicts the log of the device
-// cycles one tile-local operation costs per tile, from its kind, width, the
-// tile-local positions of its qubits (stride and bank-conflict class), how
-// many gates were fused into it, its work per tile and the tile size.  It is
-// trained on timings the engine records itself (an instrumented tile pass
-// reads clock64() around every operation), by CUDA kernels written here:
-// one CTA runs mini-batch forward, backward and Adam steps; inference is one
-// thread per candidate.  The planner asks it which fusion width makes each
-// pass cheapest; the greedy fixed-width plan stays the fallback and the judge.
+// A 16 -> 64 -> 64 -> 1 MLP (ReLU, FP32) predicts the log of the device time
+// (picoseconds per tile of the pass) one candidate costs: a CUDA-core
+// tile-local operation, from its kind, width, the tile-local positions of its
+// qubits (stride and bank-conflict class), how many gates were fused into it,
+// its work per tile and the tile size; or a 5-qubit tensor-core block, from
+// its qubit positions, gate count and the pass's block count (which carries
+// the pass's load and store).  It is trained on timings the engine records
+// itself: each pass is timed with CUDA events and its time is shared among
+// its operations by their clock64() cycles (an instrumented tile pass reads
+// the clock around every operation) or equally among its blocks.  Training
+// and inference are CUDA kernels written here: one CTA runs mini-batch
+// forward, backward and Adam steps; inference is one thread per candidate.
+// The planner asks it, per pass, which fusion width (CUDA cores) or the
+// tensor-core blocks is cheapest; the greedy plan stays the fallback and the
+// judge.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,6 +35,9 @@ constexpr int kMlpParams = kMlpH * kMlpF + kMlpH + kMlpH * kMlpH + kMlpH + kMlpH
 
 // Features of one tile-local operation in a pass of m tile qubits.
 void tile_op_features(const TileOp& op, int m, bool c64, float* out);
+// Features of one tensor-core block (local qubit mask, fused gates) in a
+// fused pass of `nblocks` blocks.
+void fused_block_features(int gates, uint32_t local_mask, int nblocks, float* out);
 
 class CostModel {
   public:
@@ -41,7 +50,7 @@ class CostModel {
         std::copy(X_.begin(), X_.end(), X);
         std::copy(y_.begin(), y_.end(), y);
     }
-    // Adam on log-cycles; returns the final epoch's mean squared error.
+    // Adam on the log targets; returns the final epoch's mean squared error.
     double train(int epochs, float lr);
     void predict(const float* X, size_t n, float* out) const;
     // Gradients of the mean squared error for one batch (n <= kMlpB), no update.
@@ -49,8 +58,10 @@ class CostModel {
     void get_params(float* out) const;
     void set_params(const float* in);
     bool trained() const { return trained_; }
-    // Sum of predicted cycles of a list of operations (one device call).
+    // Sum of the predicted costs of a list of operations (one device call).
     double predict_ops(const std::vector<TileOp>& ops, int m, bool c64) const;
+    // Sum of the predicted costs of a fused pass's blocks.
+    double predict_fused(const FusedPass& p) const;
     int device() const { return device_; }
 
   private:

@@ -199,11 +199,41 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
         o.pinned_low = kFusedPinned;
         std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
         for (auto& p : ps) {
+            // With a trained cost model each pass runs on whichever executor it
+            // predicts cheapest: tensor-core blocks (0) or CUDA-core tile
+            // operations fused to width 1..kTileMaxDense.
+            int choice = 0;
+            if (cfg_.model) {
+                std::vector<FusedBlock> tb;
+                std::vector<uint16_t> tu;
+                double best = cfg_.model->predict_fused(build_fused_pass(p.raw, p.qubits, tb, tu));
+                for (int w = 1; w <= kTileMaxDense; w++) {
+                    std::vector<double2> scratch;
+                    std::vector<TileOp> cand;
+                    lower_pass_ops(p.raw, p.qubits, cfg_.n, w, scratch, cand);
+                    const double cost = cfg_.model->predict_ops(cand, kFusedM, true);
+                    if (cost < best) {
+                        best = cost;
+                        choice = w;
+                    }
+                }
+            }
+            widths_.push_back(choice);
             Step s;
-            s.fused = int(fused_.size());
             s.type = Operation::Dense;
             s.category = 1;
-            fused_.push_back(build_fused_pass(p.raw, p.qubits, fused_blocks_host_, upool_host_));
+            if (choice == 0) {
+                s.fused = int(fused_.size());
+                fused_.push_back(build_fused_pass(p.raw, p.qubits, fused_blocks_host_, upool_host_));
+                fused_src_.push_back(std::move(p));
+            } else {
+                lower_pass_ops(p.raw, p.qubits, cfg_.n, choice, pool_host_, p.ops);
+                p.raw.clear();
+                p.op_begin = int(tile_ops_host_.size());
+                tile_ops_host_.insert(tile_ops_host_.end(), p.ops.begin(), p.ops.end());
+                s.pass = int(passes_.size());
+                passes_.push_back(std::move(p));
+            }
             steps_.push_back(std::move(s));
         }
         return;
@@ -222,34 +252,94 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
 }
 
 void Executor::record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y) {
-    run(b, nullptr, nullptr);  // uploads the pools; the state it leaves is overwritten below
-    DevMem cyc;
-    size_t most = 1;
-    for (auto& p : passes_) most = std::max(most, p.ops.size());
-    cyc.alloc(most * 8, "cycle counters");
-    std::vector<unsigned long long> host(most);
-    k::init_basis(b);
+    run(b, nullptr, nullptr);  // uploads the pools; the state it leaves is reused below
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    // Device milliseconds of one launch sequence (the faster of two runs).
+    auto time_ms = [&](auto&& launch) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            cuda_check(cudaEventRecord(e0, b.stream), "cudaEventRecord");
+            launch();
+            cuda_check(cudaEventRecord(e1, b.stream), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            best = std::min(best, ms);
+        }
+        return double(best);
+    };
+    DevMem cyc, tops, tpool;
+    std::vector<unsigned long long> host;
+    // One CUDA-core pass: its event time shared among its operations by cycles.
+    auto record_tile = [&](const TilePass& p, const TileOp* ops_dev, const double2* pool_dev,
+                           const std::vector<TileOp>& ops_host) {
+        if (ops_host.empty()) return;
+        const int m = int(p.qubits.size());
+        const int nops = int(ops_host.size());
+        const double tiles = double(b.W << (b.n - m));
+        const double ms = time_ms([&] { k::tile_pass(b, nullptr, m, ops_dev, nops, pool_dev, p, nullptr); });
+        cyc.ensure(size_t(nops) * 8, "cycle counters");
+        cuda_check(cudaMemsetAsync(cyc.p, 0, size_t(nops) * 8, b.stream), "clear cycle counters");
+        k::tile_pass(b, nullptr, m, ops_dev, nops, pool_dev, p, cyc.as<unsigned long long>());
+        host.resize(size_t(nops));
+        cuda_check(cudaMemcpyAsync(host.data(), cyc.p, size_t(nops) * 8, cudaMemcpyDeviceToHost, b.stream), "read");
+        cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
+        double total = 0;
+        for (auto c : host) total += double(std::max<unsigned long long>(c, 1));
+        for (int i = 0; i < nops; i++) {
+            float f[kMlpF];
+            tile_op_features(ops_host[size_t(i)], m, b.c64, f);
+            X.insert(X.end(), f, f + kMlpF);
+            const double share = double(std::max<unsigned long long>(host[size_t(i)], 1)) / total;
+            y.push_back(float(std::log(std::max(1.0, ms * 1e9 / tiles * share))));
+        }
+    };
     for (size_t si = 0; si < steps_.size(); si++) {
         const Step& s = steps_[si];
-        if (s.pass < 0) {
-            // Non-pass steps keep the state evolving as in a normal run.
-            continue;
-        }
-        const TilePass& p = passes_[size_t(s.pass)];
-        const int m = int(p.qubits.size());
-        cuda_check(cudaMemsetAsync(cyc.p, 0, p.ops.size() * 8, b.stream), "clear cycle counters");
-        k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()), pool_.as<double2>(), p,
-                     cyc.as<unsigned long long>());
-        cuda_check(cudaMemcpyAsync(host.data(), cyc.p, p.ops.size() * 8, cudaMemcpyDeviceToHost, b.stream), "read");
-        cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
-        const double tiles = double(b.W << (b.n - m));
-        for (size_t i = 0; i < p.ops.size(); i++) {
-            float f[kMlpF];
-            tile_op_features(p.ops[i], m, b.c64, f);
-            X.insert(X.end(), f, f + kMlpF);
-            y.push_back(float(std::log(std::max(1.0, double(host[i]) / tiles))));
+        if (s.pass >= 0) {
+            const TilePass& p = passes_[size_t(s.pass)];
+            record_tile(p, tile_ops_.as<TileOp>() + p.op_begin, pool_.as<double2>(), p.ops);
+        } else if (s.fused >= 0) {
+            const FusedPass& fp = fused_[size_t(s.fused)];
+            const double tiles = double(b.W << (b.n - kFusedM));
+            norm_tiles_.ensure(size_t(tiles) * 8, "fused tile norms");
+            const double ms = time_ms([&] {
+                k::fused_pass(b, fp, fused_blocks_.as<FusedBlock>(), upool_.as<uint16_t>(), b.err, nullptr,
+                              norm_tiles_.as<double>());
+            });
+            for (int j = 0; j < fp.nblocks; j++) {
+                float f[kMlpF];
+                fused_block_features(fp.block_gates[size_t(j)], fp.block_masks[size_t(j)], fp.nblocks, f);
+                X.insert(X.end(), f, f + kMlpF);
+                y.push_back(float(std::log(std::max(1.0, ms * 1e9 / tiles / fp.nblocks))));
+            }
+            // The same pass on CUDA cores at each fusion width.
+            const TilePass& src = fused_src_[size_t(s.fused)];
+            for (int w = 1; w <= kTileMaxDense; w++) {
+                std::vector<double2> pool;
+                std::vector<TileOp> ops;
+                lower_pass_ops(src.raw, src.qubits, b.n, w, pool, ops);
+                if (ops.empty()) continue;
+                tops.ensure(ops.size() * sizeof(TileOp), "tile operations");
+                tpool.ensure(std::max<size_t>(pool.size(), 1) * sizeof(double2), "gate matrices");
+                cuda_check(cudaMemcpyAsync(tops.p, ops.data(), ops.size() * sizeof(TileOp), cudaMemcpyHostToDevice,
+                                           b.stream),
+                           "upload tile operations");
+                if (!pool.empty())
+                    cuda_check(cudaMemcpyAsync(tpool.p, pool.data(), pool.size() * sizeof(double2),
+                                               cudaMemcpyHostToDevice, b.stream),
+                               "upload gate matrices");
+                record_tile(src, tops.as<TileOp>(), tpool.as<double2>(), ops);
+            }
         }
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // The timed passes left the state arbitrary and its norm unchecked.
+    cuda_check(cudaMemsetAsync(b.err, 0, 16, b.stream), "clear error flag");
+    cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
 }
 
 size_t Executor::raw_ops_in_passes() const {

@@ -130,8 +130,11 @@ class Executor {
     size_t raw_ops_in_passes() const;
     const std::vector<int>& chosen_widths() const { return widths_; }
     size_t tile_ops() const { return tile_ops_host_.size(); }
-    // Runs every step once, timing each tile-local operation of every pass
-    // (clock64 cycles per tile), and appends (features, log cycles) samples.
+    // Times every pass (CUDA events), shares each pass's time among its
+    // operations by their clock64 cycles or equally among its tensor-core
+    // blocks, and appends (features, log picoseconds per tile) samples.  Fused
+    // passes are also timed on CUDA cores at each fusion width, so that the
+    // planner can compare the two executors pass by pass.
     void record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y);
 
   private:
@@ -155,6 +158,7 @@ class Executor {
     std::vector<TilePass> passes_;
     std::vector<TileOp> tile_ops_host_;
     std::vector<FusedPass> fused_;
+    std::vector<TilePass> fused_src_;  // each fused pass's tile qubits and raw operations
     std::vector<FusedBlock> fused_blocks_host_;
     std::vector<uint16_t> upool_host_;
     DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_;

@@ -101,7 +101,9 @@ ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate, const 
     c.tiled = !force_per_gate && o.execution != 1;
     c.tile_m = o.tile_qubits > 0 ? o.tile_qubits : (c.c64 ? 13 : 12);
     c.fuse = o.fusion_width > 0 ? o.fusion_width : 2;
-    c.fused = c.c64 && c.tiled && o.fusion_width == 5;
+    // complex64 runs its tile passes as fused 5-qubit tensor-core blocks unless a
+    // CUDA-core tile shape or a narrower fusion width is asked for.
+    c.fused = c.c64 && c.tiled && (o.fusion_width == 5 || (o.fusion_width == 0 && o.tile_qubits == 0));
     c.n = int(n);
     return c;
 }

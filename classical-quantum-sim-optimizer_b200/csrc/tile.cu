@@ -260,6 +260,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
     struct Blk {
         int q[5];
         std::vector<cplx> u;
+        int gates = 0;
     };
     std::vector<Blk> blk;
     for (const Operation& op : fuse_ops(pass_ops, 5)) {
@@ -277,6 +278,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         Blk b;
         for (int t = 0; t < 5; t++) b.q[t] = local[bq[t]];
         b.u = std::move(acc);
+        b.gates = std::max(1, op.fused_count);
         blk.push_back(std::move(b));
     }
     if (blk.empty()) {  // a pass of nothing but identities: one identity block
@@ -463,6 +465,12 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         blocks.push_back(d);
     }
     fp.nblocks = int(blk.size());
+    for (const Blk& b : blk) {
+        uint32_t mask = 0;
+        for (int t = 0; t < 5; t++) mask |= 1u << b.q[t];
+        fp.block_gates.push_back(b.gates);
+        fp.block_masks.push_back(mask);
+    }
     return fp;
 }
 
@@ -660,6 +668,13 @@ TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::ve
 }
 
 }  // namespace
+
+void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,
+                    std::vector<double2>& pool, std::vector<TileOp>& out) {
+    std::vector<int> local(size_t(n), -1);
+    for (size_t i = 0; i < tile_qubits.size(); i++) local[size_t(tile_qubits[i])] = int(i);
+    for (auto& op : fuse_ops(raw, width)) lower_tile_op(op, local, pool, out);
+}
 
 std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
                                  const TilePlanOptions& opt, std::vector<double2>* pool) {

@@ -112,7 +112,14 @@ struct FusedPass {
     uint16_t in_lo[64], in_hi[64];    // natural local index l -> operand offset of block 0 (lo ^ hi)
     uint16_t out_lo[64], out_hi[64];  // natural local index l -> stage offset (lo ^ hi)
     int raw_ops = 0;
+    std::vector<int> block_gates;        // gates fused into each block
+    std::vector<uint32_t> block_masks;   // each block's local qubits
 };
+
+// A pass's raw operations fused to `width` and lowered to tile-local
+// operations for the CUDA-core tile kernel (matrices appended to `pool`).
+void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,
+                    std::vector<double2>& pool, std::vector<TileOp>& out);
 
 // Fuses a pass's operations into 5-qubit blocks and appends their descriptors
 // and f16 hi/lo gate images (K-major, 128-byte swizzled operand layout).
