@@ -1,4 +1,4 @@
-"""Benchmark: 30-qubit depth-40 random brickwork, plain complex128 vs complex64 form.
+"""Benchmark: 30-qubit depth-40 random brickwork, plain complex128 vs the fused complex64 form.
 
 One step = one full circuit on one GPU: |0...0>, every compiled operation,
 FP64 terminal probabilities, CDF and 10^5 seeded samples, with the circuit
@@ -6,15 +6,24 @@ plan and state buffers resident in HBM (dq_plan_*).  Each form is timed with
 CUDA events on the engine's stream.  The 16 GiB / 8 GiB state is far larger
 than the 126 MB L2, so no flush is needed between steps.
 
-`value` is the circuit time of the complex64 form (seconds per circuit; for
-N GPUs, replicas: N circuits / max-over-ranks time, reported as seconds per
-circuit).  The plain complex128 time, both forms' algorithmic HBM GB/s, and the
-complex64 state's fidelity / max amplitude error against the complex128 run
-are reported beside it.
+`value` is the circuit time of the chosen complex64 form (fused 5-qubit blocks
+on tcgen05 tensor cores; seconds per circuit; for N GPUs, replicas: N circuits
+/ max-over-ranks time, reported as seconds per circuit).  The plain complex128
+per-gate form (its per-pass HBM fraction), complex128 shared-memory tiles,
+complex64 CUDA-core tiles, the algorithmic GB/s of each and every complex64
+state's fidelity / max amplitude error against the plain run are reported
+beside it.  The roofline is the fused kernel's tensor-pipe throughput (f16
+FLOPs it issues: three 128x64x64 products per block and tile).
 
 --impl reference times the CPU restatement of the reference's engine
 (oracle/, OpenMP on every host core) on a bounded sample of the same circuit:
 the first operations at 30 qubits, scaled by operation count.
+
+--workload selects the other measured configurations (their own JSON line):
+qft (32-qubit QFT, complex64 fused vs complex128 plain), batch (512 uneven HEA
+circuits in one persistent launch vs a per-circuit complex128 loop) and
+learned (cost model trained on recorded timings; learned vs greedy plans on
+held-out 26/30/33-qubit brickwork).
 """
 
 import argparse
@@ -35,6 +44,7 @@ for _p in (str(PKG), str(ROOT)):
 
 METRIC = "30q circuit time & HBM GB/s: fused FP32 vs plain FP64 at fidelity≥1−1e-6"
 FALLBACK_HBM = 6650.0
+FALLBACK_TFLOPS = 1590.0
 
 
 def peaks():
@@ -43,6 +53,21 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d.get("hbm_gbs", FALLBACK_HBM)), "measured"
     return FALLBACK_HBM, "fallback"
+
+
+def tensor_peak():
+    """Dense f16/bf16 tensor peak (TFLOP/s): the measured burst cuBLAS bf16 figure."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    return FALLBACK_TFLOPS, FALLBACK_TFLOPS, "fallback"
+
+
+# f16 tensor FLOPs one fused block issues per 4096-amplitude tile: hi*hi, hi*lo
+# and lo*hi products of the 128 x 64 operand with the 64 x 64 real gate image.
+FUSED_FLOPS_PER_TILE_BLOCK = 3 * 2 * 128 * 64 * 64
 
 
 class ClockSampler:
@@ -133,9 +158,9 @@ def max_over_ranks(pg, local, value):
     return float(t.item())
 
 
-def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed, execution="auto"):
+def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed, execution="auto", **kw):
     sim = dqsim.StatevectorSimulator(seed=seed, max_memory_mb=1 << 20, precision=precision, device=local,
-                                     execution=execution)
+                                     execution=execution, **kw)
     plan = dqsim._core.PreparedCircuit(sim, circuit, shots=shots)
     for _ in range(warmup):
         plan.run()
@@ -204,12 +229,37 @@ def workload_config(args):
             "parallelism": "replicas", "l2": "state (16 GiB c128 / 8 GiB c64) exceeds L2; no flush"}
 
 
+def bytes_of(stats):
+    return sum(v["bytes"] for k, v in stats.items() if k != "sample")
+
+
+def summarize(stats, ms_, peak):
+    gbs = bytes_of(stats) / (ms_ * 1e-3) / 1e9
+    return {"s": ms_ * 1e-3, "gbs": gbs, "frac_of_hbm": gbs / peak, "kernels": stats}
+
+
+def fused_roofline(plan, stats, n):
+    """Tensor-pipe roofline of the fused kernel class from the plan's block count."""
+    fused = stats.get("fused")
+    if not fused or fused["ms"] <= 0:
+        return None
+    tiles = 1 << (n - 12)
+    flops = tiles * plan.shape()["fused_blocks"] * FUSED_FLOPS_PER_TILE_BLOCK
+    burst, sustained, kind = tensor_peak()
+    achieved = flops / (fused["ms"] * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": "k_fused (tcgen05 kind::f16)", "achieved": achieved, "peak": burst,
+            "unit": "TFLOP/s", "frac": achieved / burst, "frac_of_sustained": achieved / sustained,
+            "peak_kind": kind, "flops": flops, "launches": fused["launches"],
+            "hbm_gbs": fused["bytes"] / (fused["ms"] * 1e-3) / 1e9, "traffic": None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="brickwork", choices=["brickwork", "qft", "batch", "learned"])
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--shots", type=int, default=100000)
@@ -220,19 +270,14 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "brickwork":
+        return {"qft": run_qft, "batch": run_batch, "learned": run_learned}[args.workload](args)
 
     world, rank, local, pg = dist_setup(args)
     import dqsim
 
     peak, peak_kind = peaks()
     circuit = dqsim.workloads.brickwork(args.qubits, args.depth, seed=args.seed, measure=True)
-
-    def bytes_of(stats):
-        return sum(v["bytes"] for k, v in stats.items() if k != "sample")
-
-    def summarize(stats, ms_):
-        gbs = bytes_of(stats) / (ms_ * 1e-3) / 1e9
-        return {"s": ms_ * 1e-3, "gbs": gbs, "frac_of_hbm": gbs / peak, "kernels": stats}
 
     # Plain complex128 form: the reference's arithmetic, one HBM pass per operation.
     sim128, plan128 = time_form(dqsim, circuit, "complex128", local, 1, 0, args.shots, args.seed,
@@ -257,7 +302,17 @@ def main():
     tiled_fid, tiled_err = plant.compare(plan128)
     del plant, simt
 
-    # Complex64 form (the chosen form).
+    # complex64 on CUDA cores (13-qubit tiles, width-2 fusion).
+    simc, planc = time_form(dqsim, circuit, "complex64", local, 1, 1, args.shots, args.seed,
+                            tile_qubits=13, fusion_width=2)
+    tc = [planc.run() for _ in range(args.plain_steps)]
+    planc.run(record=True)
+    stc = planc.stats()
+    msc = statistics.mean(tc)
+    cc_fid, cc_err = planc.compare(plan128)
+    del planc, simc
+
+    # The chosen form: complex64 with fused 5-qubit blocks on tensor cores.
     sim64, plan64 = time_form(dqsim, circuit, "complex64", local, 1, args.warmup, args.shots, args.seed)
     barrier(pg)
     with ClockSampler(local) as clocks:
@@ -267,23 +322,19 @@ def main():
     plan64.run(record=True)
     st64 = plan64.stats()
     fidelity, max_err = plan64.compare(plan128)
+    shape64 = plan64.shape()
+    roof = fused_roofline(plan64, st64, args.qubits)
     del plan128, sim128
 
-    gb64 = bytes_of(st64) / (ms * 1e-3) / 1e9
-    dom = max(st64.items(), key=lambda kv: kv[1]["ms"])
-    dom_achieved = dom[1]["bytes"] / (dom[1]["ms"] * 1e-3) / 1e9
-
     # End to end through the public API: host JSON in, host counts out.
-    e2e = None
-    if True:
-        api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64", device=local)
-        api.simulate_shots(circuit, shots=args.shots)
-        t0 = time.perf_counter()
-        counts = api.simulate_shots(circuit, shots=args.shots)
-        e2e_s = time.perf_counter() - t0
-        assert sum(counts.values()) == args.shots
-        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": len(circuit.model_dump_json()),
-               "d2h_bytes_per_step": 8 * args.shots}
+    api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64", device=local)
+    api.simulate_shots(circuit, shots=args.shots)
+    t0 = time.perf_counter()
+    counts = api.simulate_shots(circuit, shots=args.shots)
+    e2e_s = time.perf_counter() - t0
+    assert sum(counts.values()) == args.shots
+    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": len(circuit.model_dump_json()),
+           "d2h_bytes_per_step": 8 * args.shots}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -297,16 +348,19 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 (f32, FP64 reductions)", "data": "synthetic",
-        "config": workload_config(args),
+        "vs_baseline": None, "dtype": "c64 (f16x3 tensor products, f32 accumulate, FP64 reductions)",
+        "data": "synthetic", "config": workload_config(args),
         "forms": {
-            "complex64": {**summarize(st64, ms), "fidelity": fidelity, "max_amp_err": max_err},
-            "complex128_per_gate": {**summarize(st128, ms128), "dominant": plain_kernel},
-            "complex128_tiled": {**summarize(stt, mst), "fidelity": tiled_fid, "max_amp_err": tiled_err},
-            "speedup_c64_vs_plain": ms128 / ms,
+            "complex64_fused": {**summarize(st64, ms, peak), "fidelity": fidelity, "max_amp_err": max_err,
+                                "passes": shape64["passes"], "fused_blocks": shape64["fused_blocks"]},
+            "complex64_cuda_core": {**summarize(stc, msc, peak), "fidelity": cc_fid, "max_amp_err": cc_err},
+            "complex128_per_gate": {**summarize(st128, ms128, peak), "dominant": plain_kernel},
+            "complex128_tiled": {**summarize(stt, mst, peak), "fidelity": tiled_fid, "max_amp_err": tiled_err},
+            "speedup_fused_vs_plain": ms128 / ms,
+            "speedup_fused_vs_c64_cuda_core": msc / ms,
         },
-        "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
-                     "frac": dom_achieved / peak, "peak_kind": peak_kind, "traffic": None},
+        "roofline": roof,
+        "hbm_peak": {"value": peak, "kind": peak_kind},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
@@ -316,6 +370,110 @@ def main():
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
+    return 0
+
+
+def run_qft(args):
+    """32-qubit QFT: complex64 fused (32 GiB) vs complex128 per-gate (64 GiB), time and fidelity."""
+    import dqsim
+
+    n = args.qubits if args.qubits != 30 else 32
+    circuit = dqsim.workloads.qft(n, seed=args.seed)
+    _, plan128 = time_form(dqsim, circuit, "complex128", 0, 1, 0, 0, args.seed, execution="per_gate")
+    t128 = [plan128.run() for _ in range(max(1, args.plain_steps))]
+    sim64, plan64 = time_form(dqsim, circuit, "complex64", 0, 1, 1, 0, args.seed)
+    t64 = [plan64.run() for _ in range(args.steps)]
+    plan64.run(record=True)
+    st64 = plan64.stats()
+    fid, err = plan64.compare(plan128)
+    print(json.dumps({"workload": f"qft-{n}q-seed{args.seed}", "complex64_fused_s": statistics.mean(t64) * 1e-3,
+                      "complex128_per_gate_s": statistics.mean(t128) * 1e-3,
+                      "speedup": statistics.mean(t128) / statistics.mean(t64), "fidelity": fid, "max_amp_err": err,
+                      "shape": plan64.shape(), "roofline": fused_roofline(plan64, st64, n),
+                      "state_gib": {"complex64": (8 << n) / 2 ** 30, "complex128": (16 << n) / 2 ** 30}}))
+    return 0
+
+
+def run_batch(args):
+    """512 uneven HEA circuits (12..22 qubits, depth 4..16), 1024 shots and <Z0 Z1> each, in one
+    persistent launch under a CUDA graph, vs a per-circuit complex128 per-gate loop."""
+    import numpy as np
+
+    import dqsim
+
+    circuits = dqsim.workloads.hea_batch(512, seed=args.seed)
+    sim = dqsim.StatevectorSimulator(seed=args.seed, precision="complex64", max_memory_mb=1 << 16)
+    t0 = time.perf_counter()
+    batch = dqsim._core.BatchedCircuits(sim, circuits, shots=1024, autotune=True)
+    setup_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        batch.run()
+    ms = [batch.run() for _ in range(args.steps)]
+    zz = batch.expect_zz()
+    sim128 = dqsim.StatevectorSimulator(seed=args.seed, precision="complex128", max_memory_mb=1 << 16,
+                                        execution="per_gate")
+    loop_ms, zz_err = 0.0, 0.0
+    t1 = time.perf_counter()
+    for i, c in enumerate(circuits):
+        plan = dqsim._core.PreparedCircuit(sim128, c, shots=1024)
+        loop_ms += plan.run()
+        if i < 16:  # <Z0 Z1> of the complex128 state for a spot check
+            sv = plan.statevector()
+            p = np.abs(sv) ** 2
+            idx = np.arange(p.shape[0])
+            sign = 1 - 2 * (((idx >> 0) & 1) ^ ((idx >> 1) & 1))
+            zz_err = max(zz_err, abs(float(np.dot(p, sign)) - float(zz[i])))
+        del plan
+    loop_wall = time.perf_counter() - t1
+    print(json.dumps({"workload": f"hea-batch-512-seed{args.seed}", "batch_ms": statistics.mean(ms),
+                      "batch_setup_s": setup_s, "passes": batch.passes, "work_items": batch.items,
+                      "per_circuit_c128_device_ms": loop_ms, "per_circuit_c128_wall_s": loop_wall,
+                      "speedup_device": loop_ms / statistics.mean(ms), "zz_max_err_first16": zz_err}))
+    return 0
+
+
+def run_learned(args):
+    """Cost model trained on this engine's recorded timings (brickwork and QFT, 24..30 qubits),
+    then learned vs greedy plans on held-out depth-40 brickwork at 26, 30 and 33 qubits."""
+    import dqsim
+    from dqsim import _core
+
+    model = _core.CostModel(seed=args.seed)
+    rec = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
+    t0 = time.perf_counter()
+    for n in (24, 26, 28, 30):
+        for s in range(2):
+            model.record(rec, dqsim.workloads.brickwork(n, 40, seed=1000 + 10 * n + s, measure=False))
+        model.record(rec, dqsim.workloads.qft(n, seed=2000 + n))
+    record_s = time.perf_counter() - t0
+    samples = model.num_samples
+    mse = model.train(epochs=60, lr=2e-3)
+    results = []
+    for n in (26, 30, 33):
+        circuit = dqsim.workloads.brickwork(n, 40, seed=9000 + n, measure=False)
+        sim = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
+        _core.set_cost_model(sim, model)
+        learned = _core.PreparedCircuit(sim, circuit)
+        info = learned.planner()
+        log = _core.planner_log(sim)[-1]
+        greedy_sim = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
+        greedy = _core.PreparedCircuit(greedy_sim, circuit)
+        tl = min(learned.run() for _ in range(2))
+        tg = min(greedy.run() for _ in range(2))
+        fid, err = learned.compare(greedy)
+        row = {"qubits": n, "greedy_ms": tg, "kept_ms": tl, "ab_greedy_ms": info["greedy_ms"],
+               "ab_learned_ms": info["learned_ms"], "rejected": info["rejected"],
+               "per_pass_choice": log.get("widths"), "fidelity_vs_greedy": fid, "max_amp_err_vs_greedy": err}
+        if n <= 30:
+            _, ref = time_form(dqsim, circuit, "complex128", 0, 1, 0, 0, 1)
+            row["fidelity_vs_c128"] = learned.compare(ref)[0]
+            del ref
+        results.append(row)
+        _core.set_cost_model(sim, None)
+        del learned, greedy
+    print(json.dumps({"workload": "learned-vs-greedy", "samples": samples, "record_s": record_s,
+                      "train_mse": mse, "results": results,
+                      "rejection_rate": sum(r["rejected"] for r in results) / len(results)}))
     return 0
 
 
