@@ -68,6 +68,9 @@ def tensor_peak():
 # f16 tensor FLOPs one fused block issues per 4096-amplitude tile: hi*hi, hi*lo
 # and lo*hi products of the 128 x 64 operand with the 64 x 64 real gate image.
 FUSED_FLOPS_PER_TILE_BLOCK = 3 * 2 * 128 * 64 * 64
+# DRAM bytes (read + write) per tile of one k_fused launch, from the ncu capture
+# of a 25-qubit pass (483.8 MB over 8192 tiles; traffic grows with the tiles).
+FUSED_TRAFFIC_PER_TILE = 483.76e6 / 8192
 
 
 class ClockSampler:
@@ -250,7 +253,9 @@ def fused_roofline(plan, stats, n):
     return {"bound": "tensor", "kernel": "k_fused (tcgen05 kind::f16)", "achieved": achieved, "peak": burst,
             "unit": "TFLOP/s", "frac": achieved / burst, "frac_of_sustained": achieved / sustained,
             "peak_kind": kind, "flops": flops, "launches": fused["launches"],
-            "hbm_gbs": fused["bytes"] / (fused["ms"] * 1e-3) / 1e9, "traffic": None}
+            "hbm_gbs": fused["bytes"] / (fused["ms"] * 1e-3) / 1e9,
+            "traffic": FUSED_TRAFFIC_PER_TILE * tiles, "traffic_unit": "bytes per launch (scaled from 25 qubits)",
+            "algorithmic_bytes_per_launch": 16.0 * tiles * 4096}
 
 
 def main():
