@@ -43,7 +43,7 @@ namespace {
 
 constexpr int kGroupThreads = 256;                       // one group (8 warps)
 constexpr int kThreads = 2 * kGroupThreads;              // two groups
-constexpr uint32_t kTmemCols = 128;                      // one 64-column accumulator per group
+constexpr uint32_t kTmemCols = 256;                      // one 128-column accumulator per group
 constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part of a tile (4096 x 4 B)
 constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
 constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
@@ -96,8 +96,14 @@ __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
     return d;
 }
 
-// kind::f16 instruction descriptor: D FP32, A/B F16, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16 instruction descriptors: D FP32, A/B F16, both K-major, M = 128,
+// N = 128 (A_hi against [U_hi; U_lo]) and N = 64 (A_lo against U_hi).
+constexpr uint32_t kIdescN128 = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdescN64 = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// Fixed power-of-two scale of the operands: states are normalised, so every
+// amplitude and every output of a unitary block is at most 1 in magnitude and
+// 2^13 of it stays inside f16 range; values down to 2^-27 keep full precision.
+constexpr float kScale = 8192.f, kInvScale = 1.f / 8192.f;
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
@@ -243,16 +249,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int g = warp >> 3, gw = warp & 7, gt = tid & (kGroupThreads - 1);
     unsigned char* x = sm + uint32_t(g) * kTileBytes;
     unsigned char* raw = sm + kOffRaw + uint32_t(g) * kTileBytes;
-    const uint32_t row = uint32_t(gt >> 6);  // this thread's elements: l = (gt & 63) | (row + 4k) << 6
+    const uint32_t row = uint32_t(gt >> 6);  // store phase: elements l = (gt & 63) | (row + 4k) << 6
     const uint64_t glo = lo_tab[gt & 63];
-    const uint32_t plo = io[gt & 63], olo = io[128 + (gt & 63)];
+    const uint32_t olo = io[128 + (gt & 63)];
     const uint32_t col = uint32_t((gw & 3) * 32 + lane);
     const uint32_t half = uint32_t(gw >> 2);
-    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 64u * uint32_t(g) + half * 32u;
+    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 128u * uint32_t(g) + half * 32u;
     const uint64_t desc_x = make_desc_sw128(smem_addr(x));
     // Prefetch of tile t into this group's raw buffer, natural local order, 16
     // bytes per copy (local qubit 0 is global qubit 0: pairs are adjacent).
     const uint64_t pair_lo = lo_tab[(2 * gt) & 63];
+    const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
+    const uint32_t pair_row = uint32_t((2 * gt) >> 6);  // the pairs are (e, e+1), e = 2*gt + 512k
+    double scale = 1.0;
+    uint64_t scale_state = ~uint64_t(0);
     auto prefetch = [&](uint64_t t) {
         const float2* src = s + tile_base(t, n, fq);
 #pragma unroll
@@ -275,31 +285,25 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint64_t base = tile_base(t, n, fq);
         // FP64 renormalisation of the previous pass (tensor-core accumulation
         // rounds toward zero, so unitary blocks shrink the norm slightly).
-        const double scale = in_norm ? 1.0 / sqrt(in_norm[base >> n]) : 1.0;
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        group_sync(g);
-        float2 v[16];
-        float part = 0.f;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            const float2 r = *reinterpret_cast<const float2*>(raw + (gt + 256u * k) * 8u);
-            v[k] = make_float2(float(double(r.x) * scale), float(double(r.y) * scale));
-            part += v[k].x * v[k].x + v[k].y * v[k].y;
+        if (in_norm && (base >> n) != scale_state) {
+            scale_state = base >> n;
+            scale = 1.0 / sqrt(in_norm[scale_state]);
         }
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-        if (lane == 0) wsum[g * 8 + gw] = double(part);
-        group_sync(g);  // raw read and partial norms written
+        // Each thread reads back exactly the pairs its own cp.async brought
+        // in, so no barrier is needed before it prefetches the next tile.
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        float4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = *reinterpret_cast<const float4*>(raw + (2u * gt + 512u * k) * 8u);
         if (pair + gridDim.x < npairs && 2 * (pair + gridDim.x) + uint64_t(g) < total_tiles)
             prefetch(2 * (pair + gridDim.x) + uint64_t(g));
-        // Power-of-two scale putting the tile norm in [2^13, 2^14).
-        float m2 = 0.f;
-        for (int w2 = 0; w2 < 8; w2++) m2 += float(wsum[g * 8 + w2]);
-        int em = -100;
-        if (m2 > 1e-30f) em = ((__float_as_int(sqrtf(m2)) >> 23) & 0xFF) - 127;
-        const int e = min(max(13 - em, -120), 120);
-        const float sc = __int_as_float((127 + e) << 23), inv_sc = __int_as_float((127 - e) << 23);
+        const double ds = scale * double(kScale);
 #pragma unroll
-        for (int k = 0; k < 16; k++) put_split(x, plo ^ io[64 + row + 4 * k], v[k].x * sc, v[k].y * sc);
+        for (int k = 0; k < 8; k++) {
+            const uint32_t hi_part = io[64 + pair_row + 8 * k];
+            put_split(x, pair_even ^ hi_part, float(double(v[k].x) * ds), float(double(v[k].y) * ds));
+            put_split(x, pair_odd ^ hi_part, float(double(v[k].z) * ds), float(double(v[k].w) * ds));
+        }
         double norm_acc = 0.0;
         for (int j = 0; j < nblocks; j++, st++) {
             // Operand of step st written: one thread issues its MMAs.
@@ -314,16 +318,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                     asm volatile("tcgen05.fence::after_thread_sync;");
                     const uint64_t desc_u = make_desc_sw128(u0 + ub * kUBytes);
                     // Descriptors advance by (byte offset >> 4) in their start-address field.
+                    // A_hi x [U_hi; U_lo] (N = 128: columns 0..63 hi*hi, 64..127 hi*lo),
+                    // then A_lo x U_hi accumulated into columns 0..63.
 #pragma unroll
-                    for (int q = 0; q < 12; q++) {
-                        const int part3 = q >> 2, ks = q & 3;
-                        const uint64_t ad = desc_x + (part3 == 2 ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
-                        const uint64_t bd = desc_u + (part3 == 1 ? uint64_t((kUBytes / 2) >> 4) : 0) + uint64_t(ks * 2);
+                    for (int q = 0; q < 8; q++) {
+                        const int ks = q & 3;
+                        const bool lo = q >= 4;
+                        const uint64_t ad = desc_x + (lo ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
+                        const uint64_t bd = desc_u + uint64_t(ks * 2);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 64u * g),
-                            "l"(ad), "l"(bd), "r"(kIdesc), "r"(q > 0 ? 1u : 0u));
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 128u * g),
+                            "l"(ad), "l"(bd), "r"(lo ? kIdescN64 : kIdescN128), "r"(q > 0 ? 1u : 0u));
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                         bar(kBarMma + g))
@@ -356,31 +363,43 @@ __global__ void __launch_bounds__(kThreads, 1)
                 nbw[0] = w0.x, nbw[1] = w0.y, nbw[2] = w0.z, nbw[3] = w0.w;
                 nbw[4] = w1.x, nbw[5] = w1.y, nbw[6] = w1.z, nbw[7] = w1.w;
             }
-            uint32_t r[32];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                "[%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (j + 1 < nblocks) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                    put_split(x, off, __uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
-                }
-            } else {
+            for (int h = 0; h < 2; h++) {
+                // Columns 16h.. of this half: hi*hi + lo*hi, and hi*lo 64 columns on.
+                uint32_t r[16], q[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(taddr + 16u * h));
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+                      "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]),
+                      "=r"(q[15])
+                    : "r"(taddr + 64u + 16u * h));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (j + 1 < nblocks) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                    const float re = __uint_as_float(r[2 * i]) * inv_sc, im = __uint_as_float(r[2 * i + 1]) * inv_sc;
-                    *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
-                    norm_acc += double(re) * re + double(im) * im;
+                    for (int i = 0; i < 8; i++) {
+                        const int o = 8 * h + i;
+                        const uint32_t off = cpart ^ ((nbw[o >> 1] >> (16 * (o & 1))) & 0xFFFFu);
+                        put_split(x, off, __uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i]),
+                                  __uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1]));
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int o = 8 * h + i;
+                        const uint32_t off = cpart ^ ((nbw[o >> 1] >> (16 * (o & 1))) & 0xFFFFu);
+                        const float re = (__uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i])) * kInvScale;
+                        const float im = (__uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1])) * kInvScale;
+                        *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
+                        norm_acc += double(re) * re + double(im) * im;
+                    }
                 }
             }
         }
@@ -393,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             gp[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + row + 4 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
-        group_sync(g);  // stage read; the scale partials are consumed
+        group_sync(g);  // stage read
         if (lane == 0) wsum[g * 8 + gw] = norm_acc;
         group_sync(g);
         if (gt == 0) {

@@ -309,7 +309,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
     // complex entries (f16 re, im), so the bank of a store has bits (b0, b1,
     // b2^c0, b3^c1, b4^c2) of the block's basis (b) and column (c) index.
     // Across a warp, the readback of block j-1 varies the five qubits of its
-    // column bits 0..4 (its TMEM lanes; local qubits 0..4 for the tile load).
+    // column bits 0..4 (its TMEM lanes; local qubits 1..5 for the tile load).
     // Block j's basis and column bit order is chosen greedily so that those
     // five qubits reach five independent bank bits (one wavefront per warp):
     // lane qubits of the block at basis bits 0 and 1, lane qubits outside it
@@ -318,7 +318,9 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
     // bits 0 and 1).
     const size_t J = blk.size();
     std::vector<std::vector<int>> oth(J);
-    uint32_t lanes = 0x1Fu;  // qubits varying across a warp of the incoming stores
+    // Qubits varying across a warp of the incoming stores: the tile load stores
+    // pairs (l, l+1), so a warp's stores of one parity vary local qubits 1..5.
+    uint32_t lanes = 0x3Eu;
     for (size_t j = 0; j < J; j++) {
         Blk& bj = blk[j];
         uint32_t bmask = 0, nmask = 0;
