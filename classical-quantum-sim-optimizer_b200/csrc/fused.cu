@@ -41,36 +41,38 @@ namespace dq {
 namespace k {
 namespace {
 
-constexpr int kGroupThreads = 256;                       // one group (8 warps)
-constexpr int kThreads = 2 * kGroupThreads;              // two groups
-constexpr uint32_t kTmemCols = 256;                      // one 128-column accumulator per group
+constexpr int kGroups = 4;                               // tiles in flight per CTA (one per group)
+constexpr int kGroupWarps = 4;
+constexpr int kGroupThreads = 32 * kGroupWarps;
+constexpr int kThreads = kGroups * kGroupThreads;
+constexpr uint32_t kTmemCols = 512;                      // one 128-column accumulator per group
 constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part of a tile (4096 x 4 B)
 constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
 constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
 constexpr uint32_t kDescBytes = 320;                     // next_b[32] + next_c[128] (u16) of one block
-constexpr uint32_t kOffRaw = 2 * kTileBytes;             // group g: operand at g*32K, prefetch at 64K + g*32K
 constexpr uint32_t kUBufs = 3;                           // gate images in flight (fetched kUBufs blocks ahead)
 constexpr uint32_t kTBufs = kUBufs + 1;                  // block tables (also read during the readback)
-constexpr uint32_t kOffU = kOffRaw + 2 * kTileBytes;     // gate-image buffers
+constexpr uint32_t kOffU = kGroups * kTileBytes;         // group g's operand at g*32K; then the gate images
 constexpr uint32_t kOffTabs = kOffU + kUBufs * kUBytes;  // lo_tab[64], hi_tab[64] (u64)
 constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
 constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // block-table buffers
 constexpr uint32_t kOffBar = kOffDesc + kTBufs * kDescBytes;  // mbarriers, 8-byte aligned
-constexpr uint32_t kOffWsum = kOffBar + 16 * 8;          // per-group warp sums (double)
-constexpr uint32_t kSmemBytes = kOffWsum + 2 * 8 * 8;
+constexpr uint32_t kOffWsum = kOffBar + 16 * 8;          // per-warp tile-norm partials (double)
+constexpr uint32_t kSmemBytes = kOffWsum + kGroups * kGroupWarps * 8;
 constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
 constexpr long long kWaitCycles = 4000000000LL;          // ... or this many SM cycles
 static_assert(kOffDesc % 16 == 0 && kDescBytes % 16 == 0, "bulk copies need 16-byte alignment");
 static_assert(kOffU % 1024 == 0 && kOffBar % 8 == 0 && kOffWsum % 8 == 0, "operand and mbarrier alignment");
 static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
 static_assert(kUBytes == kFusedUHalves * 2, "gate image size");
+static_assert(kGroupWarps == 4, "a group's warps cover the four TMEM lane quarters");
 
 // mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
-constexpr uint32_t kBarUFull = 0;                  // [kUBufs] gate image of buffer b landed (expect_tx)
-constexpr uint32_t kBarTFull = kBarUFull + kUBufs;  // [kTBufs] block tables of buffer b landed (expect_tx)
-constexpr uint32_t kBarMma = kBarTFull + kTBufs;    // [2] MMAs of group g's tile complete (tcgen05.commit)
-constexpr uint32_t kBarDrain = kBarMma + 2;         // [2] group g's MMAs in flight complete (abort path)
-constexpr uint32_t kNumBars = kBarDrain + 2;
+constexpr uint32_t kBarUFull = 0;                     // [kUBufs] gate image of buffer b landed (expect_tx)
+constexpr uint32_t kBarTFull = kBarUFull + kUBufs;    // [kTBufs] block tables of buffer b landed (expect_tx)
+constexpr uint32_t kBarMma = kBarTFull + kTBufs;      // [kGroups] MMAs of group g's tile complete (commit)
+constexpr uint32_t kBarDrain = kBarMma + kGroups;     // [kGroups] group g's MMAs in flight complete (abort path)
+constexpr uint32_t kNumBars = kBarDrain + kGroups;
 static_assert(kNumBars <= 16, "mbarrier slots");
 
 struct FusedQubits {
@@ -196,10 +198,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t bars = smem_addr(sm + kOffBar);
     auto bar = [bars](uint32_t slot) { return bars + 8u * slot; };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint64_t npairs = (total_tiles + 1) / 2;
-    uint64_t my_pairs = 0;
-    if (blockIdx.x < npairs) my_pairs = (npairs - 1 - blockIdx.x) / gridDim.x + 1;
-    const uint64_t steps = my_pairs * uint64_t(nblocks);
+    const uint64_t nquads = (total_tiles + kGroups - 1) / kGroups;
+    uint64_t my_quads = 0;
+    if (blockIdx.x < nquads) my_quads = (nquads - 1 - blockIdx.x) / gridDim.x + 1;
+    const uint64_t steps = my_quads * uint64_t(nblocks);
     const uint32_t u0 = smem_addr(sm + kOffU);
     // Copies of step st: its block's gate image into buffer st % kUBufs and
     // its tables into buffer st % kTBufs.
@@ -246,42 +248,27 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
 
-    const int g = warp >> 3, gw = warp & 7, gt = tid & (kGroupThreads - 1);
+    // Group g (warps 4g..4g+3) runs tile kGroups*quad + g.
+    const int g = warp / kGroupWarps, gw = warp % kGroupWarps, gt = tid % kGroupThreads;
     unsigned char* x = sm + uint32_t(g) * kTileBytes;
-    unsigned char* raw = sm + kOffRaw + uint32_t(g) * kTileBytes;
-    const uint32_t row = uint32_t(gt >> 6);  // store phase: elements l = (gt & 63) | (row + 4k) << 6
-    const uint64_t glo = lo_tab[gt & 63];
-    const uint32_t olo = io[128 + (gt & 63)];
-    const uint32_t col = uint32_t((gw & 3) * 32 + lane);
-    const uint32_t half = uint32_t(gw >> 2);
-    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 128u * uint32_t(g) + half * 32u;
-    const uint64_t desc_x = make_desc_sw128(smem_addr(x));
-    // Prefetch of tile t into this group's raw buffer, natural local order, 16
-    // bytes per copy (local qubit 0 is global qubit 0: pairs are adjacent).
-    const uint64_t pair_lo = lo_tab[(2 * gt) & 63];
+    const uint64_t glo = lo_tab[gt & 63];                  // store: elements l = (gt & 63) | ((gt >> 6) + 2k) << 6
+    const uint32_t olo = io[128 + (gt & 63)], srow = uint32_t(gt >> 6);
+    const uint64_t pair_lo = lo_tab[(2 * gt) & 63];       // load: pairs (e, e+1), e = 2*gt + 256k
     const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
-    const uint32_t pair_row = uint32_t((2 * gt) >> 6);  // the pairs are (e, e+1), e = 2*gt + 512k
+    const uint32_t prow = uint32_t((2 * gt) >> 6);
+    const uint32_t col = uint32_t(gw * 32 + lane);        // readback: TMEM lane = tile column
+    const uint32_t taddr = tmem + ((uint32_t(gw) * 32u) << 16) + 128u * uint32_t(g);
+    const uint64_t desc_x = make_desc_sw128(smem_addr(x));
     double scale = 1.0;
     uint64_t scale_state = ~uint64_t(0);
-    auto prefetch = [&](uint64_t t) {
-        const float2* src = s + tile_base(t, n, fq);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const uint32_t e = 2u * gt + 512u * k;
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(raw + e * 8u)),
-                         "l"(src + (pair_lo | hi_tab[e >> 6]))
-                         : "memory");
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
     uint32_t mma_cnt = 0;
     uint64_t st = 0;
     bool ok = !s_abort;
-    if (ok && uint64_t(blockIdx.x) * 2 + uint64_t(g) < total_tiles) prefetch(uint64_t(blockIdx.x) * 2 + uint64_t(g));
-    for (uint64_t pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
-        const uint64_t t = 2 * pair + uint64_t(g);
-        if (t >= total_tiles) break;  // only the last pair of the grid can be odd
-        const bool partner = 2 * pair + uint64_t(g ^ 1) < total_tiles;
+    for (uint64_t quad = blockIdx.x; quad < nquads && ok; quad += gridDim.x) {
+        const uint64_t t = kGroups * quad + uint64_t(g);
+        if (t >= total_tiles) break;  // only the last quad of the grid can be short
+        const uint64_t left = total_tiles - kGroups * quad;
+        const uint32_t valid = left < uint64_t(kGroups) ? uint32_t(left) : uint32_t(kGroups);
         const uint64_t base = tile_base(t, n, fq);
         // FP64 renormalisation of the previous pass (tensor-core accumulation
         // rounds toward zero, so unitary blocks shrink the norm slightly).
@@ -289,20 +276,20 @@ __global__ void __launch_bounds__(kThreads, 1)
             scale_state = base >> n;
             scale = 1.0 / sqrt(in_norm[scale_state]);
         }
-        // Each thread reads back exactly the pairs its own cp.async brought
-        // in, so no barrier is needed before it prefetches the next tile.
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        float4 v[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) v[k] = *reinterpret_cast<const float4*>(raw + (2u * gt + 512u * k) * 8u);
-        if (pair + gridDim.x < npairs && 2 * (pair + gridDim.x) + uint64_t(g) < total_tiles)
-            prefetch(2 * (pair + gridDim.x) + uint64_t(g));
         const double ds = scale * double(kScale);
+        const float2* __restrict__ src = s + base;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const uint32_t hi_part = io[64 + pair_row + 8 * k];
-            put_split(x, pair_even ^ hi_part, float(double(v[k].x) * ds), float(double(v[k].y) * ds));
-            put_split(x, pair_odd ^ hi_part, float(double(v[k].z) * ds), float(double(v[k].w) * ds));
+        for (int h = 0; h < 2; h++) {
+            float4 v[8];  // 16-byte pairs: local qubit 0 is global qubit 0
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                v[k] = __ldcg(reinterpret_cast<const float4*>(src + (pair_lo | hi_tab[prow + 4 * (8 * h + k)])));
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t hi_part = io[64 + prow + 4 * (8 * h + k)];
+                put_split(x, pair_even ^ hi_part, float(double(v[k].x) * ds), float(double(v[k].y) * ds));
+                put_split(x, pair_odd ^ hi_part, float(double(v[k].z) * ds), float(double(v[k].w) * ds));
+            }
         }
         double norm_acc = 0.0;
         for (int j = 0; j < nblocks; j++, st++) {
@@ -346,9 +333,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             if (gt == 0 && st + kUBufs < steps) {
-                // The gate-image buffer is free once both tiles' MMAs on it completed:
-                // the second group to get here fetches step st + kUBufs into it.
-                if (!partner || (atomicAdd(&s_ucnt[ub], 1u) & 1u)) {
+                // The gate-image buffer is free once every tile's MMAs on it completed:
+                // the last group to get here resets the count and fetches step st + kUBufs.
+                if (atomicAdd(&s_ucnt[ub], 1u) + 1u == valid) {
+                    atomicExch(&s_ucnt[ub], 0u);
                     fetch(st + kUBufs);
                     atomicMax(&s_fetched, st + kUBufs + 1);
                 }
@@ -356,16 +344,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % kTBufs) * kDescBytes);
             const uint32_t cpart = nb[32 + col];
-            uint32_t nbw[8];  // this half's 16 destination parts, two per word
-            {
-                const uint4 w0 = *reinterpret_cast<const uint4*>(nb + half * 16);
-                const uint4 w1 = *reinterpret_cast<const uint4*>(nb + half * 16 + 8);
-                nbw[0] = w0.x, nbw[1] = w0.y, nbw[2] = w0.z, nbw[3] = w0.w;
-                nbw[4] = w1.x, nbw[5] = w1.y, nbw[6] = w1.z, nbw[7] = w1.w;
-            }
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                // Columns 16h.. of this half: hi*hi + lo*hi, and hi*lo 64 columns on.
+            for (int h = 0; h < 4; h++) {
+                // Outputs 8h..8h+7: columns 16h.. (hi*hi + lo*hi) plus 64 + 16h.. (hi*lo).
                 uint32_t r[16], q[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
@@ -381,20 +362,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                       "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]),
                       "=r"(q[15])
                     : "r"(taddr + 64u + 16u * h));
+                const uint4 nw = *reinterpret_cast<const uint4*>(nb + 8 * h);
+                const uint32_t nbw[4] = {nw.x, nw.y, nw.z, nw.w};
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 if (j + 1 < nblocks) {
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
-                        const int o = 8 * h + i;
-                        const uint32_t off = cpart ^ ((nbw[o >> 1] >> (16 * (o & 1))) & 0xFFFFu);
+                        const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
                         put_split(x, off, __uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i]),
                                   __uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1]));
                     }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
-                        const int o = 8 * h + i;
-                        const uint32_t off = cpart ^ ((nbw[o >> 1] >> (16 * (o & 1))) & 0xFFFFu);
+                        const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
                         const float re = (__uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i])) * kInvScale;
                         const float im = (__uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1])) * kInvScale;
                         *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
@@ -407,21 +388,20 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.fence::before_thread_sync;");
         group_sync(g);  // stage complete
         float2* __restrict__ gp = s + base;
-#pragma unroll
-        for (int k = 0; k < 16; k++)
-            gp[glo | hi_tab[row + 4 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + row + 4 * k]));
+#pragma unroll 8
+        for (int k = 0; k < 32; k++)
+            gp[glo | hi_tab[srow + 2 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + srow + 2 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
-        group_sync(g);  // stage read
-        if (lane == 0) wsum[g * 8 + gw] = norm_acc;
-        group_sync(g);
+        if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;
+        group_sync(g);  // stage read and partial sums written
         if (gt == 0) {
             double tsum = 0.0;
-            for (int w2 = 0; w2 < 8; w2++) tsum += wsum[g * 8 + w2];
+            for (int w2 = 0; w2 < kGroupWarps; w2++) tsum += wsum[g * kGroupWarps + w2];
             tile_norm[t] = tsum;
         }
+        group_sync(g);  // sums read before the next tile writes them
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
     if (!ok && gt == 0) {
         s_abort = 1;
         atomicExch(err, 3);
@@ -526,9 +506,9 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
         if (e != cudaSuccess) fail(kCudaError, std::string("fused pass setup: ") + cudaGetErrorString(e));
         configured[dev & 63] = true;
     }
-    // One CTA per SM, persistent over pairs of tiles.
+    // One CTA per SM, persistent over groups of kGroups tiles.
     const uint64_t total = b.W << (b.n - kFusedM);
-    const uint64_t grid = std::min<uint64_t>((total + 1) / 2, uint64_t(sm_count()));
+    const uint64_t grid = std::min<uint64_t>((total + kGroups - 1) / kGroups, uint64_t(sm_count()));
     k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq,
                                                                blocks_dev + p.first_block, p.nblocks, upool_dev, total,
                                                                err, in_norm, tile_norm);
