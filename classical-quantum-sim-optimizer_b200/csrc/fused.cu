@@ -3,31 +3,29 @@
 // A tile is 2^12 amplitudes.  For block j (a 32x32 complex matrix U on 5 tile
 // qubits) the tile is held in shared memory as the A operand of D = A * B: 128
 // rows (the tile's 128 "columns", i.e. values of the other 7 tile qubits) by
-// K = 64 real inputs (re/im of the 32 basis states), split into f16 hi and lo
-// parts after scaling the tile by a power of two (its norm is kept in
-// [2^13, 2^14), so every amplitude and every block output stays in f16 range;
-// blocks are unitary).  B is the block's real 64x64 form of U (f16 hi and lo),
-// brought in by a cp.async.bulk (TMA) copy.  12 tcgen05.mma.kind::f16
-// instructions (M=128, N=64, K=16) accumulate A_hi*B_hi + A_hi*B_lo +
-// A_lo*B_hi into a 128 x 64 FP32 tile in tensor memory.  The readback
-// (tcgen05.ld, one TMEM lane per tile column) writes every output amplitude
-// straight into the layout the next block needs (128-byte swizzled, bit orders
-// chosen on the host so that each warp's stores hit every bank once), or,
-// after the last block, unscaled into a swizzled natural-order FP32 stage for
-// the store to HBM.
+// K = 64 real inputs (re/im of the 32 basis states), scaled by 2^13 and split
+// into f16 hi and lo parts (states are normalised and blocks unitary, so every
+// value stays in f16 range).  B is the block's real 64x64 form of U as f16 hi
+// and lo images, brought in by cp.async.bulk; [U_hi; U_lo] together form one
+// N = 128 operand.  Eight tcgen05.mma.kind::f16 instructions (M = 128, K = 16)
+// give A_hi*[U_hi; U_lo] (N = 128) and add A_lo*U_hi (N = 64) in FP32 in
+// tensor memory; the readback (tcgen05.ld, one TMEM lane per tile column) sums
+// the two halves and writes every output amplitude straight into the layout
+// the next block needs (128-byte swizzled, bit orders chosen on the host so a
+// warp's stores hit every bank once), or, after the last block, unscaled into
+// a swizzled natural-order FP32 stage for the store to HBM.
 //
-// One CTA per SM, persistent over pairs of tiles, with two groups of 8 warps.
-// Group g owns tile 2*pair + g, one 64-column TMEM accumulator, its operand
-// buffers and a buffer into which its next tile is prefetched (cp.async)
-// while the current one runs; one thread of the group issues its MMAs, so one
-// tile's MMAs run while the other tile is read back.  The two tiles walk the
-// same block sequence and share the gate images (two buffers, fetched two
-// blocks ahead by whichever group finishes its MMAs on a buffer last).
-// Hand-offs are mbarriers (copies, MMA completion) and per-group named
-// barriers; every mbarrier wait is bounded, and a group stops only by a
-// group-wide vote, so no thread is left waiting on a named barrier.  On expiry
-// the CTA records an error, waits (bounded) for its own copies and MMAs, frees
-// its tensor memory and stops.
+// One CTA per SM, persistent over groups of four tiles, with four groups of
+// four warps.  Group g owns one tile, one 128-column TMEM accumulator and one
+// 32 KB operand buffer (also its stage); one thread of the group issues its
+// MMAs, so some tiles' MMAs run while others are read back, loaded or stored.
+// All tiles walk the same block sequence and share the gate images (three
+// buffers, fetched three blocks ahead by whichever group finishes its MMAs on
+// a buffer last).  Hand-offs are mbarriers (copies, MMA completion) and
+// per-group named barriers; every mbarrier wait is bounded, and a group stops
+// only by a group-wide vote, so no thread is left waiting on a named barrier.
+// On expiry the CTA records an error, waits (bounded) for its own copies and
+// MMAs, frees its tensor memory and stops.
 #include <cuda_fp16.h>
 
 #include <algorithm>

@@ -1,10 +1,11 @@
 """The tensor-core fused plan, replayed on the CPU.
 
 The host side of the fused complex64 form -- 12-qubit passes, 5-qubit block
-fusion, the per-block layout tables (which TMEM column / tile row every output
-amplitude goes to next) and the TF32 hi/lo gate images in the canonical
-K-major operand layout -- is replayed here with numpy, block by block, exactly
-as the kernel consumes it, and compared with the FP64 oracle.  No GPU needed.
+fusion, the per-block layout tables (where in the next block's swizzled
+operand every output amplitude goes) and the f16 hi/lo gate images in the
+K-major 128-byte swizzled operand layout -- is replayed here with numpy, block
+by block, exactly as the kernel consumes it, and compared with the FP64
+oracle.  No GPU needed.
 """
 
 import struct
