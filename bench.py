@@ -69,8 +69,8 @@ def tensor_peak():
 # and lo*hi products of the 128 x 64 operand with the 64 x 64 real gate image.
 FUSED_FLOPS_PER_TILE_BLOCK = 3 * 2 * 128 * 64 * 64
 # DRAM bytes (read + write) per tile of one k_fused launch, from the ncu capture
-# of a 25-qubit pass (483.8 MB over 8192 tiles; traffic grows with the tiles).
-FUSED_TRAFFIC_PER_TILE = 483.76e6 / 8192
+# of a 25-qubit pass (483.2 MB over 8192 tiles; traffic grows with the tiles).
+FUSED_TRAFFIC_PER_TILE = 483.245e6 / 8192
 
 
 class ClockSampler:
@@ -264,7 +264,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="brickwork", choices=["brickwork", "qft", "batch", "learned"])
+    ap.add_argument("--workload", default="brickwork", choices=["brickwork", "qft", "batch", "learned", "cases"])
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--shots", type=int, default=100000)
@@ -276,7 +276,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "brickwork":
-        return {"qft": run_qft, "batch": run_batch, "learned": run_learned}[args.workload](args)
+        return {"qft": run_qft, "batch": run_batch, "learned": run_learned, "cases": run_cases}[args.workload](args)
 
     world, rank, local, pg = dist_setup(args)
     import dqsim
@@ -434,6 +434,47 @@ def run_batch(args):
                       "batch_setup_s": setup_s, "passes": batch.passes, "work_items": batch.items,
                       "per_circuit_c128_device_ms": loop_ms, "per_circuit_c128_wall_s": loop_wall,
                       "speedup_device": loop_ms / statistics.mean(ms), "zz_max_err_first16": zz_err}))
+    return 0
+
+
+def run_cases(args):
+    """The reference's own statevector benchmark cases (benchmarks/statevector_benchmark.py:60-90):
+    median of 5 wall-clock repeats after one warm-up, through the public API, on the GPU engine
+    (complex128, the reference's precision) and on the CPU restatement with every host thread."""
+    import dqsim
+    from oracle import oracle
+
+    cases = dqsim.workloads.benchmark_cases()
+
+    def timed(make_sim):
+        sim = make_sim()
+        out = {}
+        for name, (circuit, shots) in cases.items():
+            if name == "full_probabilities_14q":
+                res = sim.simulate(circuit)
+                call = res.probabilities
+            elif shots is not None:
+                call = lambda c=circuit, k=shots: sim.simulate_shots(c, shots=k)
+            else:
+                call = lambda c=circuit: sim.simulate(c)
+            call()
+            times = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                r = call()
+                times.append(time.perf_counter() - t0)
+                if shots is not None:
+                    assert sum(r.values()) == shots
+                elif name == "full_probabilities_14q":
+                    assert abs(sum(r.values()) - 1) < 1e-10
+            out[name] = statistics.median(times)
+        return out
+
+    gpu = timed(lambda: dqsim.StatevectorSimulator(seed=71))
+    cpu = timed(lambda: oracle.OracleSimulator(seed=71))
+    print(json.dumps({"workload": "reference-statevector-benchmark-cases", "unit": "s (median of 5)",
+                      "gpu_complex128": gpu, "cpu_restatement": cpu,
+                      "cpu_threads": oracle.lib().orc_num_threads()}))
     return 0
 
 

@@ -89,3 +89,38 @@ def hea_batch(count=512, seed=0, qmin=12, qmax=22, dmin=4, dmax=16):
         d = int(rng.integers(dmin, dmax + 1))
         out.append(hea(n, d, seed=int(rng.integers(1 << 31)), measure=True))
     return out
+
+
+def benchmark_layers(n, depth):
+    """The layered circuit of the reference's statevector benchmark
+    (benchmarks/statevector_benchmark.py:30-37): per layer RY(0.23 + 0.017 (q + layer))
+    and RZ(-0.41 + 0.019 layer) on every qubit, then CX(q, q + 1) down the register."""
+    ins = []
+    for layer in range(depth):
+        for q in range(n):
+            ins.append({"kind": "ry", "qubit": q, "theta": 0.23 + 0.017 * (q + layer)})
+            ins.append({"kind": "rz", "qubit": q, "phi": -0.41 + 0.019 * layer})
+        for q in range(n - 1):
+            ins.append({"kind": "cx", "control": q, "target": q + 1})
+    return ins
+
+
+def benchmark_cases():
+    """The four cases of benchmarks/statevector_benchmark.py:60-76, as circuits:
+    terminal 12 q (256 shots), dynamic 10 q with a mid-circuit measure and a
+    conditional X (128 shots), unitary 16 q, and a 14-qubit uniform state whose
+    full probability table is queried."""
+    def measure_all(n):
+        return [{"kind": "measure", "qubit": q, "cbit": q} for q in range(n)]
+
+    dynamic = benchmark_layers(10, 3) + [
+        {"kind": "measure", "qubit": 0, "cbit": 0},
+        {"kind": "conditional", "condition": {"creg_base": 0, "creg_size": 1, "creg_value": 1},
+         "op": {"kind": "x", "qubit": 9}},
+    ] + benchmark_layers(10, 3) + measure_all(10)
+    return {
+        "terminal_12q_256shots": (TransportCircuit(12, benchmark_layers(12, 8) + measure_all(12), 12), 256),
+        "dynamic_10q_128shots": (TransportCircuit(10, dynamic, 10), 128),
+        "unitary_16q": (TransportCircuit(16, benchmark_layers(16, 8)), None),
+        "full_probabilities_14q": (TransportCircuit(14, [{"kind": "h", "qubit": q} for q in range(14)]), None),
+    }
