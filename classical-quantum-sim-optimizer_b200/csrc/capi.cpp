@@ -266,6 +266,33 @@ int dq_result_counts(const dq_result* r, uint64_t shots, const uint64_t* qubits,
     });
 }
 
+int dq_result_amplitudes(const dq_result* r, const uint64_t* indices, uint64_t count, double* out) {
+    return guard([&] {
+        need(r, "result");
+        if (count) {
+            need(indices, "indices");
+            need(out, "out");
+        }
+        r->impl->amplitudes(indices, count, out);
+    });
+}
+
+int dq_result_pauli_expectation(const dq_result* r, uint64_t x_mask, uint64_t z_mask, double* re, double* im) {
+    return guard([&] {
+        need(r, "result");
+        need(re, "re");
+        need(im, "im");
+        r->impl->pauli_xz(x_mask, z_mask, re, im);
+        // X^x Z^z differs from the Pauli product by i per Y (Y = i X Z).
+        const int ny = __builtin_popcountll(x_mask & z_mask) & 3;
+        for (int k = 0; k < ny; k++) {
+            const double t = *re;
+            *re = -*im;
+            *im = t;
+        }
+    });
+}
+
 int dq_result_fidelity(const dq_result* r, const double* other, uint64_t other_len, double* out) {
     return guard([&] {
         need(r, "result");

@@ -527,6 +527,32 @@ __global__ void __launch_bounds__(256) k_compare(const VA* __restrict__ a, const
     }
 }
 
+template <typename V>
+__global__ void k_gather(const V* __restrict__ s, const uint64_t* __restrict__ idx, uint64_t count,
+                         double2* __restrict__ out) {
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < count; g += uint64_t(gridDim.x) * blockDim.x) {
+        const V v = s[idx[g]];
+        out[g] = make_double2(v.x, v.y);
+    }
+}
+
+// Partials of sum_i (-1)^popcount((i ^ x) & z) conj(a_i) a_(i ^ x): <a|X^x Z^z|a>.
+template <typename V>
+__global__ void __launch_bounds__(256) k_pauli(const V* __restrict__ a, uint64_t len, uint64_t x, uint64_t z,
+                                              double2* __restrict__ partial) {
+    double re = 0.0, im = 0.0;
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x) {
+        const V u = a[g];
+        const V w = a[g ^ x];
+        const double sgn = (__popcll((g ^ x) & z) & 1) ? -1.0 : 1.0;
+        const double ur = u.x, ui = -double(u.y);
+        re += sgn * (ur * w.x - ui * w.y);
+        im += sgn * (ur * w.y + ui * w.x);
+    }
+    block_sum2(re, im);
+    if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(re, im);
+}
+
 __global__ void k_widen(const float2* __restrict__ s, double2* __restrict__ out, uint64_t len) {
     for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x)
         out[g] = make_double2(s[g].x, s[g].y);
@@ -789,6 +815,26 @@ int dot_partials(const Batch& b, const double2* other, double2* partial) {
     else
         k_dot<double2><<<kDotBlocks, 256, 0, b.stream>>>(static_cast<const double2*>(b.amps), other, len, partial);
     check_launch("dot");
+    return kDotBlocks;
+}
+
+void gather(const Batch& b, const uint64_t* idx, uint64_t count, double2* out) {
+    if (count == 0) return;
+    const unsigned grid = unsigned(std::min<uint64_t>((count + 255) / 256, 1184));
+    if (b.c64)
+        k_gather<float2><<<grid, 256, 0, b.stream>>>(static_cast<const float2*>(b.amps), idx, count, out);
+    else
+        k_gather<double2><<<grid, 256, 0, b.stream>>>(static_cast<const double2*>(b.amps), idx, count, out);
+    check_launch("gather");
+}
+
+int pauli_partials(const Batch& b, uint64_t x, uint64_t z, double2* partial) {
+    const uint64_t len = uint64_t(1) << b.n;
+    if (b.c64)
+        k_pauli<float2><<<kDotBlocks, 256, 0, b.stream>>>(static_cast<const float2*>(b.amps), len, x, z, partial);
+    else
+        k_pauli<double2><<<kDotBlocks, 256, 0, b.stream>>>(static_cast<const double2*>(b.amps), len, x, z, partial);
+    check_launch("pauli expectation");
     return kDotBlocks;
 }
 

@@ -87,6 +87,10 @@ int dot_partials(const Batch& b, const double2* other, double2* partial);
 constexpr int kDotBlocks = 1184;
 // c64 -> c128 widening copy of state 0.
 void widen(const Batch& b, double2* out);
+// out[j] = amplitude idx[j] of state 0 (device index list), widened to c128.
+void gather(const Batch& b, const uint64_t* idx, uint64_t count, double2* out);
+// Partial sums of (-1)^popcount((i^x)&z) conj(a_i) a_(i^x) for state 0; returns block count.
+int pauli_partials(const Batch& b, uint64_t x, uint64_t z, double2* partial);
 // Per-block partials of <a|b> and max |a_i - b_i| for two states of `len`
 // amplitudes, each c128 or c64; partial holds kDotBlocks * 3 doubles.
 void compare(cudaStream_t s, const void* a, bool a64, const void* b, bool b64, uint64_t len, double* partial);

@@ -416,6 +416,45 @@ double Result::fidelity(const double* other, uint64_t len) const {
     return re * re + im * im;
 }
 
+void Result::amplitudes(const uint64_t* indices, uint64_t count, double* out) const {
+    const uint64_t len = uint64_t(1) << n;
+    for (uint64_t j = 0; j < count; j++)
+        if (indices[j] >= len) fail(kValueError, "amplitude index out of range");
+    if (count == 0) return;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    DevMem idx, buf;
+    idx.alloc(count * 8, "amplitude indices");
+    buf.alloc(count * 16, "amplitudes");
+    cuda_check(cudaMemcpyAsync(idx.p, indices, count * 8, cudaMemcpyHostToDevice, dev->stream), "upload indices");
+    k::Batch b = state.view(dev->stream, 1);
+    k::gather(b, idx.as<uint64_t>(), count, buf.as<double2>());
+    cuda_check(cudaMemcpyAsync(out, buf.p, count * 16, cudaMemcpyDeviceToHost, dev->stream), "read amplitudes");
+    dev->sync();
+}
+
+void Result::pauli_xz(uint64_t x, uint64_t z, double* re, double* im) const {
+    const uint64_t len = uint64_t(1) << n;
+    if (x >= len || z >= len) fail(kValueError, "Pauli masks exceed the register");
+    std::lock_guard<std::mutex> lk(dev->mu);
+    dev->activate();
+    DevMem part;
+    part.alloc(k::kDotBlocks * 16, "expectation partial sums");
+    k::Batch b = state.view(dev->stream, 1);
+    const int nb = k::pauli_partials(b, x, z, part.as<double2>());
+    std::vector<double2> hp(static_cast<size_t>(nb));
+    cuda_check(cudaMemcpyAsync(hp.data(), part.p, size_t(nb) * 16, cudaMemcpyDeviceToHost, dev->stream),
+               "read partials");
+    dev->sync();
+    double r = 0, i = 0;
+    for (auto& v : hp) {  // fixed order: deterministic
+        r += v.x;
+        i += v.y;
+    }
+    *re = r;
+    *im = i;
+}
+
 void write_shots_profile(const ShotOutput& out, double preprocessing, double fusion, double shots_total, double total,
                          uint64_t shots) {
     ::mkdir("dqsim_profiles", 0777);

@@ -67,6 +67,10 @@ class Result {
     std::unordered_map<uint64_t, uint64_t> counts(uint64_t shots, const std::vector<uint64_t>& qubits,
                                                   uint64_t seed) const;
     double fidelity(const double* other_interleaved, uint64_t len) const;
+    // Amplitudes at the given indices (interleaved re/im), read on the device.
+    void amplitudes(const uint64_t* indices, uint64_t count, double* out_interleaved) const;
+    // <psi| X^x Z^z |psi> as (re, im), reduced on the device in FP64.
+    void pauli_xz(uint64_t x, uint64_t z, double* re, double* im) const;
 };
 
 class Simulator {

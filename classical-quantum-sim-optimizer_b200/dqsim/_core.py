@@ -91,6 +91,9 @@ _res_probs = _sig("dq_result_probabilities", [_P, _P, ctypes.c_size_t, ctypes.c_
 _res_counts = _sig("dq_result_counts", [_P, _u64, _P, ctypes.c_size_t, ctypes.c_int, _u64, ctypes.c_int,
                                         ctypes.POINTER(_P)])
 _res_fidelity = _sig("dq_result_fidelity", [_P, _P, _u64, ctypes.POINTER(ctypes.c_double)])
+_res_amps = _sig("dq_result_amplitudes", [_P, _P, _u64, _P])
+_res_pauli = _sig("dq_result_pauli_expectation", [_P, _u64, _u64, ctypes.POINTER(ctypes.c_double),
+                                                  ctypes.POINTER(ctypes.c_double)])
 _res_free = _sig("dq_result_free", [_P], None)
 _compile_dump = _sig("dq_compile_dump", [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p)])
 _string_free = _sig("dq_string_free", [ctypes.c_void_p], None)
@@ -248,6 +251,43 @@ class SimulationResult:
         _check(_res_counts(self._h, shots, arr.ctypes.data_as(_P), len(qs or []), 0 if qs is None else 1, seed_v,
                            1 if has_seed else 0, ctypes.byref(h)))
         return _take_counts(h)
+
+    def amplitude(self, bitstring):
+        """One amplitude, read on the device; the bitstring has one binary digit
+        per qubit, highest qubit first.  Extra query (the reference offers it on
+        MPS and P-block results, src/monolithic/mps/result.rs:114-130)."""
+        if not isinstance(bitstring, str) or len(bitstring) != self._n or any(ch not in "01" for ch in bitstring):
+            raise ValueError("Expected one binary digit per qubit, MSB first")
+        return complex(self.amplitudes([int(bitstring, 2)])[0]) if self._n else complex(self.amplitudes([0])[0])
+
+    def amplitudes(self, indices):
+        """Amplitudes at little-endian basis indices, as a complex128 array (device gather)."""
+        arr = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64).ravel())
+        out = np.empty(arr.shape[0], dtype=np.complex128)
+        _check(_res_amps(self._h, arr.ctypes.data_as(_P), arr.shape[0], out.ctypes.data_as(_P)))
+        return out
+
+    def expectation_value(self, pauli):
+        """<psi|P|psi> for a Pauli string with one of I, X, Y, Z per qubit, highest
+        qubit first, reduced in FP64 on the device.  Extra query (the reference
+        offers it on MPS results, src/monolithic/mps/result.rs:209-236)."""
+        if not isinstance(pauli, str) or len(pauli) != self._n:
+            raise ValueError("Expected one Pauli per qubit")
+        x = z = 0
+        for pos, ch in enumerate(pauli):
+            bit = 1 << (self._n - 1 - pos)
+            if ch == "X":
+                x |= bit
+            elif ch == "Z":
+                z |= bit
+            elif ch == "Y":
+                x |= bit
+                z |= bit
+            elif ch != "I":
+                raise ValueError("Pauli string must contain only I, X, Y, Z")
+        re, im = ctypes.c_double(), ctypes.c_double()
+        _check(_res_pauli(self._h, x, z, ctypes.byref(re), ctypes.byref(im)))
+        return re.value
 
     def fidelity(self, other):
         """|<self|other>|^2 for a complex128 array; 0.0 on a length mismatch."""

@@ -127,6 +127,21 @@ DQ_API int dq_result_counts(const dq_result* r, uint64_t shots, const uint64_t* 
                      uint64_t seed, int has_seed, dq_counts** out);
 /* .fidelity(other): |<self|other>|^2; 0.0 when the lengths differ. */
 DQ_API int dq_result_fidelity(const dq_result* r, const double* other, uint64_t other_len, double* out);
+
+/* Amplitudes of the result's state at `count` indices (little-endian basis
+ * index, qubit 0 = LSB), written as 2*count doubles (re, im), read on the device
+ * without copying the state to the host.  Extra query: the reference's
+ * statevector result has no counterpart; it mirrors the MPS / P-block results'
+ * `amplitude` (src/monolithic/mps/result.rs:114-130,
+ * src/distributed/pblock/result.rs:141).  Out-of-range index -> DQ_VALUE_ERROR. */
+DQ_API int dq_result_amplitudes(const dq_result* r, const uint64_t* indices, uint64_t count, double* out);
+
+/* <psi|P|psi> for the Pauli product P with X on the bits of x_mask & ~z_mask,
+ * Z on z_mask & ~x_mask and Y on x_mask & z_mask (qubit q = bit q), reduced in
+ * FP64 on the device; *re is the expectation, *im its (rounding-level)
+ * imaginary part.  Extra query mirroring the MPS result's `expectation_value`
+ * (src/monolithic/mps/result.rs:209-236); no statevector counterpart. */
+DQ_API int dq_result_pauli_expectation(const dq_result* r, uint64_t x_mask, uint64_t z_mask, double* re, double* im);
 DQ_API void dq_result_free(dq_result* r);
 
 /* Prepared circuits: parse, validate, compile and lower once, keep the state
