@@ -262,6 +262,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t mma_cnt = 0;
     uint64_t st = 0;
     bool ok = !s_abort;
+    // Tile t into this group's operand buffer as raw complex64 in natural local
+    // order, 16 bytes per copy (local qubit 0 is global qubit 0); issued as soon
+    // as the buffer is free, read back at the start of the tile.
+    auto prefetch = [&](uint64_t tt) {
+        const float2* __restrict__ src = s + tile_base(tt, n, fq);
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(x + (2u * gt + 256u * k) * 8u)),
+                         "l"(src + (pair_lo | hi_tab[prow + 4 * k]))
+                         : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (ok && uint64_t(blockIdx.x) * kGroups + uint64_t(g) < total_tiles) prefetch(uint64_t(blockIdx.x) * kGroups + g);
     for (uint64_t quad = blockIdx.x; quad < nquads && ok; quad += gridDim.x) {
         const uint64_t t = kGroups * quad + uint64_t(g);
         if (t >= total_tiles) break;  // only the last quad of the grid can be short
@@ -275,16 +288,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             scale = 1.0 / sqrt(in_norm[scale_state]);
         }
         const double ds = scale * double(kScale);
-        const float2* __restrict__ src = s + base;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        group_sync(g);  // the group's copies of this tile have landed
+        {
+            float4 v[16];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float4 v[8];  // 16-byte pairs: local qubit 0 is global qubit 0
+            for (int k = 0; k < 16; k++) v[k] = *reinterpret_cast<const float4*>(x + (2u * gt + 256u * k) * 8u);
+            group_sync(g);  // raw tile read: the split may overwrite it
 #pragma unroll
-            for (int k = 0; k < 8; k++)
-                v[k] = __ldcg(reinterpret_cast<const float4*>(src + (pair_lo | hi_tab[prow + 4 * (8 * h + k)])));
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const uint32_t hi_part = io[64 + prow + 4 * (8 * h + k)];
+            for (int k = 0; k < 16; k++) {
+                const uint32_t hi_part = io[64 + prow + 4 * k];
                 put_split(x, pair_even ^ hi_part, float(double(v[k].x) * ds), float(double(v[k].y) * ds));
                 put_split(x, pair_odd ^ hi_part, float(double(v[k].z) * ds), float(double(v[k].w) * ds));
             }
@@ -393,6 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;
         group_sync(g);  // stage read and partial sums written
+        if (t + uint64_t(kGroups) * gridDim.x < total_tiles) prefetch(t + uint64_t(kGroups) * gridDim.x);
         if (gt == 0) {
             double tsum = 0.0;
             for (int w2 = 0; w2 < kGroupWarps; w2++) tsum += wsum[g * kGroupWarps + w2];
@@ -400,6 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         group_sync(g);  // sums read before the next tile writes them
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     if (!ok && gt == 0) {
         s_abort = 1;
         atomicExch(err, 3);
