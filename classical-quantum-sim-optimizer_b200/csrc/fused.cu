@@ -169,6 +169,38 @@ __device__ __forceinline__ void put_split(unsigned char* x, uint32_t off, float 
     *reinterpret_cast<__half2*>(x + kPartBytes + off) = l;
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic: one instruction per pair).
+__device__ __forceinline__ uint64_t pack2(uint32_t a, uint32_t b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(a), "r"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// put_split for a packed (re, im) pair.
+__device__ __forceinline__ void put_split2(unsigned char* x, uint32_t off, uint64_t v) {
+    uint32_t re, im;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(re), "=r"(im) : "l"(v));
+    const __half2 h = __floats2half2_rn(__uint_as_float(re), __uint_as_float(im));
+    const float2 hf = __half22float2(h);
+    const uint64_t lo = sub2(v, pack2(__float_as_uint(hf.x), __float_as_uint(hf.y)));
+    uint32_t lr, li;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(lr), "=r"(li) : "l"(lo));
+    *reinterpret_cast<__half2*>(x + off) = h;
+    *reinterpret_cast<__half2*>(x + kPartBytes + off) = __floats2half2_rn(__uint_as_float(lr), __uint_as_float(li));
+}
+
 // Global position of the first amplitude of tile t (its local index 0).
 __device__ __forceinline__ uint64_t tile_base(uint64_t t, int n, const FusedQubits& fq) {
     const int rest = n - kFusedM;
@@ -380,8 +412,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
                         const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                        put_split(x, off, __uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i]),
-                                  __uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1]));
+                        put_split2(x, off, add2(pack2(r[2 * i], r[2 * i + 1]), pack2(q[2 * i], q[2 * i + 1])));
                     }
                 } else {
 #pragma unroll
