@@ -160,15 +160,6 @@ __device__ __forceinline__ bool group_all(bool v, int g) {
     return r != 0;
 }
 
-// f16 hi part rounded to nearest, lo = f16 of the remainder.
-__device__ __forceinline__ void put_split(unsigned char* x, uint32_t off, float re, float im) {
-    const __half2 h = __floats2half2_rn(re, im);
-    const float2 hf = __half22float2(h);
-    const __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
-    *reinterpret_cast<__half2*>(x + off) = h;
-    *reinterpret_cast<__half2*>(x + kPartBytes + off) = l;
-}
-
 // Packed FP32 pairs (sm_100 f32x2 arithmetic: one instruction per pair).
 __device__ __forceinline__ uint64_t pack2(uint32_t a, uint32_t b) {
     uint64_t r;
@@ -182,13 +173,20 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
     return r;
 }
 
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
     uint64_t r;
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
     return r;
 }
 
-// put_split for a packed (re, im) pair.
+// f16 hi part of a packed (re, im) pair rounded to nearest, lo = f16 of the
+// remainder; stored at `off` in the hi and lo operand parts.
 __device__ __forceinline__ void put_split2(unsigned char* x, uint32_t off, uint64_t v) {
     uint32_t re, im;
     asm("mov.b64 {%0, %1}, %2;" : "=r"(re), "=r"(im) : "l"(v));
@@ -281,9 +279,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // Group g (warps 4g..4g+3) runs tile kGroups*quad + g.
     const int g = warp / kGroupWarps, gw = warp % kGroupWarps, gt = tid % kGroupThreads;
     unsigned char* x = sm + uint32_t(g) * kTileBytes;
-    const uint64_t glo = lo_tab[gt & 63];                  // store: elements l = (gt & 63) | ((gt >> 6) + 2k) << 6
-    const uint32_t olo = io[128 + (gt & 63)], srow = uint32_t(gt >> 6);
-    const uint64_t pair_lo = lo_tab[(2 * gt) & 63];       // load: pairs (e, e+1), e = 2*gt + 256k
+    const uint64_t pair_lo = lo_tab[(2 * gt) & 63];       // load and store: pairs (e, e+1), e = 2*gt + 256k
+    const uint32_t pair_out = io[128 + ((2 * gt) & 63)];
     const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
     const uint32_t prow = uint32_t((2 * gt) >> 6);
     const uint32_t col = uint32_t(gw * 32 + lane);        // readback: TMEM lane = tile column
@@ -319,7 +316,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             scale_state = base >> n;
             scale = 1.0 / sqrt(in_norm[scale_state]);
         }
-        const double ds = scale * double(kScale);
+        const float fs = float(scale * double(kScale));
+        const uint64_t fs2 = pack2(__float_as_uint(fs), __float_as_uint(fs));
         asm volatile("cp.async.wait_all;" ::: "memory");
         group_sync(g);  // the group's copies of this tile have landed
         {
@@ -330,8 +328,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int k = 0; k < 16; k++) {
                 const uint32_t hi_part = io[64 + prow + 4 * k];
-                put_split(x, pair_even ^ hi_part, float(double(v[k].x) * ds), float(double(v[k].y) * ds));
-                put_split(x, pair_odd ^ hi_part, float(double(v[k].z) * ds), float(double(v[k].w) * ds));
+                put_split2(x, pair_even ^ hi_part,
+                           mul2(pack2(__float_as_uint(v[k].x), __float_as_uint(v[k].y)), fs2));
+                put_split2(x, pair_odd ^ hi_part,
+                           mul2(pack2(__float_as_uint(v[k].z), __float_as_uint(v[k].w)), fs2));
             }
         }
         double norm_acc = 0.0;
@@ -431,8 +431,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         group_sync(g);  // stage complete
         float2* __restrict__ gp = s + base;
 #pragma unroll 8
-        for (int k = 0; k < 32; k++)
-            gp[glo | hi_tab[srow + 2 * k]] = *reinterpret_cast<const float2*>(x + (olo ^ io[192 + srow + 2 * k]));
+        for (int k = 0; k < 16; k++)  // 16-byte pairs: adjacent stage slots, adjacent in HBM
+            *reinterpret_cast<float4*>(gp + (pair_lo | hi_tab[prow + 4 * k])) =
+                *reinterpret_cast<const float4*>(x + (pair_out ^ io[192 + prow + 4 * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;

@@ -408,7 +408,9 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
     int hn = 0;
     {
         std::vector<uint32_t> free_bits, high;
-        for (uint32_t b = 0; b < 4; b++)
+        // Bit 0 is never a destination: slots of l and l ^ 1 stay adjacent, so
+        // the store phase reads 16-byte pairs.
+        for (uint32_t b = 1; b < 4; b++)
             if (!((lanes >> b) & 1u)) free_bits.push_back(b);
         for (uint32_t b = 4; b < 12; b++)
             if ((lanes >> b) & 1u) high.push_back(b);
