@@ -36,7 +36,7 @@ struct dq_result {
 };
 struct dq_counts {
     uint64_t width = 0;
-    std::vector<std::string> keys;
+    std::string keys;  // distinct keys of `width` characters back to back
     std::vector<uint64_t> counts;
 };
 
@@ -140,11 +140,16 @@ int dq_simulate_shots(dq_sim* sim, const char* json, size_t len, uint64_t shots,
         need(out, "out");
         ShotOutput so = sim->impl->simulate_shots(json, len, shots, profile != 0, nullptr, nullptr);
         auto c = std::make_unique<dq_counts>();
-        c->width = 0;
-        for (auto& kv : so.counts) {
-            c->width = kv.first.size();
-            c->keys.push_back(kv.first);
-            c->counts.push_back(kv.second);
+        if (!so.flat_counts.empty()) {
+            c->width = so.key_width;
+            c->keys = std::move(so.flat_keys);
+            c->counts = std::move(so.flat_counts);
+        } else {
+            for (auto& kv : so.counts) {
+                c->width = kv.first.size();
+                c->keys += kv.first;
+                c->counts.push_back(kv.second);
+            }
         }
         *out = c.release();
     });
@@ -164,7 +169,7 @@ int dq_simulate(dq_sim* sim, const char* json, size_t len, dq_result** out) {
 int dq_counts_size(const dq_counts* c, uint64_t* n_keys, uint64_t* key_width) {
     return guard([&] {
         need(c, "counts");
-        if (n_keys) *n_keys = c->keys.size();
+        if (n_keys) *n_keys = c->counts.size();
         if (key_width) *key_width = c->width;
     });
 }
@@ -172,10 +177,8 @@ int dq_counts_size(const dq_counts* c, uint64_t* n_keys, uint64_t* key_width) {
 int dq_counts_copy(const dq_counts* c, char* keys, uint64_t* counts) {
     return guard([&] {
         need(c, "counts");
-        for (size_t i = 0; i < c->keys.size(); i++) {
-            if (keys && c->width) std::memcpy(keys + i * c->width, c->keys[i].data(), c->width);
-            if (counts) counts[i] = c->counts[i];
-        }
+        if (keys && !c->keys.empty()) std::memcpy(keys, c->keys.data(), c->keys.size());
+        if (counts && !c->counts.empty()) std::memcpy(counts, c->counts.data(), c->counts.size() * 8);
     });
 }
 
@@ -259,7 +262,7 @@ int dq_result_counts(const dq_result* r, uint64_t shots, const uint64_t* qubits,
             std::string key(q.size(), '0');
             for (size_t b = 0; b < q.size(); b++)
                 if ((kv.first >> (q.size() - 1 - b)) & 1) key[b] = '1';
-            c->keys.push_back(key);
+            c->keys += key;
             c->counts.push_back(kv.second);
         }
         *out = c.release();
@@ -426,7 +429,7 @@ int dq_batch_counts(const dq_batch* b, uint64_t index, dq_counts** out) {
         auto c = std::make_unique<dq_counts>();
         for (auto& kv : m) {
             c->width = kv.first.size();
-            c->keys.push_back(kv.first);
+            c->keys += kv.first;
             c->counts.push_back(kv.second);
         }
         *out = c.release();

@@ -1,8 +1,13 @@
 #include "engine.hpp"
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
+#include <functional>
+#include <thread>
 
 #include "cost.hpp"
 
@@ -17,17 +22,83 @@ void cuda_check(cudaError_t e, const char* what) {
     fail(kCudaError, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const size_t workers = std::min<size_t>({count, hw, 16});
+    if (workers <= 1) {
+        for (size_t i = 0; i < count; i++) fn(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::exception_ptr> errors(workers);
+    std::vector<std::thread> pool;
+    for (size_t w = 0; w < workers; w++)
+        pool.emplace_back([&, w] {
+            try {
+                for (size_t i = next++; i < count; i = next++) fn(i);
+            } catch (...) {
+                errors[w] = std::current_exception();
+                next = count;
+            }
+        });
+    for (auto& t : pool) t.join();
+    for (auto& e : errors)
+        if (e) std::rethrow_exception(e);
+}
+
+namespace {
+
+// Returns the memory the current device's pool keeps cached to the driver.
+void trim_pool() {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(pool, 0);
+    }
+}
+
+}  // namespace
+
 void DevMem::alloc(size_t b, const char* what) {
     release();
     if (b == 0) b = 16;
-    cuda_check(cudaMalloc(&p, b), what);
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaErrorMemoryAllocation) {  // memory cached by the stream-ordered pool: give it back, retry
+        cudaGetLastError();
+        trim_pool();
+        e = cudaMalloc(&p, b);
+    }
+    if (e != cudaSuccess) p = nullptr;
+    cuda_check(e, what);
     bytes = b;
 }
 
+void DevMem::alloc_on(size_t b, cudaStream_t s, const char* what) {
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMallocAsync(&p, b, s);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        trim_pool();
+        e = cudaMallocAsync(&p, b, s);
+    }
+    if (e != cudaSuccess) p = nullptr;
+    cuda_check(e, what);
+    bytes = b;
+    stream = s;
+}
+
 void DevMem::release() {
-    if (p) cudaFree(p);
+    if (p) {
+        if (stream)
+            cudaFreeAsync(p, stream);
+        else
+            cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
+    stream = nullptr;
 }
 
 Device::Device(int ord) : ordinal(ord) {
@@ -38,6 +109,14 @@ Device::Device(int ord) : ordinal(ord) {
     if (ord < 0 || ord >= count) fail(kValueError, "CUDA device ordinal out of range");
     cuda_check(cudaSetDevice(ord), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // Freed stream-ordered blocks stay cached in the device pool (statevector
+    // and sampling-table sized), returned on destruction or when a plain
+    // allocation runs out of memory.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ord) == cudaSuccess) {
+        uint64_t keep = ~uint64_t(0);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
 }
 
 Device::~Device() {
@@ -45,6 +124,7 @@ Device::~Device() {
         cudaSetDevice(ordinal);
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
+        trim_pool();
     }
 }
 
@@ -52,13 +132,16 @@ void Device::activate() const { cuda_check(cudaSetDevice(ordinal), "cudaSetDevic
 
 void Device::sync() { cuda_check(cudaStreamSynchronize(stream), "stream synchronize"); }
 
-void StateBatch::allocate(int n_, uint64_t W_, uint64_t ncb_, bool c64_) {
+void StateBatch::allocate(int n_, uint64_t W_, uint64_t ncb_, bool c64_, cudaStream_t pool_stream) {
     n = n_;
     W = W_;
     ncb = ncb_;
     c64 = c64_;
     cwords = int(std::max<uint64_t>(1, (ncb + 63) / 64));
-    amps.alloc((size_t(W) << n) * (c64 ? 8 : 16), "the statevector");
+    if (pool_stream)
+        amps.alloc_on((size_t(W) << n) * (c64 ? 8 : 16), pool_stream, "the statevector");
+    else
+        amps.alloc((size_t(W) << n) * (c64 ? 8 : 16), "the statevector");
     cbits.alloc(size_t(W) * cwords * 8, "classical bits");
     seeds.alloc(size_t(W) * 8, "rng seeds");
     draws.alloc(size_t(W) * 8, "rng counters");
@@ -198,15 +281,24 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
         o.keep_raw = true;
         o.pinned_low = kFusedPinned;
         std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
-        for (auto& p : ps) {
+        // Each pass's choice and fused blocks are independent host work: built on
+        // a few threads into per-pass buffers, then appended in pass order.
+        struct Built {
+            int choice = 0;
+            FusedPass fp;
+            std::vector<FusedBlock> blocks;
+            std::vector<uint16_t> upool;
+        };
+        std::vector<Built> built(ps.size());
+        parallel_for(ps.size(), [&](size_t i) {
+            const TilePass& p = ps[i];
+            Built& bt = built[i];
             // With a trained cost model each pass runs on whichever executor it
             // predicts cheapest: tensor-core blocks (0) or CUDA-core tile
             // operations fused to width 1..kTileMaxDense.
-            int choice = 0;
+            bt.fp = build_fused_pass(p.raw, p.qubits, bt.blocks, bt.upool);
             if (cfg_.model) {
-                std::vector<FusedBlock> tb;
-                std::vector<uint16_t> tu;
-                double best = cfg_.model->predict_fused(build_fused_pass(p.raw, p.qubits, tb, tu));
+                double best = cfg_.model->predict_fused(bt.fp);
                 for (int w = 1; w <= kTileMaxDense; w++) {
                     std::vector<double2> scratch;
                     std::vector<TileOp> cand;
@@ -214,17 +306,26 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
                     const double cost = cfg_.model->predict_ops(cand, kFusedM, true);
                     if (cost < best) {
                         best = cost;
-                        choice = w;
+                        bt.choice = w;
                     }
                 }
             }
+        });
+        for (size_t i = 0; i < ps.size(); i++) {
+            TilePass& p = ps[i];
+            Built& bt = built[i];
+            const int choice = bt.choice;
             widths_.push_back(choice);
             Step s;
             s.type = Operation::Dense;
             s.category = 1;
             if (choice == 0) {
                 s.fused = int(fused_.size());
-                fused_.push_back(build_fused_pass(p.raw, p.qubits, fused_blocks_host_, upool_host_));
+                bt.fp.first_block += int(fused_blocks_host_.size());
+                for (FusedBlock& fb : bt.blocks) fb.u_off += uint32_t(upool_host_.size());
+                fused_blocks_host_.insert(fused_blocks_host_.end(), bt.blocks.begin(), bt.blocks.end());
+                upool_host_.insert(upool_host_.end(), bt.upool.begin(), bt.upool.end());
+                fused_.push_back(std::move(bt.fp));
                 fused_src_.push_back(std::move(p));
             } else {
                 lower_pass_ops(p.raw, p.qubits, cfg_.n, choice, pool_host_, p.ops);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -18,14 +19,23 @@ void cuda_check(cudaError_t e, const char* what);
 
 // Owning device allocation.  Allocation failure is a MemoryError, as the
 // reference reports a failed statevector reservation (shots.rs:33-41).
+// Runs fn(0) .. fn(count - 1) on up to 16 host threads; the first exception
+// a call throws is rethrown here after every thread has finished.
+void parallel_for(size_t count, const std::function<void(size_t)>& fn);
+
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;  // set: stream-ordered block from the device's memory pool
     DevMem() = default;
     DevMem(const DevMem&) = delete;
     DevMem& operator=(const DevMem&) = delete;
     ~DevMem() { release(); }
     void alloc(size_t b, const char* what);
+    // Stream-ordered allocation: the block returns to the device pool when
+    // released, in order on stream s, so the next large buffer of the same
+    // size costs no driver mapping.
+    void alloc_on(size_t b, cudaStream_t s, const char* what);
     void ensure(size_t b, const char* what) {
         if (b > bytes) alloc(b, what);
     }
@@ -51,7 +61,8 @@ struct StateBatch {
     uint64_t W = 0, ncb = 0;
     int cwords = 1;
     bool c64 = false;
-    void allocate(int n, uint64_t W, uint64_t ncb, bool c64);
+    // With a stream, the statevector comes from the stream-ordered pool.
+    void allocate(int n, uint64_t W, uint64_t ncb, bool c64, cudaStream_t pool_stream = nullptr);
     k::Batch view(cudaStream_t s, uint64_t W_active) const;
     size_t amp_bytes() const { return size_t(1) << n; }
 };

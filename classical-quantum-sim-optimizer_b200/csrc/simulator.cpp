@@ -205,7 +205,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
             uint64_t kept_seed = seed;
             {
                 StateBatch st;
-                st.allocate(int(n), 1, ncb, c64);
+                st.allocate(int(n), 1, ncb, c64, s);
                 k::Batch b = st.view(s, 1);
                 k::init_basis(b);
                 reset_bookkeeping(st, 1, {kept_seed}, s);
@@ -213,7 +213,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 ex.run(b, nullptr);
                 DevMem cdf, tmp, idx;
                 const uint64_t clen = uint64_t(1) << kq;
-                cdf.alloc(clen * 8, "the sampling table");
+                cdf.alloc_on(clen * 8, s, "the sampling table");
                 probs_to(b, qubits, cdf.as<double>());
                 double total = build_cdf(s, cdf.as<double>(), clen, tmp);
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
@@ -224,12 +224,44 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 std::vector<uint64_t> h(shots);
                 cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
                 cuda_check(cudaStreamSynchronize(s), "stream synchronize");
-                std::unordered_map<uint64_t, uint64_t> sampled;
-                for (uint64_t v : h) sampled[v]++;
-                std::vector<uint8_t> cb(ncb, 0);
-                for (auto& kv : sampled) {
-                    for (auto& sh : shifts) cb[sh.first] = uint8_t((kv.first >> sh.second) & 1);
-                    out.counts[format_bits(cb.data(), ncb)] += kv.second;
+                std::sort(h.begin(), h.end());
+                if (ncb <= 64) {
+                    // Classical-register value of each distinct outcome, merged by value.
+                    std::vector<std::pair<uint64_t, uint64_t>> kc;
+                    for (size_t i = 0; i < h.size();) {
+                        size_t j = i;
+                        while (j < h.size() && h[j] == h[i]) j++;
+                        uint64_t key = 0;
+                        for (auto& sh : shifts) key |= ((h[i] >> sh.second) & 1) << sh.first;
+                        kc.emplace_back(key, uint64_t(j - i));
+                        i = j;
+                    }
+                    if (!std::is_sorted(kc.begin(), kc.end())) std::sort(kc.begin(), kc.end());
+                    size_t distinct = 0;
+                    for (size_t i = 0; i < kc.size(); i++) {
+                        if (distinct && kc[i].first == kc[distinct - 1].first)
+                            kc[distinct - 1].second += kc[i].second;
+                        else
+                            kc[distinct++] = kc[i];
+                    }
+                    out.key_width = ncb;
+                    out.flat_keys.assign(distinct * ncb, '0');
+                    out.flat_counts.resize(distinct);
+                    char* key = &out.flat_keys[0];
+                    for (size_t i = 0; i < distinct; i++, key += ncb) {
+                        for (uint64_t c = 0; c < ncb; c++)  // cbit 0 is the rightmost character
+                            key[ncb - 1 - c] = char('0' + ((kc[i].first >> c) & 1));
+                        out.flat_counts[i] = kc[i].second;
+                    }
+                } else {
+                    std::vector<uint8_t> cb(ncb, 0);
+                    for (size_t i = 0; i < h.size();) {
+                        size_t j = i;
+                        while (j < h.size() && h[j] == h[i]) j++;
+                        for (auto& sh : shifts) cb[sh.first] = uint8_t((h[i] >> sh.second) & 1);
+                        out.counts[format_bits(cb.data(), ncb)] += uint64_t(j - i);
+                        i = j;
+                    }
                 }
             }
             out.strategy = "terminal_sampling";

@@ -40,6 +40,11 @@ ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate = false
 
 struct ShotOutput {
     std::unordered_map<std::string, uint64_t> counts;
+    // Terminal sampling fills these instead of `counts`: distinct keys of
+    // key_width characters back to back, one count each.
+    std::string flat_keys;
+    std::vector<uint64_t> flat_counts;
+    uint64_t key_width = 0;
     std::vector<double> shot_times;
     std::string strategy;
     uint64_t parallel_shots = 0;

@@ -147,10 +147,10 @@ def _take_counts(handle):
         _check(_counts_size(handle, ctypes.byref(n), ctypes.byref(w)))
         n, w = n.value, w.value
         keys = ctypes.create_string_buffer(max(1, n * w))
-        counts = (_u64 * max(1, n))()
-        _check(_counts_copy(handle, keys, counts))
-        raw = keys.raw
-        return {raw[i * w:(i + 1) * w].decode("ascii"): int(counts[i]) for i in range(n)}
+        counts = np.zeros(max(1, n), dtype=np.uint64)
+        _check(_counts_copy(handle, keys, counts.ctypes.data))
+        text = keys.raw[:n * w].decode("ascii")
+        return dict(zip([text[i:i + w] for i in range(0, n * w, w)] if w else [""] * n, counts[:n].tolist()))
     finally:
         _counts_free(handle)
 
