@@ -70,42 +70,60 @@ void op_matrix(const Operation& op, std::vector<uint64_t>& qs, std::vector<cplx>
     }
 }
 
-// E = op matrix embedded on block qubits `bq` (MSB-first), then out = E * acc.
+// Where op qubits `oq` sit in the index of block qubits `bq` (both MSB-first):
+// ext[j] = op index of block index j, dep[v] = block bits of op index v.
+struct Embedding {
+    int dim = 0, odim = 0;
+    uint32_t opmask = 0;
+    std::vector<int> ext, dep;
+    Embedding(const std::vector<uint64_t>& bq, const std::vector<uint64_t>& oq) {
+        const int k = int(bq.size()), ko = int(oq.size());
+        dim = 1 << k;
+        odim = 1 << ko;
+        std::vector<int> pos(static_cast<size_t>(ko));  // bit position (LSB = 0) of each op qubit in the block index
+        for (int t = 0; t < ko; t++) {
+            const int idx = int(std::find(bq.begin(), bq.end(), oq[size_t(t)]) - bq.begin());
+            pos[size_t(t)] = k - 1 - idx;
+            opmask |= 1u << pos[size_t(t)];
+        }
+        ext.assign(size_t(dim), 0);
+        for (int j = 0; j < dim; j++)
+            for (int t = 0; t < ko; t++) ext[size_t(j)] = (ext[size_t(j)] << 1) | ((j >> pos[size_t(t)]) & 1);
+        dep.assign(size_t(odim), 0);
+        for (int v = 0; v < odim; v++)
+            for (int t = 0; t < ko; t++)
+                if ((v >> (ko - 1 - t)) & 1) dep[size_t(v)] |= 1 << pos[size_t(t)];
+    }
+};
+
+// The op matrix embedded on block qubits `bq` (identity on the others).
+std::vector<cplx> embed(const std::vector<uint64_t>& bq, const std::vector<uint64_t>& oq,
+                        const std::vector<cplx>& om) {
+    const Embedding e(bq, oq);
+    std::vector<cplx> out(size_t(e.dim) * e.dim, cplx(0));
+    for (int r = 0; r < e.dim; r++) {
+        const int rest = r & ~int(e.opmask), ro = e.ext[size_t(r)];
+        for (int x = 0; x < e.odim; x++)
+            out[size_t(r) * e.dim + (rest | e.dep[size_t(x)])] = om[size_t(ro) * e.odim + x];
+    }
+    return out;
+}
+
+// E = op matrix embedded on block qubits `bq` (MSB-first), then acc = E * acc.
 void left_multiply(const std::vector<uint64_t>& bq, std::vector<cplx>& acc, const std::vector<uint64_t>& oq,
                    const std::vector<cplx>& om) {
-    const int k = int(bq.size()), ko = int(oq.size());
-    const int dim = 1 << k, odim = 1 << ko;
-    std::vector<int> pos(ko);  // bit position (LSB = 0) of each op qubit in the block index
-    uint32_t opmask = 0;
-    for (int t = 0; t < ko; t++) {
-        int idx = int(std::find(bq.begin(), bq.end(), oq[t]) - bq.begin());
-        pos[t] = k - 1 - idx;
-        opmask |= 1u << pos[t];
-    }
-    auto extract = [&](int j) {
-        int v = 0;
-        for (int t = 0; t < ko; t++) v = (v << 1) | ((j >> pos[t]) & 1);
-        return v;
-    };
-    auto deposit = [&](int v) {
-        int j = 0;
-        for (int t = 0; t < ko; t++)
-            if ((v >> (ko - 1 - t)) & 1) j |= 1 << pos[t];
-        return j;
-    };
+    const Embedding e(bq, oq);
+    const int dim = e.dim, odim = e.odim;
     std::vector<cplx> out(size_t(dim) * dim, cplx(0));
     for (int r = 0; r < dim; r++) {
-        int ro = extract(r);
-        int rest = r & ~int(opmask);
-        for (int c = 0; c < dim; c++) {
-            cplx s(0);
-            for (int x = 0; x < odim; x++) {
-                cplx e = om[size_t(ro) * odim + x];
-                if (e.re == 0.0 && e.im == 0.0) continue;
-                int mid = rest | deposit(x);
-                s = s + e * acc[size_t(mid) * dim + c];
-            }
-            out[size_t(r) * dim + c] = s;
+        const int ro = e.ext[size_t(r)];
+        const int rest = r & ~int(e.opmask);
+        cplx* o = &out[size_t(r) * dim];
+        for (int x = 0; x < odim; x++) {
+            const cplx m = om[size_t(ro) * odim + x];
+            if (m.re == 0.0 && m.im == 0.0) continue;
+            const cplx* a = &acc[size_t(rest | e.dep[size_t(x)]) * dim];
+            for (int c = 0; c < dim; c++) o[c] = o[c] + m * a[c];
         }
     }
     acc.swap(out);
@@ -120,7 +138,12 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
     const size_t N = ops.size();
     std::vector<std::vector<uint64_t>> qs(N);
     for (size_t i = 0; i < N; i++) qs[i] = ops[i].touched();
+    uint64_t maxq = 0;
+    for (auto& q : qs)
+        for (auto v : q) maxq = std::max(maxq, v);
     std::vector<char> done(N, 0);
+    std::vector<char> blocked(size_t(maxq) + 1, 0);
+    std::vector<uint64_t> blocked_list;
     std::vector<Operation> out;
     for (size_t first = 0; first < N; first++) {
         if (done[first]) continue;
@@ -133,23 +156,29 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
         std::vector<uint64_t> bq = qs[first];
         done[first] = 1;
         // qubits blocked by an unfused operation that stays after this block
-        std::set<uint64_t> blocked;
+        for (auto q : blocked_list) blocked[size_t(q)] = 0;
+        blocked_list.clear();
         for (size_t o = first + 1; o < N; o++) {
             if (done[o]) continue;
             bool touches_blocked = false;
-            for (auto q : qs[o])
-                if (blocked.count(q)) touches_blocked = true;
-            std::set<uint64_t> uni(bq.begin(), bq.end());
-            for (auto q : qs[o]) uni.insert(q);
-            if (!touches_blocked && uni.size() <= size_t(width)) {
+            size_t uni = bq.size();
+            for (auto q : qs[o]) {
+                if (blocked[size_t(q)]) touches_blocked = true;
+                if (std::find(bq.begin(), bq.end(), q) == bq.end()) uni++;
+            }
+            if (!touches_blocked && uni <= size_t(width)) {
                 for (auto q : qs[o])
                     if (std::find(bq.begin(), bq.end(), q) == bq.end()) bq.push_back(q);
                 members.push_back(o);
                 done[o] = 1;
             } else {
-                for (auto q : qs[o]) blocked.insert(q);
+                for (auto q : qs[o])
+                    if (!blocked[size_t(q)]) {
+                        blocked[size_t(q)] = 1;
+                        blocked_list.push_back(q);
+                    }
             }
-            if (blocked.size() >= 64) break;
+            if (blocked_list.size() >= 64) break;
         }
         if (members.size() == 1) {
             out.push_back(ops[first]);
@@ -157,13 +186,15 @@ std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
         }
         std::sort(bq.begin(), bq.end(), std::greater<uint64_t>());
         const int dim = 1 << bq.size();
-        std::vector<cplx> acc(size_t(dim) * dim, cplx(0));
-        for (int i = 0; i < dim; i++) acc[size_t(i) * dim + i] = cplx(1);
+        std::vector<cplx> acc;
         std::vector<uint64_t> oq;
         std::vector<cplx> om;
         for (size_t mi : members) {
             op_matrix(ops[mi], oq, om);
-            left_multiply(bq, acc, oq, om);
+            if (acc.empty())
+                acc = embed(bq, oq, om);
+            else
+                left_multiply(bq, acc, oq, om);
         }
         Operation d;
         d.type = Operation::Dense;
@@ -219,10 +250,17 @@ uint16_t f16_rn(float v) {
     return uint16_t(sign | q);
 }
 
+// Exact value of finite binary16 bits: a normal number's exponent and
+// fraction move into binary32 fields; a subnormal is its fraction times 2^-24.
 float f16_value(uint16_t h) {
-    const int e = (h >> 10) & 0x1F;
-    const float m = float(h & 0x3FF);
-    const float v = e ? std::ldexp(1024.0f + m, e - 25) : std::ldexp(m, -24);
+    const uint32_t e = (h >> 10) & 0x1Fu, frac = h & 0x3FFu;
+    float v;
+    if (e) {
+        const uint32_t bits = ((e + 112u) << 23) | (frac << 13);
+        std::memcpy(&v, &bits, 4);
+    } else {
+        v = float(frac) * 0x1p-24f;
+    }
     return (h & 0x8000u) ? -v : v;
 }
 
@@ -272,9 +310,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
             uint64_t g = uint64_t(tile_qubits[i]);
             if (std::find(bq.begin(), bq.end(), g) == bq.end()) bq.push_back(g);
         }
-        std::vector<cplx> acc(32 * 32, cplx(0));
-        for (int i = 0; i < 32; i++) acc[size_t(i) * 32 + i] = cplx(1);
-        left_multiply(bq, acc, oq, om);
+        std::vector<cplx> acc = embed(bq, oq, om);
         Blk b;
         for (int t = 0; t < 5; t++) b.q[t] = local[bq[t]];
         b.u = std::move(acc);
@@ -476,6 +512,68 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         fp.block_masks.push_back(mask);
     }
     return fp;
+}
+
+
+FusedTma fused_tma_plan(const std::vector<int>& tile_qubits, int n, uint64_t states) {
+    FusedTma t;
+    const int m = int(tile_qubits.size());
+    if (m != kFusedM || n < kFusedM || states == 0) return t;
+    // Items in ascending bit order: tile chunks (<= 8 bits: a box side is at
+    // most 256 elements) and the gaps between them.
+    struct Item {
+        int lo, bits;
+        bool tile;
+    };
+    std::vector<Item> items;
+    int pos = 0;
+    for (int i = 0; i < m;) {
+        int j = i;
+        while (j + 1 < m && tile_qubits[size_t(j + 1)] == tile_qubits[size_t(j)] + 1) j++;
+        const int a = tile_qubits[size_t(i)], e = tile_qubits[size_t(j)] + 1;
+        if (a > pos) items.push_back({pos, a - pos, false});
+        for (int c = a; c < e; c += 8) items.push_back({c, std::min(8, e - c), true});
+        pos = e;
+        i = j + 1;
+    }
+    uint64_t total = states << n;
+    int total_bits = 0;
+    while ((uint64_t(1) << total_bits) < total) total_bits++;
+    int best_k = 0, best_cov = -1;
+    for (int k = 1; k <= 5 && k <= int(items.size()); k++) {
+        const Item& last = items[size_t(k - 1)];
+        if (!last.tile) continue;
+        // The last dimension's extent and coordinates must stay below 2^31.
+        if (total_bits - last.lo > 31) continue;
+        int cov = 0;
+        for (int i = 0; i < k; i++)
+            if (items[size_t(i)].tile) cov += items[size_t(i)].bits;
+        if (cov > best_cov) {
+            best_cov = cov;
+            best_k = k;
+        }
+    }
+    // At least 2 KiB per box (at most 16 boxes a tile).
+    if (best_k == 0 || best_cov < 8) return t;
+    t.ok = 1;
+    t.dims = best_k;
+    for (int i = 0; i < best_k; i++) {
+        const Item& it = items[size_t(i)];
+        t.lo[i] = it.lo;
+        t.bits[i] = it.bits;
+        t.box[i] = it.tile ? (1u << it.bits) : 1u;
+        t.extent[i] = uint64_t(1) << it.bits;
+    }
+    t.extent[best_k - 1] = total >> t.lo[best_k - 1];
+    t.copies = 1 << (kFusedM - best_cov);
+    t.copy_bytes = uint32_t(8) << best_cov;
+    for (int c = 0; c < t.copies; c++) {
+        uint64_t extra = 0;
+        for (int b = 0; best_cov + b < kFusedM; b++)
+            if ((c >> b) & 1) extra |= uint64_t(1) << tile_qubits[size_t(best_cov + b)];
+        t.copy_step[c] = int32_t(extra >> t.lo[best_k - 1]);
+    }
+    return t;
 }
 
 // ---------------------------------------------------------------------------

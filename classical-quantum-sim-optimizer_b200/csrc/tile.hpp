@@ -116,6 +116,29 @@ struct FusedPass {
     std::vector<uint32_t> block_masks;   // each block's local qubits
 };
 
+// TMA loads of a fused pass's tiles.  The state buffer (8-byte complex64
+// elements) is viewed as a tensor of up to 5 dimensions: dimension i covers
+// global bits [lo[i], lo[i] + bits[i]) and the last dimension in use runs to
+// the top of the buffer.  A tile is a box of that tensor: runs of tile qubits
+// (chunks of at most 8 bits) are copied whole, the gaps between them one
+// element at a time.  Tile qubits above the box come from `copies` boxes,
+// copy c landing copy_bytes * c into the tile and starting copy_step[c]
+// further along the last dimension; each box holds natural local order.
+struct FusedTma {
+    int ok = 0;          // 0: per-thread copies instead (shape or size outside the rules)
+    int dims = 0;        // dimensions in use; the rest have extent 1
+    int lo[5] = {0, 0, 0, 0, 0};
+    int bits[5] = {0, 0, 0, 0, 0};  // span of a bounded dimension; the last one: its box bits
+    uint32_t box[5] = {1, 1, 1, 1, 1};
+    uint64_t extent[5] = {1, 1, 1, 1, 1};
+    int copies = 1;
+    uint32_t copy_bytes = 0;
+    int32_t copy_step[16] = {};
+};
+
+// The TMA view for tiles of `tile_qubits` over `states` states of n qubits.
+FusedTma fused_tma_plan(const std::vector<int>& tile_qubits, int n, uint64_t states);
+
 // A pass's raw operations fused to `width` and lowered to tile-local
 // operations for the CUDA-core tile kernel (matrices appended to `pool`).
 void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,
