@@ -711,7 +711,21 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_lo[i]);
             s += "],\"out_hi\":[";
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_hi[i]);
-            s += "],\"blocks\":[";
+            const FusedTma t = fused_tma_plan(fp.qubits, int(n), 1);
+            s += "],\"tma\":{\"ok\":" + std::to_string(t.ok) + ",\"dims\":" + std::to_string(t.dims) +
+                 ",\"copies\":" + std::to_string(t.copies) + ",\"copy_bytes\":" + std::to_string(t.copy_bytes);
+            const char* names[4] = {"lo", "bits", "box", "extent"};
+            for (int f = 0; f < 4; f++) {
+                s += std::string(",\"") + names[f] + "\":[";
+                for (int i = 0; i < 5; i++) {
+                    const uint64_t v = f == 0 ? uint64_t(t.lo[i]) : f == 1 ? uint64_t(t.bits[i]) : f == 2 ? t.box[i] : t.extent[i];
+                    s += (i ? "," : "") + std::to_string(v);
+                }
+                s += "]";
+            }
+            s += ",\"copy_step\":[";
+            for (int c = 0; c < t.copies; c++) s += (c ? "," : "") + std::to_string(t.copy_step[c]);
+            s += "]},\"blocks\":[";
             for (int bi = 0; bi < fp.nblocks; bi++) {
                 const FusedBlock& b = blocks[size_t(fp.first_block + bi)];
                 s += bi ? ",{" : "{";

@@ -19,6 +19,10 @@
 // four warps.  Group g owns one tile, one 128-column TMEM accumulator and one
 // 32 KB operand buffer (also its stage); one thread of the group issues its
 // MMAs, so some tiles' MMAs run while others are read back, loaded or stored.
+// Tiles arrive by TMA (cp.async.bulk.tensor): the state is viewed as a tensor
+// of up to five dimensions whose boxes are the tile's runs of qubits, so one
+// thread issues a tile's load and no load passes through the LSU; tiles whose
+// qubits need more dimensions fall back to 16-byte cp.async copies.
 // All tiles walk the same block sequence and share the gate images (three
 // buffers, fetched three blocks ahead by whichever group finishes its MMAs on
 // a buffer last).  Hand-offs are mbarriers (copies, MMA completion) and
@@ -26,11 +30,15 @@
 // only by a group-wide vote, so no thread is left waiting on a named barrier.
 // On expiry the CTA records an error, waits (bounded) for its own copies and
 // MMAs, frees its tensor memory and stops.
+#include <cuda.h>
 #include <cuda_fp16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstddef>
 #include <cstdio>
+#include <cstring>
+#include <mutex>
 
 #include "common.hpp"
 #include "tile.hpp"
@@ -55,7 +63,7 @@ constexpr uint32_t kOffTabs = kOffU + kUBufs * kUBytes;  // lo_tab[64], hi_tab[6
 constexpr uint32_t kOffIO = kOffTabs + 128 * 8;          // in_lo, in_hi, out_lo, out_hi [64] (u16)
 constexpr uint32_t kOffDesc = kOffIO + 4 * 64 * 2;       // block-table buffers
 constexpr uint32_t kOffBar = kOffDesc + kTBufs * kDescBytes;  // mbarriers, 8-byte aligned
-constexpr uint32_t kOffWsum = kOffBar + 16 * 8;          // per-warp tile-norm partials (double)
+constexpr uint32_t kOffWsum = kOffBar + 32 * 8;          // per-warp tile-norm partials (double)
 constexpr uint32_t kSmemBytes = kOffWsum + kGroups * kGroupWarps * 8;
 constexpr uint64_t kSpinLimit = uint64_t(1) << 26;       // polls of an mbarrier before giving up
 constexpr long long kWaitCycles = 4000000000LL;          // ... or this many SM cycles
@@ -70,12 +78,14 @@ constexpr uint32_t kBarUFull = 0;                     // [kUBufs] gate image of 
 constexpr uint32_t kBarTFull = kBarUFull + kUBufs;    // [kTBufs] block tables of buffer b landed (expect_tx)
 constexpr uint32_t kBarMma = kBarTFull + kTBufs;      // [kGroups] MMAs of group g's tile complete (commit)
 constexpr uint32_t kBarDrain = kBarMma + kGroups;     // [kGroups] group g's MMAs in flight complete (abort path)
-constexpr uint32_t kNumBars = kBarDrain + kGroups;
-static_assert(kNumBars <= 16, "mbarrier slots");
+constexpr uint32_t kBarTile = kBarDrain + kGroups;    // [kGroups] TMA loads of group g's next tile landed (expect_tx)
+constexpr uint32_t kNumBars = kBarTile + kGroups;
+static_assert(kNumBars <= 32, "mbarrier slots");
 
 struct FusedQubits {
     int q[kFusedM];
     uint16_t io[4][64];  // in_lo, in_hi, out_lo, out_hi
+    FusedTma tma;        // tile loads by TMA when tma.ok
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -139,6 +149,15 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(bar)
                  : "memory");
+}
+
+// One box of the tile tensor map into shared memory (5 coordinates).
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, const int32_t* c, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(bar)
+        : "memory");
 }
 
 // Barrier over one group (named barrier 1 + g, 256 threads).
@@ -211,7 +230,8 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t t, int n, const FusedQubi
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-    k_fused(float2* __restrict__ s, int n, FusedQubits fq, const FusedBlock* __restrict__ blocks, int nblocks,
+    k_fused(float2* __restrict__ s, int n, const __grid_constant__ FusedQubits fq,
+            const __grid_constant__ CUtensorMap tile_map, const FusedBlock* __restrict__ blocks, int nblocks,
             const uint16_t* __restrict__ upool, uint64_t total_tiles, int* __restrict__ err,
             const double* __restrict__ in_norm, double* __restrict__ tile_norm) {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -292,9 +312,34 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t st = 0;
     bool ok = !s_abort;
     // Tile t into this group's operand buffer as raw complex64 in natural local
-    // order, 16 bytes per copy (local qubit 0 is global qubit 0); issued as soon
-    // as the buffer is free, read back at the start of the tile.
+    // order (local qubit 0 is global qubit 0), issued as soon as the buffer is
+    // free and read back at the start of the tile: by TMA (one thread issues the
+    // boxes, the tile's mbarrier counts the bytes) or by 16-byte copies of every
+    // thread.
+    const bool use_tma = fq.tma.ok != 0;
+    uint32_t tiles_loaded = 0, tiles_landed = 0;
     auto prefetch = [&](uint64_t tt) {
+        if (use_tma) {
+            tiles_loaded++;
+            if (gt != 0) return;
+            const uint64_t b = tile_base(tt, n, fq);
+            int32_t c[5] = {0, 0, 0, 0, 0}, top = 0;
+            const int last = fq.tma.dims - 1;
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                if (i < last) c[i] = int32_t((b >> fq.tma.lo[i]) & ((uint64_t(1) << fq.tma.bits[i]) - 1));
+                if (i == last) top = int32_t(b >> fq.tma.lo[i]);
+            }
+            const uint32_t tb = bar(kBarTile + uint32_t(g));
+            mbar_expect(tb, kTileBytes);
+            for (int cp = 0; cp < fq.tma.copies; cp++) {
+#pragma unroll
+                for (int i = 0; i < 5; i++)
+                    if (i == last) c[i] = top + fq.tma.copy_step[cp];
+                tma_load_5d(smem_addr(x) + uint32_t(cp) * fq.tma.copy_bytes, &tile_map, c, tb);
+            }
+            return;
+        }
         const float2* __restrict__ src = s + tile_base(tt, n, fq);
 #pragma unroll
         for (int k = 0; k < 16; k++)
@@ -318,8 +363,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const float fs = float(scale * double(kScale));
         const uint64_t fs2 = pack2(__float_as_uint(fs), __float_as_uint(fs));
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        group_sync(g);  // the group's copies of this tile have landed
+        if (use_tma) {
+            // Every thread observes the tile's mbarrier phase (bounded), then votes.
+            const bool landed = mbar_wait(bar(kBarTile + uint32_t(g)), tiles_landed & 1u);
+            tiles_landed++;
+            if (!group_all(landed, g)) {
+                ok = false;
+                break;
+            }
+        } else {
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            group_sync(g);  // the group's copies of this tile have landed
+        }
         {
             float4 v[16];
 #pragma unroll
@@ -437,6 +492,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // stage reads before the next tile's TMA writes
         group_sync(g);  // stage read and partial sums written
         if (t + uint64_t(kGroups) * gridDim.x < total_tiles) prefetch(t + uint64_t(kGroups) * gridDim.x);
         if (gt == 0) {
@@ -467,6 +523,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             bar(kBarDrain + g))
                      : "memory");
         mbar_wait(bar(kBarDrain + g), 0);
+        // A tile load still in flight lands before the CTA exits.
+        for (uint32_t l = tiles_landed; l < tiles_loaded; l++) mbar_wait(bar(kBarTile + uint32_t(g)), l & 1u);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -526,6 +584,45 @@ void fused_renormalize(const Batch& b, const double* norm) {
     if (e != cudaSuccess) fail(kCudaError, std::string("renormalize: ") + cudaGetErrorString(e));
 }
 
+namespace {
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// The 5-dimensional view of the state buffer that the tile boxes come from;
+// false when the driver cannot encode it (the pass then loads per thread).
+bool encode_tile_map(const FusedTma& t, void* amps, uint64_t total, CUtensorMap* map) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || !t.ok) return false;
+    cuuint64_t dim[5], stride[4];
+    cuuint32_t box[5], estride[5] = {1, 1, 1, 1, 1};
+    const uint64_t pad = ((total * 8 + 15) / 16) * 16;  // stride of unused dimensions (extent 1)
+    for (int i = 0; i < 5; i++) {
+        dim[i] = t.extent[i];
+        box[i] = t.box[i];
+        if (i > 0) stride[i - 1] = i < t.dims ? (uint64_t(8) << t.lo[i]) : pad;
+    }
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, amps, dim, stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev, int* err,
                 const double* in_norm, double* tile_norm) {
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
@@ -540,6 +637,10 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
         fq.io[2][e] = p.out_lo[e];
         fq.io[3][e] = p.out_hi[e];
     }
+    CUtensorMap tile_map;
+    std::memset(&tile_map, 0, sizeof tile_map);
+    fq.tma = fused_tma_plan(p.qubits, b.n, b.W);
+    if (fq.tma.ok && !encode_tile_map(fq.tma, b.amps, b.W << b.n, &tile_map)) fq.tma.ok = 0;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -554,7 +655,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     // One CTA per SM, persistent over groups of kGroups tiles.
     const uint64_t total = b.W << (b.n - kFusedM);
     const uint64_t grid = std::min<uint64_t>((total + kGroups - 1) / kGroups, uint64_t(sm_count()));
-    k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq,
+    k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq, tile_map,
                                                                blocks_dev + p.first_block, p.nblocks, upool_dev, total,
                                                                err, in_norm, tile_norm);
     cudaError_t e = cudaGetLastError();

@@ -56,6 +56,16 @@ PACKED = np.arange(4096)
 SLOT_OF_PACKED = operand_offset(PACKED) // 4  # 4-byte operand slot holding packed position p
 
 
+def tile_bases(T, n, tiles):
+    other = [q for q in range(n) if q not in T]
+    return ((tiles >> (n - 12)) << n) | deposit(tiles & ((1 << (n - 12)) - 1), other)
+
+
+def random_circuit_n(n, gates, seed):
+    ins = [g for g in random_circuit(seed, n, gates) if g.get("kind") not in ("barrier", "measure", "reset")]
+    return Circuit(n, ins)
+
+
 def emulate(plan):
     n = plan["n"]
     upool = np.asarray(plan["upool"], dtype=np.uint16).view(np.float16)
@@ -117,6 +127,46 @@ def test_gate_images_are_f16_hi_lo_pairs():
         # lo is at most half an f16 unit of hi: it carries the next 11 bits
         assert np.all(np.abs(lo.astype(np.float64)) <= np.abs(hi.astype(np.float64)) * 2.0 ** -11 + 2.0 ** -24)
     assert plan["passes"][0]["blocks"][-1]["last"] == 1
+
+
+def tma_tile(tma, base):
+    """Global element index of each local index of the tile whose local index 0 is at `base`, as the TMA boxes load it."""
+    dims, lo, box = tma["dims"], tma["lo"], tma["box"]
+    coord = [(base >> lo[i]) & ((1 << tma["bits"][i]) - 1) for i in range(dims - 1)] + [base >> lo[dims - 1]]
+    per_copy = tma["copy_bytes"] // 8
+    out = np.empty(per_copy * tma["copies"], dtype=np.int64)
+    e = np.arange(per_copy)
+    for c in range(tma["copies"]):
+        addr = np.zeros(per_copy, dtype=np.int64)
+        rem = e.copy()
+        for i in range(dims):  # box elements in row-major order, dimension 0 fastest
+            k = rem % box[i]
+            rem //= box[i]
+            ci = coord[i] + (tma["copy_step"][c] if i == dims - 1 else 0)
+            addr += (ci + k) << lo[i]
+        out[c * per_copy:(c + 1) * per_copy] = addr
+    return out
+
+
+@pytest.mark.parametrize("maker", [lambda: brickwork(30, 40, seed=0, measure=False), lambda: qft(26, seed=0),
+                                   lambda: hea(22, 8, seed=0), lambda: brickwork(14, 8, seed=3, measure=False),
+                                   lambda: random_circuit_n(20, 400, 5)])
+def test_tma_boxes_load_each_tile_in_natural_order(maker):
+    plan = _core.fused_plan_dump(maker().model_dump_json())
+    n = plan["n"]
+    local = np.arange(4096)
+    for p in plan["passes"]:
+        tma = p["tma"]
+        if not tma["ok"]:
+            continue
+        assert tma["dims"] <= 5 and max(tma["box"]) <= 256 and tma["copies"] <= 16
+        assert all(b * 8 % 16 == 0 for b in tma["box"][:1])  # inner box side: whole 16-byte units
+        assert tma["copy_bytes"] * tma["copies"] == 32768
+        T = p["qubits"]
+        for t in (0, 1, (1 << (n - 12)) - 1, 12345 % (1 << (n - 12))):
+            base = int(tile_bases(T, n, np.array([t]))[0])
+            assert np.array_equal(tma_tile(tma, base), base | deposit(local, T))
+    assert any(p["tma"]["ok"] for p in plan["passes"])
 
 
 def test_operand_offsets_are_a_bijection():
