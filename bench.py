@@ -331,15 +331,18 @@ def main():
     roof = fused_roofline(plan64, st64, args.qubits)
     del plan128, sim128
 
-    # End to end through the public API: host JSON in, host counts out.
+    # End to end through the public API: host JSON in, host counts out (median of three calls after one warm-up).
     api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64", device=local)
     api.simulate_shots(circuit, shots=args.shots)
-    t0 = time.perf_counter()
-    counts = api.simulate_shots(circuit, shots=args.shots)
-    e2e_s = time.perf_counter() - t0
-    assert sum(counts.values()) == args.shots
+    e2e_runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        counts = api.simulate_shots(circuit, shots=args.shots)
+        e2e_runs.append(time.perf_counter() - t0)
+        assert sum(counts.values()) == args.shots
+    e2e_s = statistics.median(e2e_runs)
     e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": len(circuit.model_dump_json()),
-           "d2h_bytes_per_step": 8 * args.shots}
+           "d2h_bytes_per_step": 8 * args.shots, "runs_s": e2e_runs}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -517,9 +520,47 @@ def run_learned(args):
         results.append(row)
         _core.set_cost_model(sim, None)
         del learned, greedy
+    # CUDA-core tiles in complex128: the model picks each pass's fusion width (1, 2 or 3)
+    # against the greedy fixed width 2, trained on passes recorded at all three widths.
+    model128 = _core.CostModel(seed=args.seed + 1)
+    t0 = time.perf_counter()
+    for fw in (1, 2, 3):
+        rec = dqsim.StatevectorSimulator(seed=1, precision="complex128", execution="tiled", fusion_width=fw,
+                                         max_memory_mb=1 << 20)
+        for n in (22, 24, 26):
+            model128.record(rec, dqsim.workloads.brickwork(n, 20, seed=3000 + 10 * n + fw, measure=False))
+            model128.record(rec, dqsim.workloads.qft(n, seed=4000 + n + fw))
+    record128_s = time.perf_counter() - t0
+    samples128 = model128.num_samples
+    mse128 = model128.train(epochs=60, lr=2e-3)
+    results128 = []
+    for n in (26, 30):
+        for kind, circuit in (("brickwork-d40", dqsim.workloads.brickwork(n, 40, seed=9100 + n, measure=False)),
+                              ("qft", dqsim.workloads.qft(n, seed=9200 + n))):
+            sim = dqsim.StatevectorSimulator(seed=1, execution="tiled", max_memory_mb=1 << 20)
+            _core.set_cost_model(sim, model128)
+            learned = _core.PreparedCircuit(sim, circuit)
+            info = learned.planner()
+            log = _core.planner_log(sim)[-1]
+            greedy = _core.PreparedCircuit(dqsim.StatevectorSimulator(seed=1, execution="tiled",
+                                                                      max_memory_mb=1 << 20), circuit)
+            tl = min(learned.run() for _ in range(2))
+            tg = min(greedy.run() for _ in range(2))
+            fid, err = learned.compare(greedy)
+            widths = log.get("widths") or []
+            results128.append({"circuit": kind, "qubits": n, "greedy_ms": tg, "kept_ms": tl,
+                               "ab_greedy_ms": info["greedy_ms"], "ab_learned_ms": info["learned_ms"],
+                               "rejected": info["rejected"], "gain": tg / tl,
+                               "widths_chosen": {str(w): widths.count(w) for w in sorted(set(widths))},
+                               "fidelity_vs_greedy": fid, "max_amp_err_vs_greedy": err})
+            _core.set_cost_model(sim, None)
+            del learned, greedy
     print(json.dumps({"workload": "learned-vs-greedy", "samples": samples, "record_s": record_s,
                       "train_mse": mse, "results": results,
-                      "rejection_rate": sum(r["rejected"] for r in results) / len(results)}))
+                      "rejection_rate": sum(r["rejected"] for r in results) / len(results),
+                      "complex128_tiles": {"samples": samples128, "record_s": record128_s, "train_mse": mse128,
+                                           "results": results128,
+                                           "rejection_rate": sum(r["rejected"] for r in results128) / len(results128)}}))
     return 0
 
 
