@@ -94,6 +94,20 @@ def brickwork(n, depth, seed=0, measure=True):
     return workloads.brickwork(n, depth, seed=seed, measure=measure)
 
 
+def spread_brickwork(n, qubits, depth, seed=0):
+    """Brickwork on a chosen set of qubits only (neighbours in the list are CX partners):
+    a fused pass then has to hold exactly those qubits, however scattered they are."""
+    rng = np.random.default_rng(seed)
+    ins = []
+    for layer in range(depth):
+        for q in qubits:
+            th, ph, la = (float(x) for x in rng.uniform(0.0, 2 * math.pi, size=3))
+            ins.append(inst("u3", qubit=q, theta=th, phi=ph, lam=la))
+        for i in range(layer % 2, len(qubits) - 1, 2):
+            ins.append(inst("cx", control=qubits[i], target=qubits[i + 1]))
+    return Circuit(n, ins)
+
+
 def qft(n, seed=0):
     return workloads.qft(n, seed=seed)
 

@@ -169,6 +169,16 @@ def test_tma_boxes_load_each_tile_in_natural_order(maker):
     assert any(p["tma"]["ok"] for p in plan["passes"])
 
 
+def test_scattered_tiles_fall_back_to_per_thread_copies():
+    from helpers import spread_brickwork
+
+    scattered = [0, 1] + list(range(3, 22, 2))
+    plan = _core.fused_plan_dump(spread_brickwork(24, scattered, 6, seed=1).model_dump_json())
+    assert plan["passes"] and all(p["qubits"] == scattered for p in plan["passes"])
+    assert not any(p["tma"]["ok"] for p in plan["passes"])
+    check(spread_brickwork(16, [0, 1, 3, 5, 6, 7, 9, 10, 11, 13, 14, 15], 6, seed=2))
+
+
 def test_operand_offsets_are_a_bijection():
     offs = operand_offset(PACKED)
     assert len(set(offs.tolist())) == 4096 and offs.max() < 16384 and np.all(offs % 4 == 0)

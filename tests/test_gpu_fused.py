@@ -38,6 +38,16 @@ def test_fused_matches_oracle(maker):
     check(maker())
 
 
+def test_fused_scattered_tile_uses_per_thread_copies():
+    """A pass over qubits 0, 1 and every odd qubit up to 21 needs more than five
+    TMA dimensions per box, so its tiles load by 16-byte copies instead."""
+    from helpers import spread_brickwork
+
+    c = spread_brickwork(24, [0, 1] + list(range(3, 22, 2)), 8, seed=3)
+    assert not any(p["tma"]["ok"] for p in _core.fused_plan_dump(c.model_dump_json())["passes"])
+    check(c)
+
+
 @pytest.mark.parametrize("seed", range(3))
 def test_fused_random_circuits(seed):
     check(Circuit(15, random_circuit(seed, 15, 200)))
