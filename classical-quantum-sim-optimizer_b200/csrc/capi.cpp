@@ -280,6 +280,10 @@ int dq_result_amplitudes(const dq_result* r, const uint64_t* indices, uint64_t c
     });
 }
 
+int dq_debug_fused_fault(uint64_t withhold_step, double wait_ms) {
+    return guard([&] { k::set_fused_fault(withhold_step, wait_ms); });
+}
+
 int dq_result_pauli_expectation(const dq_result* r, uint64_t x_mask, uint64_t z_mask, double* re, double* im) {
     return guard([&] {
         need(r, "result");

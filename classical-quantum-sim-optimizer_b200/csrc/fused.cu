@@ -82,10 +82,18 @@ constexpr uint32_t kBarTile = kBarDrain + kGroups;    // [kGroups] TMA loads of 
 constexpr uint32_t kNumBars = kBarTile + kGroups;
 static_assert(kNumBars <= 32, "mbarrier slots");
 
+// Failure-path tests: gate images of steps >= withhold are never fetched, so
+// the waits on them run out after wait_cycles (a flag that nothing sets).
+struct FusedFault {
+    uint64_t withhold = ~uint64_t(0);
+    long long wait_cycles = kWaitCycles;
+};
+
 struct FusedQubits {
     int q[kFusedM];
     uint16_t io[4][64];  // in_lo, in_hi, out_lo, out_hi
     FusedTma tma;        // tile loads by TMA when tma.ok
+    FusedFault fault;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -131,12 +139,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false once about kWaitCycles SM cycles (about 2 s) have passed.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait: false once `limit` SM cycles (kWaitCycles: about 2 s) have passed.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
     const long long start = clock64();
     for (uint64_t i = 0; i < kSpinLimit; i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - start > kWaitCycles) return false;
+        if (clock64() - start > limit) return false;
     }
     return false;
 }
@@ -253,7 +261,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t u0 = smem_addr(sm + kOffU);
     // Copies of step st: its block's gate image into buffer st % kUBufs and
     // its tables into buffer st % kTBufs.
+    const long long wl = fq.fault.wait_cycles;
     auto fetch = [&](uint64_t st) {
+        if (st >= fq.fault.withhold) return;
         const FusedBlock* blk = blocks + int(st % uint64_t(nblocks));
         const uint32_t ub = uint32_t(st % kUBufs), tb = uint32_t(st % kTBufs);
         mbar_expect(bar(kBarUFull + ub), kUBytes);
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint64_t fs2 = pack2(__float_as_uint(fs), __float_as_uint(fs));
         if (use_tma) {
             // Every thread observes the tile's mbarrier phase (bounded), then votes.
-            const bool landed = mbar_wait(bar(kBarTile + uint32_t(g)), tiles_landed & 1u);
+            const bool landed = mbar_wait(bar(kBarTile + uint32_t(g)), tiles_landed & 1u, wl);
             tiles_landed++;
             if (!group_all(landed, g)) {
                 ok = false;
@@ -398,7 +408,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool w = true;
             const uint32_t ub = uint32_t(st % kUBufs);
             if (gt == 0) {
-                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u);
+                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u, wl);
                 if (w) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
                     const uint64_t desc_u = make_desc_sw128(u0 + ub * kUBytes);
@@ -422,8 +432,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                                  : "memory");
                 }
                 // The rest of the group waits in the vote below, not on the mbarriers.
-                w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u);
-                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)), uint32_t(st / kTBufs) & 1u);
+                w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u, wl);
+                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)), uint32_t(st / kTBufs) & 1u, wl);
             }
             mma_cnt++;
             if (!group_all(w, g)) {
@@ -514,17 +524,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         // (each issuing thread commits and waits for its own MMAs).
         if (g == 0) {
             const uint64_t fetched = s_fetched;
-            for (uint64_t f = fetched > kTBufs ? fetched - kTBufs : 0; f < fetched; f++) {
-                if (f + kUBufs >= fetched) mbar_wait(bar(kBarUFull + uint32_t(f % kUBufs)), uint32_t(f / kUBufs) & 1u);
-                mbar_wait(bar(kBarTFull + uint32_t(f % kTBufs)), uint32_t(f / kTBufs) & 1u);
+            for (uint64_t f = fetched > kTBufs ? fetched - kTBufs : 0; f < fetched && f < fq.fault.withhold; f++) {
+                if (f + kUBufs >= fetched)
+                    mbar_wait(bar(kBarUFull + uint32_t(f % kUBufs)), uint32_t(f / kUBufs) & 1u, wl);
+                mbar_wait(bar(kBarTFull + uint32_t(f % kTBufs)), uint32_t(f / kTBufs) & 1u, wl);
             }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
             bar(kBarDrain + g))
                      : "memory");
-        mbar_wait(bar(kBarDrain + g), 0);
+        mbar_wait(bar(kBarDrain + g), 0, wl);
         // A tile load still in flight lands before the CTA exits.
-        for (uint32_t l = tiles_landed; l < tiles_loaded; l++) mbar_wait(bar(kBarTile + uint32_t(g)), l & 1u);
+        for (uint32_t l = tiles_landed; l < tiles_loaded; l++) mbar_wait(bar(kBarTile + uint32_t(g)), l & 1u, wl);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -621,7 +632,21 @@ bool encode_tile_map(const FusedTma& t, void* amps, uint64_t total, CUtensorMap*
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+FusedFault g_fault;  // default: nothing withheld, ~2 s waits
+
 }  // namespace
+
+void set_fused_fault(uint64_t withhold_step, double wait_ms) {
+    FusedFault f;
+    f.withhold = withhold_step;
+    if (wait_ms > 0) {
+        int dev = 0, khz = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
+        f.wait_cycles = (long long)(wait_ms * double(khz > 0 ? khz : 1965000));
+    }
+    g_fault = f;
+}
 
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev, int* err,
                 const double* in_norm, double* tile_norm) {
@@ -640,6 +665,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     CUtensorMap tile_map;
     std::memset(&tile_map, 0, sizeof tile_map);
     fq.tma = fused_tma_plan(p.qubits, b.n, b.W);
+    fq.fault = g_fault;
     if (fq.tma.ok && !encode_tile_map(fq.tma, b.amps, b.W << b.n, &tile_map)) fq.tma.ok = 0;
     static bool configured[64] = {};
     int dev = 0;

@@ -162,6 +162,10 @@ void fused_state_norm(const Batch& b, const double* tile_norm, double* norm);
 // Divides every state by the square root of its norm (FP64 scale).
 void fused_renormalize(const Batch& b, const double* norm);
 size_t fused_smem_bytes();
+// Failure-path tests: gate images of fused steps >= withhold_step are never
+// fetched, and every bounded wait of the fused kernel gives up after wait_ms
+// (<= 0: the default of about 2 s).  ~0 restores normal operation.
+void set_fused_fault(uint64_t withhold_step, double wait_ms);
 }  // namespace k
 
 namespace k {

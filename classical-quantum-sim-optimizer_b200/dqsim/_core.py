@@ -734,6 +734,17 @@ def fused_plan_dump(circuit_json):
         _string_free(ctypes.cast(out, ctypes.c_void_p))
 
 
+_debug_fused_fault = _sig("dq_debug_fused_fault", [ctypes.c_uint64, ctypes.c_double])
+
+
+def debug_fused_fault(withhold_step=None, wait_ms=0.0):
+    """Failure-path testing of the fused kernel: gate images of fused steps >=
+    withhold_step are never fetched and its bounded waits give up after wait_ms
+    (<= 0: about 2 s); the call then raises RuntimeError.  No arguments: normal."""
+    step = (1 << 64) - 1 if withhold_step is None else int(withhold_step)
+    _check(_debug_fused_fault(step, float(wait_ms)))
+
+
 def library_path():
     return str(_LIB_PATH)
 

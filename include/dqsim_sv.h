@@ -263,8 +263,17 @@ DQ_API int dq_compile_dump(const char* json, size_t json_len, char** out_text);
  * counterpart in the reference; it exposes the planner for inspection. */
 DQ_API int dq_tile_plan_dump(const char* json, size_t json_len, int tile_qubits, int fusion_width, char** out_text);
 /* Host-only: the tensor-core fused plan (12-qubit passes of 32x32 blocks: layout
- * tables and TF32 hi/lo gate images) as JSON text.  No counterpart in the reference. */
+ * tables, f16 hi/lo gate images and each pass's TMA box plan) as JSON text.  No
+ * counterpart in the reference. */
 DQ_API int dq_fused_plan_dump(const char* json, size_t json_len, char** out_text);
+/* Failure-path testing of the fused tensor-core kernel (no counterpart in the
+ * reference): from the next launch on, gate images of fused steps >=
+ * withhold_step are never fetched, and every bounded wait of the kernel gives
+ * up after wait_ms milliseconds (<= 0: the default, about 2 s).  A pass that
+ * runs out sets the device error flag and the call raises DQ_RUNTIME_ERROR;
+ * the context stays usable.  withhold_step = UINT64_MAX restores normal
+ * operation.  Process-wide; not for concurrent use. */
+DQ_API int dq_debug_fused_fault(uint64_t withhold_step, double wait_ms);
 DQ_API void dq_string_free(char* s);
 
 #ifdef __cplusplus

@@ -48,6 +48,24 @@ def test_fused_scattered_tile_uses_per_thread_copies():
     check(c)
 
 
+def test_fused_bounded_wait_reports_and_recovers():
+    """A gate image that never arrives (its fetch withheld: a flag nothing sets)
+    makes the kernel's bounded waits run out: the CTAs drain, free their tensor
+    memory and set the error flag, the call raises RuntimeError, and the same
+    simulator then runs normally."""
+    c = brickwork(14, 10, seed=2, measure=False)
+    sim = fused(seed=3)
+    try:
+        _core.debug_fused_fault(withhold_step=2, wait_ms=20.0)
+        with pytest.raises(RuntimeError, match="bounded wait"):
+            sim.simulate(c)
+    finally:
+        _core.debug_fused_fault()
+    got = sim.simulate(c).statevector
+    want = o.OracleSimulator(seed=3, max_memory_mb=1 << 16).simulate(c).statevector
+    assert abs(np.vdot(got, want)) ** 2 >= 1 - 1e-6
+
+
 @pytest.mark.parametrize("seed", range(3))
 def test_fused_random_circuits(seed):
     check(Circuit(15, random_circuit(seed, 15, 200)))
