@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "common.hpp"
 #include "kernels.hpp"
@@ -401,14 +402,25 @@ __global__ void __launch_bounds__(256) k_marginal(const V* __restrict__ s, int n
 constexpr int kScanItems = 8;
 constexpr int kScanTile = 256 * kScanItems;
 
-__global__ void __launch_bounds__(256) k_scan_tiles(double* __restrict__ x, uint64_t len, double* __restrict__ sums) {
+// Tile-local inclusive scan of `in` into x (V = double: in == x, in place;
+// V = float2 / double2: the squared magnitudes of a state, as k_norm2 computes
+// them, so the probability table is never written and re-read).
+template <typename V>
+__global__ void __launch_bounds__(256) k_scan_tiles(const V* __restrict__ in, double* __restrict__ x, uint64_t len,
+                                                    double* __restrict__ sums) {
     __shared__ double warp_tot[8];
     const uint64_t base = uint64_t(blockIdx.x) * kScanTile + uint64_t(threadIdx.x) * kScanItems;
     double v[kScanItems];
     double run = 0.0;
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        double e = (base + i < len) ? x[base + i] : 0.0;
+        double e = 0.0;
+        if (base + i < len) {
+            if constexpr (std::is_same<V, double>::value)
+                e = in[base + i];
+            else
+                e = dev::norm2(in[base + i]);
+        }
         run += e;
         v[i] = run;
     }
@@ -468,16 +480,29 @@ __global__ void k_cdf_normalize_dev(double* __restrict__ cdf, uint64_t len, cons
     }
 }
 
+// With `total` (device scalar, or host value when total_dev is null and
+// total_host > 0) the table holds the unnormalised running sums and each
+// probe normalises the entry it reads exactly as k_cdf_normalize would have
+// stored it (cdf[i] / total, clamped to 1 when clamp, the last entry 1).
 __global__ void k_sample(const double* __restrict__ cdf, uint64_t len, uint64_t seed, uint64_t shots, int per_shot,
+                         const double* __restrict__ total_dev, double total_host, int clamp,
                          uint64_t* __restrict__ out) {
     uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= shots) return;
+    const bool scaled = total_dev != nullptr || total_host > 0.0;
+    const double total = total_dev ? *total_dev : total_host;
     uint64_t v = per_shot ? dev::chacha8_u64(seed + t, 0) : dev::chacha8_u64(seed, t);
     double draw = dev::u64_to_unit(v);
     uint64_t lo = 0, hi = len;
     while (lo < hi) {
         uint64_t mid = lo + (hi - lo) / 2;
-        if (cdf[mid] <= draw)
+        double c = cdf[mid];
+        if (scaled) {
+            c = c / total;
+            if (clamp) c = fmin(c, 1.0);
+            if (mid == len - 1) c = 1.0;
+        }
+        if (c <= draw)
             lo = mid + 1;
         else
             hi = mid;
@@ -781,13 +806,34 @@ size_t scan_tmp_size(uint64_t len) {
 
 void scan(cudaStream_t s, double* x, uint64_t len, double* tmp) {
     uint64_t nb = (len + kScanTile - 1) / kScanTile;
-    k_scan_tiles<<<blocks_for(nb, 1), 256, 0, s>>>(x, len, tmp);
+    k_scan_tiles<double><<<blocks_for(nb, 1), 256, 0, s>>>(x, x, len, tmp);
     check_launch("scan_tiles");
     if (nb > 1) {
         scan(s, tmp, nb, tmp + nb);
         k_scan_add<<<blocks_for(nb - 1, 1), 256, 0, s>>>(x, len, tmp);
         check_launch("scan_add");
     }
+}
+
+void scan_probs(const Batch& b, double* x, double* tmp) {
+    const uint64_t len = uint64_t(1) << b.n;
+    const uint64_t nb = (len + kScanTile - 1) / kScanTile;
+    if (b.c64)
+        k_scan_tiles<float2><<<blocks_for(nb, 1), 256, 0, b.stream>>>(static_cast<const float2*>(b.amps), x, len, tmp);
+    else
+        k_scan_tiles<double2>
+            <<<blocks_for(nb, 1), 256, 0, b.stream>>>(static_cast<const double2*>(b.amps), x, len, tmp);
+    check_launch("scan_probs");
+    if (nb > 1) {
+        scan(b.stream, tmp, nb, tmp + nb);
+        k_scan_add<<<blocks_for(nb - 1, 1), 256, 0, b.stream>>>(x, len, tmp);
+        check_launch("scan_add");
+    }
+}
+
+void take_total(cudaStream_t s, const double* cdf, uint64_t len, double* scalar, int* err) {
+    k_take_total<<<1, 1, 0, s>>>(cdf, len, scalar, err);
+    check_launch("take_total");
 }
 
 void cdf_normalize(cudaStream_t s, double* cdf, uint64_t len, double total, bool clamp) {
@@ -804,7 +850,16 @@ void cdf_normalize_device(cudaStream_t s, double* cdf, uint64_t len, double* sca
 void sample(cudaStream_t s, const double* cdf, uint64_t len, uint64_t seed, uint64_t shots, bool per_shot_seed,
             uint64_t* out) {
     if (shots == 0) return;
-    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(cdf, len, seed, shots, per_shot_seed ? 1 : 0, out);
+    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(cdf, len, seed, shots, per_shot_seed ? 1 : 0, nullptr, 0.0, 0,
+                                                     out);
+    check_launch("sample");
+}
+
+void sample_sums(cudaStream_t s, const double* sums, uint64_t len, const double* total_dev, double total_host,
+                 bool clamp, uint64_t seed, uint64_t shots, bool per_shot_seed, uint64_t* out) {
+    if (shots == 0) return;
+    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(sums, len, seed, shots, per_shot_seed ? 1 : 0, total_dev,
+                                                     total_host, clamp ? 1 : 0, out);
     check_launch("sample");
 }
 

@@ -85,18 +85,20 @@ double Plan::run(bool record) {
     ex_->run(bt, nullptr, record ? &rec : nullptr);
     if (cdf_.p) {
         const uint64_t clen = uint64_t(1) << sample_qubits_.size();
-        if (record) rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 4.0 * 8.0 * clen);
+        // State read once; running sums written, then read and written once more by the tile-offset pass.
+        if (record) rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 3.0 * 8.0 * clen);
         bool full = sample_qubits_.size() == n_;
         for (uint64_t t = 0; full && t < n_; t++) full = sample_qubits_[t] == n_ - 1 - t;
         if (full) {
-            k::norm2(bt, cdf_.as<double>());
+            k::scan_probs(bt, cdf_.as<double>(), tmp_.as<double>());
         } else {
             std::vector<int> q(sample_qubits_.begin(), sample_qubits_.end());
             k::marginal(bt, q, cdf_.as<double>());
+            k::scan(s, cdf_.as<double>(), clen, tmp_.as<double>());
         }
-        k::scan(s, cdf_.as<double>(), clen, tmp_.as<double>());
-        k::cdf_normalize_device(s, cdf_.as<double>(), clen, scalar_.as<double>(), st_.err.as<int>(), false);
-        k::sample(s, cdf_.as<double>(), clen, seed_, shots_, true, idx_.as<uint64_t>());
+        k::take_total(s, cdf_.as<double>(), clen, scalar_.as<double>(), st_.err.as<int>());
+        k::sample_sums(s, cdf_.as<double>(), clen, scalar_.as<double>(), 0.0, false, seed_, shots_, true,
+                       idx_.as<uint64_t>());
         if (record) rec.end();
     }
     cuda_check(cudaEventRecord(b, s), "cudaEventRecord");

@@ -74,10 +74,17 @@ void probs_to(const k::Batch& b, const std::vector<uint64_t>& qubits, double* ou
     }
 }
 
-// Scan probabilities into a CDF on the device; returns the total.
-double build_cdf(cudaStream_t s, double* cdf, uint64_t len, DevMem& tmp) {
+// Running sums of state 0's probabilities over `qubits` on the device (the
+// full register in descending order reads the state directly); returns the total.
+double build_sums(const k::Batch& b, const std::vector<uint64_t>& qubits, double* cdf, uint64_t len, DevMem& tmp) {
+    cudaStream_t s = b.stream;
     tmp.ensure(k::scan_tmp_size(len) * 8, "scan scratch");
-    k::scan(s, cdf, len, tmp.as<double>());
+    if (is_full_descending(qubits, uint64_t(b.n))) {
+        k::scan_probs(b, cdf, tmp.as<double>());
+    } else {
+        probs_to(b, qubits, cdf);
+        k::scan(s, cdf, len, tmp.as<double>());
+    }
     double total = 0;
     cuda_check(cudaMemcpyAsync(&total, cdf + (len - 1), 8, cudaMemcpyDeviceToHost, s), "read total");
     cuda_check(cudaStreamSynchronize(s), "stream synchronize");
@@ -214,13 +221,11 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 DevMem cdf, tmp, idx;
                 const uint64_t clen = uint64_t(1) << kq;
                 cdf.alloc_on(clen * 8, s, "the sampling table");
-                probs_to(b, qubits, cdf.as<double>());
-                double total = build_cdf(s, cdf.as<double>(), clen, tmp);
+                double total = build_sums(b, qubits, cdf.as<double>(), clen, tmp);
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
-                k::cdf_normalize(s, cdf.as<double>(), clen, total, false);
                 st.amps.release();  // the state is no longer needed (shots.rs:150)
                 idx.alloc(shots * 8, "sampled outcomes");
-                k::sample(s, cdf.as<double>(), clen, seed, shots, true, idx.as<uint64_t>());
+                k::sample_sums(s, cdf.as<double>(), clen, nullptr, total, false, seed, shots, true, idx.as<uint64_t>());
                 std::vector<uint64_t> h(shots);
                 cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
                 cuda_check(cudaStreamSynchronize(s), "stream synchronize");
@@ -414,12 +419,10 @@ std::unordered_map<uint64_t, uint64_t> Result::counts(uint64_t shots, const std:
     DevMem cdf, tmp, idx;
     cdf.alloc(m * 8, "the sampling table");
     k::Batch b = state.view(s, 1);
-    probs_to(b, qubits, cdf.as<double>());
-    double total = build_cdf(s, cdf.as<double>(), m, tmp);
+    double total = build_sums(b, qubits, cdf.as<double>(), m, tmp);
     if (!std::isfinite(total) || total <= 0.0) fail(kRuntimeError, "Cannot sample a state with nonfinite or zero norm");
-    k::cdf_normalize(s, cdf.as<double>(), m, total, true);
     idx.alloc(shots * 8, "sampled outcomes");
-    k::sample(s, cdf.as<double>(), m, seed, shots, false, idx.as<uint64_t>());
+    k::sample_sums(s, cdf.as<double>(), m, nullptr, total, true, seed, shots, false, idx.as<uint64_t>());
     std::vector<uint64_t> h(shots);
     cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
     dev->sync();
