@@ -175,7 +175,7 @@ double2 d2(cplx c) { return make_double2(c.re, c.im); }
 
 const char* kernel_class_name(int c) {
     static const char* names[kcNumClasses] = {"gate1q", "controlled", "diagonal", "swap", "dense",
-                                              "measure", "tile", "fused", "sample"};
+                                              "measure", "tile", "fused", "sample", "norm"};
     return (c >= 0 && c < kcNumClasses) ? names[c] : "?";
 }
 
@@ -198,8 +198,8 @@ cudaEvent_t EventRecorder::take() {
     return e;
 }
 
-void EventRecorder::begin(int cls, double bytes) {
-    Rec r{cls, bytes, take(), take()};
+void EventRecorder::begin(int cls, double bytes, int kernels) {
+    Rec r{cls, bytes, take(), take(), kernels};
     cuda_check(cudaEventRecord(r.a, stream_), "cudaEventRecord");
     recs_.push_back(r);
 }
@@ -217,7 +217,7 @@ void EventRecorder::collect(double* ms, uint64_t* launches, double* bytes) {
         float t = 0;
         cuda_check(cudaEventElapsedTime(&t, r.a, r.b), "cudaEventElapsedTime");
         ms[r.cls] += t;
-        launches[r.cls] += 1;
+        launches[r.cls] += uint64_t(r.kernels);
         bytes[r.cls] += r.bytes;
         pool_.push_back(r.a);
         pool_.push_back(r.b);
@@ -566,13 +566,18 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
             const FusedPass& p = fused_[size_t(s.fused)];
             const size_t tiles = size_t(b.W) << (b.n - kFusedM);
             norm_tiles_.ensure(tiles * 8, "fused tile norms");
-            norm_states_.ensure(size_t(b.W) * 8, "fused state norms");
+            norm_states_.ensure(size_t(b.W) * size_t(k::fused_norm_parts(b.n)) * 8, "fused state norms");
             if (rec) rec->begin(kcFused, step_bytes(si, b));
             k::fused_pass(b, p, fused_blocks_.as<FusedBlock>(), upool_.as<uint16_t>(), b.err,
                           norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>());
+            if (rec) rec->end();
+            const bool last_fused = si + 1 == steps_.size() || steps_[si + 1].fused < 0;
+            // Tile norms read (8 B per tile); the final rescale reads and writes the state.
+            if (rec)
+                rec->begin(kcNorm, double(tiles) * 8.0 + (last_fused ? 2.0 * double(size_t(b.W) << b.n) * 8.0 : 0.0),
+                           last_fused ? 2 : 1);
             k::fused_state_norm(b, norm_tiles_.as<double>(), norm_states_.as<double>());
             norm_pending = true;
-            const bool last_fused = si + 1 == steps_.size() || steps_[si + 1].fused < 0;
             if (last_fused) {
                 k::fused_renormalize(b, norm_states_.as<double>());
                 norm_pending = false;

@@ -83,6 +83,7 @@ enum KernelClass : int {
     kcTile,          // shared-memory multi-gate pass
     kcFused,         // tensor-core fused-block pass
     kcSample,
+    kcNorm,          // FP64 norms and rescaling between fused passes
     kcNumClasses
 };
 const char* kernel_class_name(int c);
@@ -94,7 +95,8 @@ class EventRecorder {
   public:
     explicit EventRecorder(cudaStream_t s) : stream_(s) {}
     ~EventRecorder();
-    void begin(int cls, double bytes);
+    // `kernels`: launches inside the bracket.
+    void begin(int cls, double bytes, int kernels = 1);
     void end();
     // Totals per class: milliseconds, launches, algorithmic bytes.
     void collect(double* ms, uint64_t* launches, double* bytes);
@@ -104,6 +106,7 @@ class EventRecorder {
         int cls;
         double bytes;
         cudaEvent_t a, b;
+        int kernels;
     };
     cudaStream_t stream_;
     std::vector<Rec> recs_;

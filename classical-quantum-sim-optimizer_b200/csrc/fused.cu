@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_fused(float2* __restrict__ s, int n, const __grid_constant__ FusedQubits fq,
             const __grid_constant__ CUtensorMap tile_map, const FusedBlock* __restrict__ blocks, int nblocks,
             const uint16_t* __restrict__ upool, uint64_t total_tiles, int* __restrict__ err,
-            const double* __restrict__ in_norm, double* __restrict__ tile_norm) {
+            const double* __restrict__ in_norm, int norm_parts, double* __restrict__ tile_norm) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
@@ -366,10 +366,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t valid = left < uint64_t(kGroups) ? uint32_t(left) : uint32_t(kGroups);
         const uint64_t base = tile_base(t, n, fq);
         // FP64 renormalisation of the previous pass (tensor-core accumulation
-        // rounds toward zero, so unitary blocks shrink the norm slightly).
+        // rounds toward zero, so unitary blocks shrink the norm slightly): the
+        // state's norm is the fixed-order sum of its partial sums.
         if (in_norm && (base >> n) != scale_state) {
             scale_state = base >> n;
-            scale = 1.0 / sqrt(in_norm[scale_state]);
+            double nrm = 0.0;
+            for (int p = 0; p < norm_parts; p++) nrm += in_norm[scale_state * uint64_t(norm_parts) + uint64_t(p)];
+            scale = 1.0 / sqrt(nrm);
         }
         const float fs = float(scale * double(kScale));
         const uint64_t fs2 = pack2(__float_as_uint(fs), __float_as_uint(fs));
@@ -551,26 +554,38 @@ int sm_count() {
     return c > 0 ? c : 148;
 }
 
-// norm[st] = sum of the state's tile norms, in tile order (one block per state).
-__global__ void k_state_norm(const double* __restrict__ tile_norm, uint64_t tiles_per_state,
+// Tile norms per partial: block (state st, part p) sums tiles
+// [p * kNormChunk, (p + 1) * kNormChunk) of state st in a fixed order, so the
+// state's norm (the sum of its parts in order) is the same on every run.
+constexpr uint64_t kNormChunk = 2048;
+__global__ void k_state_norm(const double* __restrict__ tile_norm, uint64_t tiles_per_state, int parts,
                              double* __restrict__ norm) {
     __shared__ double sm[256];
-    const uint64_t st = blockIdx.x;
+    const uint64_t st = blockIdx.x / uint64_t(parts), p = blockIdx.x % uint64_t(parts);
     const double* t = tile_norm + st * tiles_per_state;
+    const uint64_t lo = p * kNormChunk, hi = lo + kNormChunk < tiles_per_state ? lo + kNormChunk : tiles_per_state;
     double acc = 0.0;
-    for (uint64_t i = threadIdx.x; i < tiles_per_state; i += blockDim.x) acc += t[i];
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += t[i];
     sm[threadIdx.x] = acc;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
         if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) norm[st] = sm[0];
+    if (threadIdx.x == 0) norm[blockIdx.x] = sm[0];
 }
 
-__global__ void k_scale_states(float2* __restrict__ s, int n, uint64_t items, const double* __restrict__ norm) {
+__global__ void k_scale_states(float2* __restrict__ s, int n, uint64_t items, const double* __restrict__ norm,
+                               int parts) {
+    uint64_t cur = ~uint64_t(0);
+    double sc = 1.0;
     for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < items; g += uint64_t(gridDim.x) * blockDim.x) {
-        const double sc = 1.0 / sqrt(norm[g >> n]);
+        if ((g >> n) != cur) {
+            cur = g >> n;
+            double nrm = 0.0;
+            for (int p = 0; p < parts; p++) nrm += norm[cur * uint64_t(parts) + uint64_t(p)];
+            sc = 1.0 / sqrt(nrm);
+        }
         float2 v = s[g];
         s[g] = make_float2(float(double(v.x) * sc), float(double(v.y) * sc));
     }
@@ -580,9 +595,15 @@ __global__ void k_scale_states(float2* __restrict__ s, int n, uint64_t items, co
 
 size_t fused_smem_bytes() { return kSmemBytes; }
 
+int fused_norm_parts(int n) {
+    const uint64_t tiles = uint64_t(1) << (n - kFusedM);
+    return int((tiles + kNormChunk - 1) / kNormChunk);
+}
+
 void fused_state_norm(const Batch& b, const double* tile_norm, double* norm) {
     const uint64_t tiles = uint64_t(1) << (b.n - kFusedM);
-    k_state_norm<<<unsigned(b.W), 256, 0, b.stream>>>(tile_norm, tiles, norm);
+    const int parts = fused_norm_parts(b.n);
+    k_state_norm<<<unsigned(b.W * uint64_t(parts)), 256, 0, b.stream>>>(tile_norm, tiles, parts, norm);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(kCudaError, std::string("state norm: ") + cudaGetErrorString(e));
 }
@@ -590,7 +611,8 @@ void fused_state_norm(const Batch& b, const double* tile_norm, double* norm) {
 void fused_renormalize(const Batch& b, const double* norm) {
     const uint64_t items = b.W << b.n;
     const uint64_t grid = std::min<uint64_t>((items + 255) / 256, uint64_t(sm_count()) * 32);
-    k_scale_states<<<unsigned(grid), 256, 0, b.stream>>>(static_cast<float2*>(b.amps), b.n, items, norm);
+    k_scale_states<<<unsigned(grid), 256, 0, b.stream>>>(static_cast<float2*>(b.amps), b.n, items, norm,
+                                                          fused_norm_parts(b.n));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(kCudaError, std::string("renormalize: ") + cudaGetErrorString(e));
 }
@@ -683,7 +705,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     const uint64_t grid = std::min<uint64_t>((total + kGroups - 1) / kGroups, uint64_t(sm_count()));
     k_fused<<<unsigned(grid), kThreads, kSmemBytes, b.stream>>>(static_cast<float2*>(b.amps), b.n, fq, tile_map,
                                                                blocks_dev + p.first_block, p.nblocks, upool_dev, total,
-                                                               err, in_norm, tile_norm);
+                                                               err, in_norm, fused_norm_parts(b.n), tile_norm);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(kCudaError, std::string("fused pass: ") + cudaGetErrorString(e));
 }

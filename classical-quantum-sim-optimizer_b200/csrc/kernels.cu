@@ -804,6 +804,11 @@ size_t scan_tmp_size(uint64_t len) {
     return total + 1;
 }
 
+int scan_launches(uint64_t len) {
+    const uint64_t nb = (len + kScanTile - 1) / kScanTile;
+    return nb > 1 ? 2 + scan_launches(nb) : 1;
+}
+
 void scan(cudaStream_t s, double* x, uint64_t len, double* tmp) {
     uint64_t nb = (len + kScanTile - 1) / kScanTile;
     k_scan_tiles<double><<<blocks_for(nb, 1), 256, 0, s>>>(x, x, len, tmp);

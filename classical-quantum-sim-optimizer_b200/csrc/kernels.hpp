@@ -72,6 +72,8 @@ void norm2(const Batch& b, double* out);
 void marginal(const Batch& b, const std::vector<int>& qubits, double* out);
 // In-place inclusive FP64 scan; `tmp` needs scan_tmp_size(len) doubles.
 size_t scan_tmp_size(uint64_t len);
+// Kernel launches scan (and scan_probs) makes for `len` entries.
+int scan_launches(uint64_t len);
 void scan(cudaStream_t s, double* x, uint64_t len, double* tmp);
 // cdf[i] = cdf[i] / total (clamped to 1 when clamp), cdf[len-1] = 1.
 void cdf_normalize(cudaStream_t s, double* cdf, uint64_t len, double total, bool clamp);

@@ -85,10 +85,12 @@ double Plan::run(bool record) {
     ex_->run(bt, nullptr, record ? &rec : nullptr);
     if (cdf_.p) {
         const uint64_t clen = uint64_t(1) << sample_qubits_.size();
-        // State read once; running sums written, then read and written once more by the tile-offset pass.
-        if (record) rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 3.0 * 8.0 * clen);
         bool full = sample_qubits_.size() == n_;
         for (uint64_t t = 0; full && t < n_; t++) full = sample_qubits_[t] == n_ - 1 - t;
+        // State read once; running sums written, then read and written once more by the tile-offset pass.
+        if (record)
+            rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 3.0 * 8.0 * clen,
+                      k::scan_launches(clen) + (full ? 0 : 1) + 2);
         if (full) {
             k::scan_probs(bt, cdf_.as<double>(), tmp_.as<double>());
         } else {

@@ -152,14 +152,17 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
 namespace k {
 // One fused pass over every tile of every state (complex64 only).  err: device
 // flag set to 3 when a bounded wait on an mbarrier runs out.
-// in_norm (per state, nullable): squared norm left by the previous fused pass,
-// divided out on load; tile_norm (W * 2^(n-12) doubles) receives each output
-// tile's FP64 squared norm.
+// in_norm (nullable): the previous fused pass's partial norm sums
+// (fused_state_norm's output), divided out on load; tile_norm (W * 2^(n-12)
+// doubles) receives each output tile's FP64 squared norm.
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev,
                 int* err_dev, const double* in_norm, double* tile_norm);
-// norm[st] = fixed-order sum of state st's tile norms.
+// Partial sums of each state's tile norms, fused_norm_parts(n) per state in
+// a fixed order (state st's norm is the in-order sum of norm[st*parts ..]).
+int fused_norm_parts(int n);
 void fused_state_norm(const Batch& b, const double* tile_norm, double* norm);
-// Divides every state by the square root of its norm (FP64 scale).
+// Divides every state by the square root of its norm, summed from the partial
+// sums fused_state_norm left (FP64 scale).
 void fused_renormalize(const Batch& b, const double* norm);
 size_t fused_smem_bytes();
 // Failure-path tests: gate images of fused steps >= withhold_step are never

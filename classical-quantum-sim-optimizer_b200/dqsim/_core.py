@@ -428,7 +428,7 @@ _plan_samples = _sig("dq_plan_samples", [_P, _P, _u64])
 _plan_free = _sig("dq_plan_free", [_P], None)
 _plan_compare = _sig("dq_plan_compare", [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)])
 
-KERNEL_CLASSES = ("gate1q", "controlled", "diagonal", "swap", "dense", "measure", "tile", "fused", "sample")
+KERNEL_CLASSES = ("gate1q", "controlled", "diagonal", "swap", "dense", "measure", "tile", "fused", "sample", "norm")
 
 
 class PreparedCircuit:

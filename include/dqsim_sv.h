@@ -163,13 +163,14 @@ typedef enum dq_kernel_class {
     DQ_K_TILE = 6,
     DQ_K_FUSED = 7,
     DQ_K_SAMPLE = 8,
-    DQ_K_NUM_CLASSES = 9
+    DQ_K_NORM = 9, /* FP64 norms and rescaling between fused passes */
+    DQ_K_NUM_CLASSES = 10
 } dq_kernel_class;
 DQ_API int dq_plan_create(dq_sim* sim, const char* json, size_t json_len, uint64_t shots, dq_plan** out);
 /* One run; *device_ms is the CUDA-event time on the engine stream.  With
  * record != 0 every launch is bracketed by events for dq_plan_stats. */
 DQ_API int dq_plan_run(dq_plan* p, int record, double* device_ms);
-/* Per kernel class of the last recorded run: milliseconds, launches and
+/* Per kernel class of the last recorded run: milliseconds, kernel launches and
  * algorithmic bytes (arrays of DQ_K_NUM_CLASSES entries). */
 DQ_API int dq_plan_stats(const dq_plan* p, double* ms, uint64_t* launches, double* bytes);
 DQ_API int dq_plan_info(const dq_plan* p, uint64_t* num_qubits, uint64_t* num_ops, double* state_bytes);
