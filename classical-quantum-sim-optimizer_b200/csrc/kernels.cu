@@ -464,8 +464,18 @@ __global__ void k_cdf_normalize(double* __restrict__ cdf, uint64_t len, double t
     }
 }
 
-__global__ void k_take_total(const double* __restrict__ cdf, uint64_t len, double* scalar, int* err) {
-    double t = cdf[len - 1];
+// Entry i of running sums kept in two levels: tile-local sums x plus the
+// inclusive sums of whole tiles before it (the same addition k_scan_add makes).
+__device__ __forceinline__ double two_level(const double* __restrict__ x, const double* __restrict__ tiles,
+                                            uint64_t i) {
+    double v = x[i];
+    if (tiles && i >= uint64_t(kScanTile)) v = v + tiles[i / uint64_t(kScanTile) - 1];
+    return v;
+}
+
+__global__ void k_take_total(const double* __restrict__ cdf, uint64_t len, const double* __restrict__ tiles,
+                             double* scalar, int* err) {
+    double t = two_level(cdf, tiles, len - 1);
     *scalar = t;
     if (!(isfinite(t) && t > 0.0)) *err = 1;
 }
@@ -485,8 +495,8 @@ __global__ void k_cdf_normalize_dev(double* __restrict__ cdf, uint64_t len, cons
 // probe normalises the entry it reads exactly as k_cdf_normalize would have
 // stored it (cdf[i] / total, clamped to 1 when clamp, the last entry 1).
 __global__ void k_sample(const double* __restrict__ cdf, uint64_t len, uint64_t seed, uint64_t shots, int per_shot,
-                         const double* __restrict__ total_dev, double total_host, int clamp,
-                         uint64_t* __restrict__ out) {
+                         const double* __restrict__ tiles, const double* __restrict__ total_dev, double total_host,
+                         int clamp, uint64_t* __restrict__ out) {
     uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= shots) return;
     const bool scaled = total_dev != nullptr || total_host > 0.0;
@@ -496,7 +506,7 @@ __global__ void k_sample(const double* __restrict__ cdf, uint64_t len, uint64_t 
     uint64_t lo = 0, hi = len;
     while (lo < hi) {
         uint64_t mid = lo + (hi - lo) / 2;
-        double c = cdf[mid];
+        double c = two_level(cdf, tiles, mid);
         if (scaled) {
             c = c / total;
             if (clamp) c = fmin(c, 1.0);
@@ -820,7 +830,7 @@ void scan(cudaStream_t s, double* x, uint64_t len, double* tmp) {
     }
 }
 
-void scan_probs(const Batch& b, double* x, double* tmp) {
+void scan_probs(const Batch& b, double* x, double* tmp, bool add_tiles) {
     const uint64_t len = uint64_t(1) << b.n;
     const uint64_t nb = (len + kScanTile - 1) / kScanTile;
     if (b.c64)
@@ -831,13 +841,24 @@ void scan_probs(const Batch& b, double* x, double* tmp) {
     check_launch("scan_probs");
     if (nb > 1) {
         scan(b.stream, tmp, nb, tmp + nb);
-        k_scan_add<<<blocks_for(nb - 1, 1), 256, 0, b.stream>>>(x, len, tmp);
-        check_launch("scan_add");
+        if (add_tiles) {
+            k_scan_add<<<blocks_for(nb - 1, 1), 256, 0, b.stream>>>(x, len, tmp);
+            check_launch("scan_add");
+        }
     }
 }
 
-void take_total(cudaStream_t s, const double* cdf, uint64_t len, double* scalar, int* err) {
-    k_take_total<<<1, 1, 0, s>>>(cdf, len, scalar, err);
+void scan_local(cudaStream_t s, double* x, uint64_t len, double* tmp) {
+    uint64_t nb = (len + kScanTile - 1) / kScanTile;
+    k_scan_tiles<double><<<blocks_for(nb, 1), 256, 0, s>>>(x, x, len, tmp);
+    check_launch("scan_tiles");
+    if (nb > 1) scan(s, tmp, nb, tmp + nb);
+}
+
+uint64_t scan_tile_of(uint64_t i) { return i / uint64_t(kScanTile); }
+
+void take_total(cudaStream_t s, const double* cdf, uint64_t len, const double* tiles, double* scalar, int* err) {
+    k_take_total<<<1, 1, 0, s>>>(cdf, len, tiles, scalar, err);
     check_launch("take_total");
 }
 
@@ -847,7 +868,7 @@ void cdf_normalize(cudaStream_t s, double* cdf, uint64_t len, double total, bool
 }
 
 void cdf_normalize_device(cudaStream_t s, double* cdf, uint64_t len, double* scalar, int* err, bool clamp) {
-    k_take_total<<<1, 1, 0, s>>>(cdf, len, scalar, err);
+    k_take_total<<<1, 1, 0, s>>>(cdf, len, nullptr, scalar, err);
     k_cdf_normalize_dev<<<stream_grid(len), 256, 0, s>>>(cdf, len, scalar, clamp ? 1 : 0);
     check_launch("cdf_normalize_device");
 }
@@ -855,15 +876,15 @@ void cdf_normalize_device(cudaStream_t s, double* cdf, uint64_t len, double* sca
 void sample(cudaStream_t s, const double* cdf, uint64_t len, uint64_t seed, uint64_t shots, bool per_shot_seed,
             uint64_t* out) {
     if (shots == 0) return;
-    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(cdf, len, seed, shots, per_shot_seed ? 1 : 0, nullptr, 0.0, 0,
-                                                     out);
+    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(cdf, len, seed, shots, per_shot_seed ? 1 : 0, nullptr, nullptr,
+                                                     0.0, 0, out);
     check_launch("sample");
 }
 
-void sample_sums(cudaStream_t s, const double* sums, uint64_t len, const double* total_dev, double total_host,
-                 bool clamp, uint64_t seed, uint64_t shots, bool per_shot_seed, uint64_t* out) {
+void sample_sums(cudaStream_t s, const double* sums, const double* tiles, uint64_t len, const double* total_dev,
+                 double total_host, bool clamp, uint64_t seed, uint64_t shots, bool per_shot_seed, uint64_t* out) {
     if (shots == 0) return;
-    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(sums, len, seed, shots, per_shot_seed ? 1 : 0, total_dev,
+    k_sample<<<blocks_for(shots, 128), 128, 0, s>>>(sums, len, seed, shots, per_shot_seed ? 1 : 0, tiles, total_dev,
                                                      total_host, clamp ? 1 : 0, out);
     check_launch("sample");
 }

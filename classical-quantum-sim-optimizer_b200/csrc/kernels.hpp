@@ -86,14 +86,23 @@ void sample(cudaStream_t s, const double* cdf, uint64_t len, uint64_t seed, uint
             uint64_t* out);
 // The same over unnormalised running sums: every probe normalises the entry it
 // reads exactly as cdf_normalize would have (by *total_dev when given, else by
-// total_host), so no normalising pass over the table is needed.
-void sample_sums(cudaStream_t s, const double* sums, uint64_t len, const double* total_dev, double total_host,
-                 bool clamp, uint64_t seed, uint64_t shots, bool per_shot_seed, uint64_t* out);
+// total_host), so no normalising pass over the table is needed.  With `tiles`
+// the sums are in two levels (scan_local): entry i is sums[i] plus
+// tiles[i / 2048 - 1], the addition scan would have stored.
+void sample_sums(cudaStream_t s, const double* sums, const double* tiles, uint64_t len, const double* total_dev,
+                 double total_host, bool clamp, uint64_t seed, uint64_t shots, bool per_shot_seed, uint64_t* out);
 // Inclusive running sums of state 0's squared magnitudes (in index order, the
-// same values as norm2 then scan) into x; `tmp` needs scan_tmp_size(2^n) doubles.
-void scan_probs(const Batch& b, double* x, double* tmp);
-// *scalar = cdf[len-1]; *err = 1 when it is not finite and positive.
-void take_total(cudaStream_t s, const double* cdf, uint64_t len, double* scalar, int* err);
+// same values as norm2 then scan) into x; `tmp` needs scan_tmp_size(2^n)
+// doubles.  add_tiles = false leaves them in two levels (see scan_local).
+void scan_probs(const Batch& b, double* x, double* tmp, bool add_tiles = true);
+// scan without its last pass: x holds sums within 2048-entry tiles and tmp[0..)
+// the inclusive sums of whole tiles (entry i of the full scan is x[i] +
+// tmp[i / 2048 - 1] for i >= 2048).
+void scan_local(cudaStream_t s, double* x, uint64_t len, double* tmp);
+uint64_t scan_tile_of(uint64_t i);
+// *scalar = entry len-1 of the (two-level when tiles) sums; *err = 1 when it is
+// not finite and positive.
+void take_total(cudaStream_t s, const double* cdf, uint64_t len, const double* tiles, double* scalar, int* err);
 // Partial sums of conj(a_i) * other_i (other is c128 on the device); returns block count.
 int dot_partials(const Batch& b, const double2* other, double2* partial);
 constexpr int kDotBlocks = 1184;

@@ -87,20 +87,22 @@ double Plan::run(bool record) {
         const uint64_t clen = uint64_t(1) << sample_qubits_.size();
         bool full = sample_qubits_.size() == n_;
         for (uint64_t t = 0; full && t < n_; t++) full = sample_qubits_[t] == n_ - 1 - t;
-        // State read once; running sums written, then read and written once more by the tile-offset pass.
+        // State read once and two-level running sums written once (the sampler adds
+        // each probed entry's tile offset itself).
+        const int scans = k::scan_launches(clen) - (clen > 2048 ? 1 : 0);
         if (record)
-            rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 3.0 * 8.0 * clen,
-                      k::scan_launches(clen) + (full ? 0 : 1) + 2);
+            rec.begin(kcSample, double(uint64_t(1) << n_) * (st_.c64 ? 8.0 : 16.0) + 8.0 * clen,
+                      scans + (full ? 0 : 1) + 2);
         if (full) {
-            k::scan_probs(bt, cdf_.as<double>(), tmp_.as<double>());
+            k::scan_probs(bt, cdf_.as<double>(), tmp_.as<double>(), false);
         } else {
             std::vector<int> q(sample_qubits_.begin(), sample_qubits_.end());
             k::marginal(bt, q, cdf_.as<double>());
-            k::scan(s, cdf_.as<double>(), clen, tmp_.as<double>());
+            k::scan_local(s, cdf_.as<double>(), clen, tmp_.as<double>());
         }
-        k::take_total(s, cdf_.as<double>(), clen, scalar_.as<double>(), st_.err.as<int>());
-        k::sample_sums(s, cdf_.as<double>(), clen, scalar_.as<double>(), 0.0, false, seed_, shots_, true,
-                       idx_.as<uint64_t>());
+        k::take_total(s, cdf_.as<double>(), clen, tmp_.as<double>(), scalar_.as<double>(), st_.err.as<int>());
+        k::sample_sums(s, cdf_.as<double>(), tmp_.as<double>(), clen, scalar_.as<double>(), 0.0, false, seed_,
+                       shots_, true, idx_.as<uint64_t>());
         if (record) rec.end();
     }
     cuda_check(cudaEventRecord(b, s), "cudaEventRecord");

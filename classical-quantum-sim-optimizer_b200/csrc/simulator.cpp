@@ -74,21 +74,25 @@ void probs_to(const k::Batch& b, const std::vector<uint64_t>& qubits, double* ou
     }
 }
 
-// Running sums of state 0's probabilities over `qubits` on the device (the
-// full register in descending order reads the state directly); returns the total.
+// Two-level running sums of state 0's probabilities over `qubits` on the
+// device (sums within 2048-entry tiles in cdf, inclusive sums of whole tiles in
+// tmp; the full register in descending order reads the state directly);
+// returns the total, the last entry of the full running sums.
 double build_sums(const k::Batch& b, const std::vector<uint64_t>& qubits, double* cdf, uint64_t len, DevMem& tmp) {
     cudaStream_t s = b.stream;
     tmp.ensure(k::scan_tmp_size(len) * 8, "scan scratch");
     if (is_full_descending(qubits, uint64_t(b.n))) {
-        k::scan_probs(b, cdf, tmp.as<double>());
+        k::scan_probs(b, cdf, tmp.as<double>(), false);
     } else {
         probs_to(b, qubits, cdf);
-        k::scan(s, cdf, len, tmp.as<double>());
+        k::scan_local(s, cdf, len, tmp.as<double>());
     }
-    double total = 0;
-    cuda_check(cudaMemcpyAsync(&total, cdf + (len - 1), 8, cudaMemcpyDeviceToHost, s), "read total");
+    double last = 0, offset = 0;
+    const uint64_t t = k::scan_tile_of(len - 1);
+    cuda_check(cudaMemcpyAsync(&last, cdf + (len - 1), 8, cudaMemcpyDeviceToHost, s), "read total");
+    if (t > 0) cuda_check(cudaMemcpyAsync(&offset, tmp.as<double>() + (t - 1), 8, cudaMemcpyDeviceToHost, s), "read total");
     cuda_check(cudaStreamSynchronize(s), "stream synchronize");
-    return total;
+    return t > 0 ? last + offset : last;
 }
 
 std::string json_double(double v) {
@@ -225,7 +229,8 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
                 st.amps.release();  // the state is no longer needed (shots.rs:150)
                 idx.alloc(shots * 8, "sampled outcomes");
-                k::sample_sums(s, cdf.as<double>(), clen, nullptr, total, false, seed, shots, true, idx.as<uint64_t>());
+                k::sample_sums(s, cdf.as<double>(), tmp.as<double>(), clen, nullptr, total, false, seed, shots, true,
+                               idx.as<uint64_t>());
                 std::vector<uint64_t> h(shots);
                 cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
                 cuda_check(cudaStreamSynchronize(s), "stream synchronize");
@@ -422,7 +427,8 @@ std::unordered_map<uint64_t, uint64_t> Result::counts(uint64_t shots, const std:
     double total = build_sums(b, qubits, cdf.as<double>(), m, tmp);
     if (!std::isfinite(total) || total <= 0.0) fail(kRuntimeError, "Cannot sample a state with nonfinite or zero norm");
     idx.alloc(shots * 8, "sampled outcomes");
-    k::sample_sums(s, cdf.as<double>(), m, nullptr, total, true, seed, shots, false, idx.as<uint64_t>());
+    k::sample_sums(s, cdf.as<double>(), tmp.as<double>(), m, nullptr, total, true, seed, shots, false,
+                   idx.as<uint64_t>());
     std::vector<uint64_t> h(shots);
     cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
     dev->sync();
