@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __shared__ int s_abort;
     __shared__ unsigned s_ucnt[kUBufs];       // per gate-image buffer: groups whose MMAs on it completed
     __shared__ unsigned long long s_fetched;  // steps whose copies were issued
+    __shared__ int s_gabort[kGroups];         // group g had a wait run out; it stops at its next barrier
     uint64_t* lo_tab = reinterpret_cast<uint64_t*>(sm + kOffTabs);
     uint64_t* hi_tab = lo_tab + 64;
     uint16_t* io = reinterpret_cast<uint16_t*>(sm + kOffIO);  // in_lo | in_hi | out_lo | out_hi
@@ -289,6 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         s_abort = (smem_addr(sm) & 1023u) != 0;
         if (s_abort) atomicExch(err, 3);
         for (uint32_t i = 0; i < kUBufs; i++) s_ucnt[i] = 0;
+        for (int i = 0; i < kGroups; i++) s_gabort[i] = 0;
         for (uint32_t i = 0; i < kNumBars; i++) mbar_init(bar(i), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         uint64_t f = 0;
@@ -408,11 +410,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             asm volatile("tcgen05.fence::before_thread_sync;");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             group_sync(g);
-            bool w = true;
+            // A wait of the previous block ran out: every thread reads the same flag
+            // after the barrier, so the group stops together.
+            if (*static_cast<volatile int*>(&s_gabort[g])) {
+                ok = false;
+                break;
+            }
             const uint32_t ub = uint32_t(st % kUBufs);
             if (gt == 0) {
-                w = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u, wl);
-                if (w) {
+                const bool uw = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u, wl);
+                if (!uw) *static_cast<volatile int*>(&s_gabort[g]) = 1;
+                if (uw) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
                     const uint64_t desc_u = make_desc_sw128(u0 + ub * kUBytes);
                     // Descriptors advance by (byte offset >> 4) in their start-address field.
@@ -434,14 +442,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                         bar(kBarMma + g))
                                  : "memory");
                 }
-                // The rest of the group waits in the vote below, not on the mbarriers.
-                w = w && mbar_wait(bar(kBarMma + g), mma_cnt & 1u, wl);
-                w = w && mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)), uint32_t(st / kTBufs) & 1u, wl);
             }
+            // Every thread waits for the block's products and tables (bounded); one that
+            // runs out marks the group, which stops at its next barrier.
+            // The readback's TMEM loads are warp-collective: a warp reads back only if
+            // every lane saw both waits complete.
+            const bool w = __all_sync(0xffffffffu, mbar_wait(bar(kBarMma + g), mma_cnt & 1u, wl) &&
+                                                       mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)),
+                                                                 uint32_t(st / kTBufs) & 1u, wl));
             mma_cnt++;
-            if (!group_all(w, g)) {
-                ok = false;
-                break;
+            if (!w) {
+                *static_cast<volatile int*>(&s_gabort[g]) = 1;
+                continue;
             }
             if (gt == 0 && st + kUBufs < steps) {
                 // The gate-image buffer is free once every tile's MMAs on it completed:
@@ -497,6 +509,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         asm volatile("tcgen05.fence::before_thread_sync;");
         group_sync(g);  // stage complete
+        if (*static_cast<volatile int*>(&s_gabort[g])) {
+            ok = false;
+            break;
+        }
         float2* __restrict__ gp = s + base;
 #pragma unroll 8
         for (int k = 0; k < 16; k++)  // 16-byte pairs: adjacent stage slots, adjacent in HBM
