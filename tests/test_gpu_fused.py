@@ -66,6 +66,21 @@ def test_fused_bounded_wait_reports_and_recovers():
     assert abs(np.vdot(got, want)) ** 2 >= 1 - 1e-6
 
 
+@pytest.mark.parametrize("maker", [lambda: brickwork(28, 40, seed=11, measure=False), lambda: qft(28, seed=12)])
+def test_fused_at_scale_against_complex128_on_the_device(maker):
+    """28 qubits (2 GiB complex64 against 4 GiB complex128 per-gate, compared on
+    the device): depth-40 brickwork and QFT keep fidelity >= 1 - 1e-6 and max
+    amplitude error <= 1e-5 through ~20 fused passes."""
+    c = maker()
+    got = _core.PreparedCircuit(fused(seed=1), c)
+    got.run()
+    ref = _core.PreparedCircuit(dqsim.StatevectorSimulator(seed=1, max_memory_mb=1 << 16, execution="per_gate"), c)
+    ref.run()
+    fid, err = got.compare(ref)
+    assert abs(1 - fid) <= 1e-6 and err <= 1e-5, (fid, err)
+    assert got.shape()["passes"] >= 10
+
+
 @pytest.mark.parametrize("seed", range(3))
 def test_fused_random_circuits(seed):
     check(Circuit(15, random_circuit(seed, 15, 200)))
