@@ -133,6 +133,150 @@ bool is_identity_1(const cplx& v) { return v.re == 1.0 && v.im == 0.0; }
 
 }  // namespace
 
+namespace {
+
+// The fused operation of `members` (in order) on qubits bq: dense, or diagonal
+// when the product is.
+Operation fused_operation(const std::vector<Operation>& ops, const std::vector<size_t>& members,
+                          std::vector<uint64_t> bq) {
+    std::sort(bq.begin(), bq.end(), std::greater<uint64_t>());
+    const int dim = 1 << bq.size();
+    std::vector<cplx> acc;
+    std::vector<uint64_t> oq;
+    std::vector<cplx> om;
+    for (size_t mi : members) {
+        op_matrix(ops[mi], oq, om);
+        if (acc.empty())
+            acc = embed(bq, oq, om);
+        else
+            left_multiply(bq, acc, oq, om);
+    }
+    Operation d;
+    d.type = Operation::Dense;
+    d.qubits = bq;
+    d.values = acc;
+    d.fused_count = 0;
+    for (size_t mi : members) d.fused_count += ops[mi].fused_count;
+    bool diag = true;
+    for (int r = 0; r < dim && diag; r++)
+        for (int c = 0; c < dim; c++)
+            if (r != c && (acc[size_t(r) * dim + c].re != 0.0 || acc[size_t(r) * dim + c].im != 0.0)) {
+                diag = false;
+                break;
+            }
+    if (diag) {
+        d.type = Operation::Diagonal;
+        std::vector<cplx> dv(dim);
+        for (int i = 0; i < dim; i++) dv[i] = acc[size_t(i) * dim + i];
+        d.values = dv;
+    }
+    return d;
+}
+
+}  // namespace
+
+std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int width) {
+    if (width <= 1) return ops;
+    const size_t N = ops.size();
+    std::vector<uint64_t> mask(N, 0);  // qubit masks (fused passes hold tile-local or global qubits < 64)
+    for (size_t i = 0; i < N; i++)
+        for (auto q : ops[i].touched()) {
+            if (q >= 64) return fuse_ops(ops, width);
+            mask[i] |= uint64_t(1) << q;
+        }
+    std::vector<char> done(N, 0);
+    std::vector<Operation> out;
+    std::vector<size_t> members, best_members;
+    struct Blk {
+        std::vector<size_t> members;
+        uint64_t used;
+    };
+    std::vector<Blk> blocks;
+    // Ops absorbed by a block on qubit set S started at `first`: in order, an op
+    // inside S joins unless an op left out earlier blocks one of its qubits.
+    auto absorb = [&](size_t first, uint64_t S, std::vector<size_t>& mem) {
+        mem.clear();
+        mem.push_back(first);
+        uint64_t blocked = 0;
+        for (size_t o = first + 1; o < N && (blocked & S) != S; o++) {
+            if (done[o]) continue;
+            if ((mask[o] & ~S) == 0 && (mask[o] & blocked) == 0)
+                mem.push_back(o);
+            else
+                blocked |= mask[o];
+        }
+    };
+    for (size_t first = 0; first < N; first++) {
+        if (done[first]) continue;
+        const int k0 = __builtin_popcountll(mask[first]);
+        if (k0 > width) {  // wider than a block: stays on its own
+            done[first] = 1;
+            blocks.push_back({{first}, mask[first]});
+            continue;
+        }
+        // Candidate qubits: the first few distinct qubits of the ops that follow.
+        std::vector<int> cand;
+        uint64_t seen = mask[first];
+        for (size_t o = first + 1; o < N && cand.size() < 16; o++) {
+            if (done[o]) continue;
+            uint64_t fresh = mask[o] & ~seen;
+            while (fresh && cand.size() < 16) {
+                const int q = __builtin_ctzll(fresh);
+                fresh &= fresh - 1;
+                cand.push_back(q);
+                seen |= uint64_t(1) << q;
+            }
+        }
+        const int need = std::min<int>(width - k0, int(cand.size()));
+        // Every subset of `need` candidates (at most C(10, 4) = 210 sets): keep the
+        // block that absorbs the most operations (earliest set on ties).
+        size_t best = 0;
+        best_members.clear();
+        std::vector<int> pick(static_cast<size_t>(need));
+        for (int i = 0; i < need; i++) pick[size_t(i)] = i;
+        while (true) {
+            uint64_t S = mask[first];
+            for (int i = 0; i < need; i++) S |= uint64_t(1) << cand[size_t(pick[size_t(i)])];
+            absorb(first, S, members);
+            if (members.size() > best) {
+                best = members.size();
+                best_members = members;
+            }
+            int i = need - 1;
+            while (i >= 0 && pick[size_t(i)] == int(cand.size()) - need + i) i--;
+            if (i < 0) break;
+            pick[size_t(i)]++;
+            for (int j = i + 1; j < need; j++) pick[size_t(j)] = pick[size_t(j - 1)] + 1;
+        }
+        for (size_t mi : best_members) done[mi] = 1;
+        uint64_t used = 0;
+        for (size_t mi : best_members) used |= mask[mi];
+        blocks.push_back({best_members, used});
+    }
+    // Consecutive blocks whose qubits together fit in `width` run as one (the
+    // fused sequence is a valid order, so their members simply concatenate).
+    std::vector<Blk> merged;
+    for (auto& b : blocks) {
+        if (!merged.empty() && __builtin_popcountll(merged.back().used | b.used) <= width &&
+            __builtin_popcountll(b.used) <= width) {
+            merged.back().members.insert(merged.back().members.end(), b.members.begin(), b.members.end());
+            merged.back().used |= b.used;
+        } else {
+            merged.push_back(std::move(b));
+        }
+    }
+    for (auto& b : merged) {
+        if (b.members.size() == 1) {
+            out.push_back(ops[b.members[0]]);
+            continue;
+        }
+        std::vector<uint64_t> bq;
+        for (uint64_t u = b.used; u; u &= u - 1) bq.push_back(uint64_t(__builtin_ctzll(u)));
+        out.push_back(fused_operation(ops, b.members, bq));
+    }
+    return out;
+}
+
 std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width) {
     if (width <= 1) return ops;
     const size_t N = ops.size();
@@ -301,7 +445,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         int gates = 0;
     };
     std::vector<Blk> blk;
-    for (const Operation& op : fuse_ops(pass_ops, 5)) {
+    for (const Operation& op : fuse_ops_lookahead(pass_ops, 5)) {
         std::vector<uint64_t> oq;
         std::vector<cplx> om;
         op_matrix(op, oq, om);

@@ -78,6 +78,11 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
 // Greedy dependency-respecting fusion of a topologically ordered op list into
 // dense operations of at most `width` qubits (width 1 leaves gates alone).
 std::vector<Operation> fuse_ops(const std::vector<Operation>& ops, int width);
+// The same with a choice per block: of the qubit sets made from the block's
+// first operation and up to `width` of the next few qubits, the set that
+// absorbs the most operations (used for the 5-qubit tensor-core blocks, where
+// every block costs the same whatever it holds).
+std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int width);
 
 // ---------------------------------------------------------------------------
 // Tensor-core fused blocks (complex64): a pass of 12 tile qubits whose
