@@ -184,17 +184,13 @@ std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int
             if (q >= 64) return fuse_ops(ops, width);
             mask[i] |= uint64_t(1) << q;
         }
-    std::vector<char> done(N, 0);
-    std::vector<Operation> out;
-    std::vector<size_t> members, best_members;
     struct Blk {
         std::vector<size_t> members;
         uint64_t used;
     };
-    std::vector<Blk> blocks;
     // Ops absorbed by a block on qubit set S started at `first`: in order, an op
     // inside S joins unless an op left out earlier blocks one of its qubits.
-    auto absorb = [&](size_t first, uint64_t S, std::vector<size_t>& mem) {
+    auto absorb = [&](const std::vector<char>& done, size_t first, uint64_t S, std::vector<size_t>& mem) {
         mem.clear();
         mem.push_back(first);
         uint64_t blocked = 0;
@@ -206,41 +202,42 @@ std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int
                 blocked |= mask[o];
         }
     };
-    for (size_t first = 0; first < N; first++) {
-        if (done[first]) continue;
+    // The `keep` blocks that absorb the most operations among the 5-qubit sets
+    // made of the first unfused operation's qubits and any of the next 12
+    // distinct qubits (at most C(12, 4) = 495 sets; earliest set first on ties).
+    auto candidates = [&](const std::vector<char>& done, size_t first, size_t keep) {
+        std::vector<Blk> top;
         const int k0 = __builtin_popcountll(mask[first]);
         if (k0 > width) {  // wider than a block: stays on its own
-            done[first] = 1;
-            blocks.push_back({{first}, mask[first]});
-            continue;
+            top.push_back({{first}, mask[first]});
+            return top;
         }
-        // Candidate qubits: the first few distinct qubits of the ops that follow.
         std::vector<int> cand;
         uint64_t seen = mask[first];
-        for (size_t o = first + 1; o < N && cand.size() < 16; o++) {
+        for (size_t o = first + 1; o < N && cand.size() < 12; o++) {
             if (done[o]) continue;
-            uint64_t fresh = mask[o] & ~seen;
-            while (fresh && cand.size() < 16) {
+            for (uint64_t fresh = mask[o] & ~seen; fresh && cand.size() < 12; fresh &= fresh - 1) {
                 const int q = __builtin_ctzll(fresh);
-                fresh &= fresh - 1;
                 cand.push_back(q);
                 seen |= uint64_t(1) << q;
             }
         }
         const int need = std::min<int>(width - k0, int(cand.size()));
-        // Every subset of `need` candidates (at most C(10, 4) = 210 sets): keep the
-        // block that absorbs the most operations (earliest set on ties).
-        size_t best = 0;
-        best_members.clear();
         std::vector<int> pick(static_cast<size_t>(need));
         for (int i = 0; i < need; i++) pick[size_t(i)] = i;
+        std::vector<size_t> mem;
         while (true) {
             uint64_t S = mask[first];
             for (int i = 0; i < need; i++) S |= uint64_t(1) << cand[size_t(pick[size_t(i)])];
-            absorb(first, S, members);
-            if (members.size() > best) {
-                best = members.size();
-                best_members = members;
+            absorb(done, first, S, mem);
+            uint64_t used = 0;
+            for (size_t mi : mem) used |= mask[mi];
+            bool dup = false;  // sets that absorb the same operations give the same block
+            for (auto& t : top) dup = dup || t.members == mem;
+            if (!dup) {
+                auto at = std::find_if(top.begin(), top.end(), [&](const Blk& t) { return t.members.size() < mem.size(); });
+                top.insert(at, Blk{mem, used});
+                if (top.size() > keep) top.pop_back();
             }
             int i = need - 1;
             while (i >= 0 && pick[size_t(i)] == int(cand.size()) - need + i) i--;
@@ -248,10 +245,43 @@ std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int
             pick[size_t(i)]++;
             for (int j = i + 1; j < need; j++) pick[size_t(j)] = pick[size_t(j - 1)] + 1;
         }
-        for (size_t mi : best_members) done[mi] = 1;
-        uint64_t used = 0;
-        for (size_t mi : best_members) used |= mask[mi];
-        blocks.push_back({best_members, used});
+        return top;
+    };
+    // Beam search over block sequences: every level adds one block to each kept
+    // sequence; sequences are ranked by the operations they cover, and the
+    // first sequence that covers everything has the fewest blocks found.
+    struct Seq {
+        std::vector<char> done;
+        std::vector<Blk> blocks;
+        size_t covered = 0, first = 0;
+    };
+    constexpr size_t kBeam = 8, kBranch = 8;
+    std::vector<Seq> beam(1);
+    beam[0].done.assign(N, 0);
+    std::vector<Blk> blocks;
+    while (true) {
+        bool finished = false;
+        for (auto& q : beam) {
+            while (q.first < N && q.done[q.first]) q.first++;
+            if (q.first == N) {
+                blocks = q.blocks;
+                finished = true;
+                break;
+            }
+        }
+        if (finished || beam.empty()) break;
+        std::vector<Seq> next;
+        for (auto& q : beam)
+            for (auto& b : candidates(q.done, q.first, kBranch)) {
+                Seq c = q;
+                for (size_t mi : b.members) c.done[mi] = 1;
+                c.covered += b.members.size();
+                c.blocks.push_back(b);
+                next.push_back(std::move(c));
+            }
+        std::stable_sort(next.begin(), next.end(), [](const Seq& a, const Seq& b) { return a.covered > b.covered; });
+        if (next.size() > kBeam) next.resize(kBeam);
+        beam = std::move(next);
     }
     // Consecutive blocks whose qubits together fit in `width` run as one (the
     // fused sequence is a valid order, so their members simply concatenate).
@@ -265,6 +295,7 @@ std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int
             merged.push_back(std::move(b));
         }
     }
+    std::vector<Operation> out;
     for (auto& b : merged) {
         if (b.members.size() == 1) {
             out.push_back(ops[b.members[0]]);

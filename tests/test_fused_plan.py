@@ -190,6 +190,6 @@ def test_fused_block_counts_for_30q_brickwork():
     plan = _core.fused_plan_dump(workloads.brickwork(30, 40, seed=0, measure=False).model_dump_json())
     blocks = sum(len(p["blocks"]) for p in plan["passes"])
     assert len(plan["passes"]) < 40
-    # each block takes the 5-qubit set that absorbs the most operations (124 here;
-    # first-fit fusion gave 141)
-    assert blocks <= 126, blocks
+    # blocks chosen by a beam search over the 5-qubit sets that absorb the most
+    # operations (117 here; first-fit fusion gave 141)
+    assert blocks <= 120, blocks
