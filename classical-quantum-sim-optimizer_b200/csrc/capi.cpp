@@ -644,6 +644,7 @@ int dq_tile_plan_dump(const char* json, size_t len, int tile_qubits, int fusion_
         TilePlanOptions o;
         o.m = tile_qubits;
         o.fuse = std::min(fusion_width, kTileMaxDense);
+        o.beam = kPlanBeam;
         std::vector<double2> pool;
         auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
         std::string s = "{\"n\":" + std::to_string(n) + ",\"passes\":[";
@@ -692,18 +693,21 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
         for (auto& op : ops)
             if (!op.is_unitary()) fail(kValueError, "circuit has non-unitary operations");
         if (n < uint64_t(kFusedM)) fail(kValueError, "fused passes need at least 12 qubits");
-        TilePlanOptions o;
-        o.m = kFusedM;
-        o.keep_raw = true;
-        o.pinned_low = kFusedPinned;
-        std::vector<double2> pool;
-        auto passes = plan_tiles(ops, 0, ops.size(), int(n), o, &pool);
+        // The simulator's own plan (plan_fused), its passes' blocks and gate
+        // images concatenated in pass order.
+        std::vector<BuiltFusedPass> passes = plan_fused(ops, 0, ops.size(), int(n), TilePlanOptions{});
         std::vector<FusedBlock> blocks;
         std::vector<uint16_t> upool;
         std::string s = "{\"n\":" + std::to_string(n) + ",\"passes\":[";
         char buf[48];
         for (size_t pi = 0; pi < passes.size(); pi++) {
-            FusedPass fp = build_fused_pass(passes[pi].raw, passes[pi].qubits, blocks, upool);
+            FusedPass fp = passes[pi].fp;
+            fp.first_block += int(blocks.size());
+            for (FusedBlock b : passes[pi].blocks) {
+                b.u_off += uint32_t(upool.size());
+                blocks.push_back(b);
+            }
+            upool.insert(upool.end(), passes[pi].upool.begin(), passes[pi].upool.end());
             s += pi ? ",{" : "{";
             s += "\"raw\":" + std::to_string(fp.raw_ops) + ",\"qubits\":[";
             for (size_t i = 0; i < fp.qubits.size(); i++) s += (i ? "," : "") + std::to_string(fp.qubits[i]);

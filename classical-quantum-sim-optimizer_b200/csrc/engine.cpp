@@ -4,9 +4,12 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <exception>
 #include <functional>
+#include <mutex>
 #include <thread>
 
 #include "cost.hpp"
@@ -22,28 +25,104 @@ void cuda_check(cudaError_t e, const char* what) {
     fail(kCudaError, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+namespace {
+
+// Host worker threads shared by every parallel_for, started on first use.  A
+// call posts its job, works on it itself, then withdraws it and waits for the
+// workers still inside one of its items; a worker only ever waits for items
+// already running, so nested calls (an item that calls parallel_for) cannot
+// deadlock, and with no workers (e.g. after fork) the caller does every item.
+class WorkerPool {
+  public:
+    struct Job {
+        const std::function<void(size_t)>* fn = nullptr;
+        size_t count = 0;
+        std::atomic<size_t> next{0};
+        int refs = 0;  // workers inside this job (guarded by the pool mutex)
+        std::mutex error_mutex;
+        std::exception_ptr error;
+    };
+
+    explicit WorkerPool(size_t workers) {
+        for (size_t w = 0; w < workers; w++) threads_.emplace_back([this] { loop(); });
+    }
+    ~WorkerPool() {
+        {
+            std::lock_guard<std::mutex> l(mutex_);
+            stop_ = true;
+        }
+        wake_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+
+    void run(Job& job) {
+        {
+            std::lock_guard<std::mutex> l(mutex_);
+            jobs_.push_back(&job);
+        }
+        wake_.notify_all();
+        work(job);
+        std::unique_lock<std::mutex> l(mutex_);
+        auto it = std::find(jobs_.begin(), jobs_.end(), &job);
+        if (it != jobs_.end()) jobs_.erase(it);
+        idle_.wait(l, [&] { return job.refs == 0; });
+    }
+
+  private:
+    static void work(Job& job) {
+        for (size_t i = job.next++; i < job.count; i = job.next++) {
+            try {
+                (*job.fn)(i);
+            } catch (...) {
+                std::lock_guard<std::mutex> l(job.error_mutex);
+                if (!job.error) job.error = std::current_exception();
+                job.next = job.count;
+            }
+        }
+    }
+
+    void loop() {
+        std::unique_lock<std::mutex> l(mutex_);
+        while (true) {
+            wake_.wait(l, [&] { return stop_ || !jobs_.empty(); });
+            if (stop_) return;
+            Job* job = jobs_.front();
+            if (job->next.load() >= job->count) {
+                jobs_.pop_front();
+                continue;
+            }
+            job->refs++;
+            l.unlock();
+            work(*job);
+            l.lock();
+            if (--job->refs == 0) idle_.notify_all();
+        }
+    }
+
+    std::mutex mutex_;
+    std::condition_variable wake_, idle_;
+    std::deque<Job*> jobs_;
+    std::vector<std::thread> threads_;
+    bool stop_ = false;
+};
+
+WorkerPool& worker_pool() {
+    static WorkerPool pool(std::min<size_t>(std::max<size_t>(1, std::thread::hardware_concurrency()), 16) - 1);
+    return pool;
+}
+
+}  // namespace
+
 void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
-    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
-    const size_t workers = std::min<size_t>({count, hw, 16});
-    if (workers <= 1) {
+    if (count <= 1) {
         for (size_t i = 0; i < count; i++) fn(i);
         return;
     }
-    std::atomic<size_t> next{0};
-    std::vector<std::exception_ptr> errors(workers);
-    std::vector<std::thread> pool;
-    for (size_t w = 0; w < workers; w++)
-        pool.emplace_back([&, w] {
-            try {
-                for (size_t i = next++; i < count; i = next++) fn(i);
-            } catch (...) {
-                errors[w] = std::current_exception();
-                next = count;
-            }
-        });
-    for (auto& t : pool) t.join();
-    for (auto& e : errors)
-        if (e) std::rethrow_exception(e);
+    WorkerPool::Job job;
+    job.fn = &fn;
+    job.count = count;
+    worker_pool().run(job);
+    if (job.error) std::rethrow_exception(job.error);
 }
 
 namespace {
@@ -273,48 +352,35 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     o.m = cfg_.tile_m;
     o.fuse = cfg_.fuse;
     o.seeds = cfg_.seeds;
+    o.beam = kPlanBeam;
     o.c64 = cfg_.c64;
     o.model = cfg_.model;
     o.chosen_widths = &widths_;
     if (cfg_.fused && cfg_.c64 && cfg_.n >= kFusedM) {
-        o.m = kFusedM;
-        o.keep_raw = true;
-        o.pinned_low = kFusedPinned;
-        std::vector<TilePass> ps = plan_tiles(ops, begin, end, cfg_.n, o, &pool_host_);
-        // Each pass's choice and fused blocks are independent host work: built on
-        // a few threads into per-pass buffers, then appended in pass order.
-        struct Built {
-            int choice = 0;
-            FusedPass fp;
-            std::vector<FusedBlock> blocks;
-            std::vector<uint16_t> upool;
-        };
-        std::vector<Built> built(ps.size());
-        parallel_for(ps.size(), [&](size_t i) {
-            const TilePass& p = ps[i];
-            Built& bt = built[i];
-            // With a trained cost model each pass runs on whichever executor it
-            // predicts cheapest: tensor-core blocks (0) or CUDA-core tile
-            // operations fused to width 1..kTileMaxDense.
-            bt.fp = build_fused_pass(p.raw, p.qubits, bt.blocks, bt.upool);
-            if (cfg_.model) {
+        std::vector<BuiltFusedPass> built = plan_fused(ops, begin, end, cfg_.n, o);
+        // With a trained cost model each pass runs on whichever executor it
+        // predicts cheapest: tensor-core blocks (0) or CUDA-core tile operations
+        // fused to width 1..kTileMaxDense.
+        std::vector<int> choices(built.size(), 0);
+        if (cfg_.model)
+            parallel_for(built.size(), [&](size_t i) {
+                const BuiltFusedPass& bt = built[i];
                 double best = cfg_.model->predict_fused(bt.fp);
                 for (int w = 1; w <= kTileMaxDense; w++) {
                     std::vector<double2> scratch;
                     std::vector<TileOp> cand;
-                    lower_pass_ops(p.raw, p.qubits, cfg_.n, w, scratch, cand);
+                    lower_pass_ops(bt.src.raw, bt.src.qubits, cfg_.n, w, scratch, cand);
                     const double cost = cfg_.model->predict_ops(cand, kFusedM, true);
                     if (cost < best) {
                         best = cost;
-                        bt.choice = w;
+                        choices[i] = w;
                     }
                 }
-            }
-        });
-        for (size_t i = 0; i < ps.size(); i++) {
-            TilePass& p = ps[i];
-            Built& bt = built[i];
-            const int choice = bt.choice;
+            });
+        for (size_t i = 0; i < built.size(); i++) {
+            BuiltFusedPass& bt = built[i];
+            TilePass& p = bt.src;
+            const int choice = choices[i];
             widths_.push_back(choice);
             Step s;
             s.type = Operation::Dense;

@@ -17,12 +17,13 @@ namespace dq {
 
 void cuda_check(cudaError_t e, const char* what);
 
-// Owning device allocation.  Allocation failure is a MemoryError, as the
-// reference reports a failed statevector reservation (shots.rs:33-41).
-// Runs fn(0) .. fn(count - 1) on up to 16 host threads; the first exception
-// a call throws is rethrown here after every thread has finished.
+// Runs fn(0) .. fn(count - 1) on the calling thread and up to 15 pooled host
+// workers; the first exception a call throws is rethrown here after every
+// item that started has finished (items not yet started are skipped).
 void parallel_for(size_t count, const std::function<void(size_t)>& fn);
 
+// Owning device allocation.  Allocation failure is a MemoryError, as the
+// reference reports a failed statevector reservation (shots.rs:33-41).
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;

@@ -1,11 +1,13 @@
 // Shared-memory tile pass kernel and its host-side planner.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <map>
 #include <set>
 
 #include "common.hpp"
 #include "cost.hpp"
+#include "engine.hpp"
 #include "tile.hpp"
 
 namespace dq {
@@ -758,6 +760,7 @@ namespace {
 
 struct Dag {
     std::vector<std::vector<uint64_t>> qs;
+    std::vector<uint64_t> mask;                  // qubits of each op as a bit mask (n <= 64)
     std::vector<std::vector<size_t>> per_qubit;  // op indices touching each qubit, in order
 };
 
@@ -779,65 +782,209 @@ void take(const Dag& g, PlanState& s, size_t o) {
     while (s.first_open < s.done.size() && s.done[s.first_open]) s.first_open++;
 }
 
-bool subset(const std::vector<uint64_t>& a, const std::vector<char>& inT) {
-    for (auto q : a)
-        if (!inT[q]) return false;
-    return true;
+// The operation at the head of qubit q's list, SIZE_MAX when none is left.
+size_t head_op(const Dag& g, const PlanState& s, size_t q) {
+    return s.head[q] < g.per_qubit[q].size() ? g.per_qubit[q][s.head[q]] : SIZE_MAX;
 }
 
-// Absorb every ready op inside T until nothing changes; returns ops taken.
-size_t closure(const Dag& g, PlanState& s, const std::vector<char>& inT, std::vector<size_t>* taken) {
+// Absorbs every ready op inside T (bit mask) until nothing changes; appends
+// them to `taken` and returns how many.  Only an op at the head of one of its
+// qubits' lists can be ready, and taking an op moves only its own qubits'
+// heads, so a worklist of heads finds the whole closure.
+size_t closure(const Dag& g, PlanState& s, uint64_t T, std::vector<size_t>& taken, std::vector<size_t>& work) {
+    work.clear();
+    for (uint64_t r = T; r; r &= r - 1) {
+        const size_t o = head_op(g, s, size_t(__builtin_ctzll(r)));
+        if (o != SIZE_MAX) work.push_back(o);
+    }
     size_t count = 0;
-    bool changed = true;
-    while (changed) {
-        changed = false;
-        for (size_t o = s.first_open; o < s.done.size(); o++) {
-            if (s.done[o] || !subset(g.qs[o], inT) || !ready(g, s, o)) continue;
-            take(g, s, o);
-            if (taken) taken->push_back(o);
-            count++;
-            changed = true;
-        }
+    while (!work.empty()) {
+        const size_t o = work.back();
+        work.pop_back();
+        if (s.done[o] || (g.mask[o] & ~T) || !ready(g, s, o)) continue;
+        take(g, s, o);
+        taken.push_back(o);
+        count++;
+        for (auto q : g.qs[o])
+            if (head_op(g, s, q) != SIZE_MAX) work.push_back(head_op(g, s, q));
     }
     return count;
 }
 
-// Grow T from a seed op and absorb; returns (ops, T) without committing.
-size_t grow(const Dag& g, PlanState s, size_t seed, int m, int n, int pinned, std::vector<char>& inT,
-            std::vector<size_t>* taken) {
-    inT.assign(n, 0);
-    int size = 0;
-    for (int q = 0; q < pinned && q < n; q++, size++) inT[q] = 1;
-    for (auto q : g.qs[seed])
-        if (!inT[q]) {
-            inT[q] = 1;
-            size++;
+// Reverts the ops in `taken` (first_open is restored by the caller).
+void untake(const Dag& g, PlanState& s, const std::vector<size_t>& taken) {
+    for (size_t i = taken.size(); i-- > 0;) {
+        s.done[taken[i]] = 0;
+        for (auto q : g.qs[taken[i]]) s.head[q]--;
+    }
+}
+
+// What a pass's tile qubits may be: m of them, qubits 0..pinned-1 always, and a
+// spread (below) of at most max_spread.
+//
+// The tiles a pass has in flight at once differ in the lowest `inflight_bits`
+// qubits outside T, so together they read contiguous runs of 2^c amplitudes,
+// c the lowest qubit neither in T nor among those; the high tile qubits
+// scatter those runs.  The spread, in quarters, is 4 per tile qubit at or above
+// spread_bit + 4, 3 per tile qubit in [spread_bit, spread_bit + 4), less 12
+// per tile qubit that lengthens the runs (those in [pinned, c)).
+struct TileShape {
+    int m, n, pinned, spread_bit, max_spread, inflight_bits;
+    int spread(uint64_t T) const {
+        if (spread_bit >= 64) return 0;
+        const uint64_t hi = T >> spread_bit;
+        const int top = __builtin_popcountll(hi >> 4), mid = __builtin_popcountll(hi & 15);
+        int run_bits = 0, outside = 0;
+        for (int q = 0; q < n; q++) {
+            if ((T >> q) & 1) {
+                run_bits += q >= pinned ? 1 : 0;
+            } else if (++outside > inflight_bits) {
+                break;
+            }
         }
-    size_t total = closure(g, s, inT, taken);
+        return 4 * top + 3 * mid - 12 * run_bits;
+    }
+};
+
+// Reused buffers of one thread's grow() calls.
+struct GrowScratch {
+    std::vector<size_t> cands, trial, work;
+    std::vector<uint64_t> tried;
+};
+
+// Grows T from a seed op: the pinned qubits and the seed's, then, while T has
+// room, the new qubits of one ready op at a time.  Of the ready ops whose
+// qubits fit, the one whose new qubits let the most ops in per added qubit is
+// chosen (fewer new qubits, then the earliest op, on ties).  Returns the ops
+// absorbed, in the order taken, and T; `s` is left as it was.
+size_t grow(const Dag& g, PlanState& s, size_t seed, const TileShape& sh, bool lookahead, uint64_t& T,
+            std::vector<size_t>& taken, GrowScratch& x) {
+    const int m = sh.m, n = sh.n;
+    const size_t first_open = s.first_open;
+    taken.clear();
+    T = (sh.pinned >= 64 ? ~uint64_t(0) : (uint64_t(1) << sh.pinned) - 1) | g.mask[seed];
+    if (n < 64) T &= (uint64_t(1) << n) - 1;
+    int size = __builtin_popcountll(T);
+    closure(g, s, T, taken, x.work);
     while (size < m) {
-        // the ready op needing the fewest new qubits (earliest on ties)
+        x.cands.clear();
+        for (size_t q = 0; q < size_t(n); q++) {
+            const size_t o = head_op(g, s, q);
+            if (o != SIZE_MAX && ready(g, s, o)) x.cands.push_back(o);
+        }
+        std::sort(x.cands.begin(), x.cands.end());
+        x.cands.erase(std::unique(x.cands.begin(), x.cands.end()), x.cands.end());
         size_t best = SIZE_MAX;
-        int best_new = 1 << 30;
-        for (size_t o = s.first_open; o < s.done.size(); o++) {
-            if (s.done[o] || !ready(g, s, o)) continue;
-            int nw = 0;
-            for (auto q : g.qs[o]) nw += inT[q] ? 0 : 1;
+        size_t best_gain = 0;
+        int best_new = 1;
+        x.tried.clear();  // new-qubit sets already scored
+        for (size_t o : x.cands) {
+            const uint64_t fresh = g.mask[o] & ~T;
+            const int nw = __builtin_popcountll(fresh);
             if (nw == 0 || size + nw > m) continue;
-            if (nw < best_new) {
-                best_new = nw;
+            if (std::find(x.tried.begin(), x.tried.end(), fresh) != x.tried.end()) continue;
+            x.tried.push_back(fresh);
+            if (sh.spread(T | fresh) > sh.max_spread) continue;
+            size_t gain = 0;
+            if (lookahead) {
+                const size_t fo = s.first_open;
+                x.trial.clear();
+                gain = closure(g, s, T | fresh, x.trial, x.work);
+                untake(g, s, x.trial);
+                s.first_open = fo;
+            }
+            // gain / nw > best_gain / best_new, or equal with fewer new qubits
+            const size_t lhs = gain * size_t(best_new), rhs = best_gain * size_t(nw);
+            if (best == SIZE_MAX || lhs > rhs || (lhs == rhs && nw < best_new)) {
                 best = o;
-                if (nw == 1) break;
+                best_gain = gain;
+                best_new = nw;
             }
         }
         if (best == SIZE_MAX) break;
-        for (auto q : g.qs[best])
-            if (!inT[q]) {
-                inT[q] = 1;
-                size++;
-            }
-        total += closure(g, s, inT, taken);
+        T |= g.mask[best];
+        size = __builtin_popcountll(T);
+        closure(g, s, T, taken, x.work);
     }
+    const size_t total = taken.size();
+    untake(g, s, taken);
+    s.first_open = first_open;
     return total;
+}
+
+// One pass of a plan: its tile qubits (before padding) and the ops it takes.
+struct PassChoice {
+    uint64_t T = 0;
+    std::vector<size_t> taken;
+};
+
+// Chooses the passes.  Each pass is grown from one of the first `seeds` ready
+// ops by either growth rule (fewest new qubits; most ops let in per new
+// qubit); a beam of `beam` partial plans, ranked by the ops they cover after
+// the same number of passes, keeps the best extensions, and the first plan to
+// cover every op wins (beam 1: the single best pass each time).
+std::vector<PassChoice> choose_passes(const Dag& g, const TileShape& sh, int seeds, int beam) {
+    const size_t N = g.qs.size();
+    struct Node {
+        PlanState s;
+        size_t covered = 0;
+        std::vector<int> chain;  // indices into `arena`
+    };
+    std::vector<PassChoice> arena;
+    std::vector<Node> nodes(1);
+    nodes[0].s.head.assign(size_t(sh.n), 0);
+    nodes[0].s.done.assign(N, 0);
+    while (true) {
+        for (const Node& nd : nodes)
+            if (nd.s.first_open >= N) {
+                std::vector<PassChoice> out;
+                for (int i : nd.chain) out.push_back(arena[size_t(i)]);
+                return out;
+            }
+        struct Cand {
+            size_t node, covered;
+            PassChoice pc;
+        };
+        // Each node's extensions, distinct by tile qubits (the same qubits from
+        // the same state take the same ops); nodes expand on separate threads.
+        std::vector<std::vector<Cand>> per_node(nodes.size());
+        auto expand = [&](size_t ni) {
+            Node& nd = nodes[ni];
+            std::vector<Cand>& out = per_node[ni];
+            uint64_t T = 0;
+            std::vector<size_t> taken;
+            GrowScratch x;
+            std::vector<size_t> seed_ops;
+            for (size_t o = nd.s.first_open; o < N && int(seed_ops.size()) < seeds; o++)
+                if (!nd.s.done[o] && ready(g, nd.s, o)) seed_ops.push_back(o);
+            for (int la = 0; la < 2; la++)
+                for (size_t sd : seed_ops) {
+                    const size_t c = grow(g, nd.s, sd, sh, la == 1, T, taken, x);
+                    bool dup = false;
+                    for (size_t k = 0; k < out.size() && !dup; k++) dup = out[k].pc.T == T;
+                    if (!dup) out.push_back(Cand{ni, nd.covered + c, PassChoice{T, taken}});
+                }
+        };
+        if (nodes.size() > 1)
+            parallel_for(nodes.size(), expand);
+        else
+            expand(0);
+        std::vector<Cand> cands;
+        for (auto& v : per_node)
+            for (auto& c : v) cands.push_back(std::move(c));
+        std::stable_sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.covered > y.covered; });
+        if (cands.size() > size_t(beam)) cands.resize(size_t(beam));
+        std::vector<Node> next;
+        for (Cand& c : cands) {
+            Node nd = nodes[c.node];
+            for (size_t o : c.pc.taken) take(g, nd.s, o);
+            nd.covered = c.covered;
+            nd.chain.push_back(int(arena.size()));
+            arena.push_back(std::move(c.pc));
+            next.push_back(std::move(nd));
+        }
+        nodes = std::move(next);
+    }
 }
 
 TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::vector<double2>& pool,
@@ -946,6 +1093,60 @@ TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::ve
 
 }  // namespace
 
+std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                                       const TilePlanOptions& base) {
+    TilePlanOptions o = base;
+    o.m = kFusedM;
+    o.keep_raw = true;
+    o.pinned_low = kFusedPinned;
+    o.spread_bit = kFusedSpreadBit;
+    o.beam = kPlanBeam;
+    o.model = nullptr;
+    o.chosen_widths = nullptr;
+    // Where the cap can bind (the largest spread, every qubit from
+    // kFusedSpreadBit up in the tile, exceeds it) also plan with no cap (-1),
+    // the spread priced into the plan's cost instead, and with a cap one
+    // top qubit (4 quarters) lower.
+    std::vector<int> caps{kFusedMaxSpread};
+    if (4 * (n - kFusedSpreadBit) - 4 > kFusedMaxSpread) {
+        caps.push_back(-1);
+        caps.push_back(kFusedMaxSpread - 4);
+    }
+    std::vector<std::vector<BuiltFusedPass>> plans(caps.size());
+    parallel_for(caps.size(), [&](size_t i) {
+        TilePlanOptions oi = o;
+        oi.max_spread = caps[i];
+        std::vector<double2> unused;
+        std::vector<TilePass> ps = plan_tiles(ops, begin, end, n, oi, &unused);
+        std::vector<BuiltFusedPass>& plan = plans[i];
+        plan.resize(ps.size());
+        parallel_for(ps.size(), [&](size_t k) {
+            BuiltFusedPass& b = plan[k];
+            b.fp = build_fused_pass(ps[k].raw, ps[k].qubits, b.blocks, b.upool);
+            b.src = std::move(ps[k]);
+        });
+    });
+    const TileShape sh{kFusedM, n, kFusedPinned, kFusedSpreadBit, INT_MAX, o.inflight_bits};
+    size_t best = 0;
+    double best_cost = 0;
+    for (size_t i = 0; i < plans.size(); i++) {
+        double cost = kFusedPassCostBlocks * double(plans[i].size());
+        for (const BuiltFusedPass& b : plans[i]) {
+            uint64_t T = 0;
+            for (int q : b.src.qubits) T |= uint64_t(1) << q;
+            const int spread = sh.spread(T);
+            cost += b.fp.nblocks + (spread > kFusedMaxSpread + 4   ? kFusedSpreadCostBlocks[1]
+                                    : spread > kFusedMaxSpread ? kFusedSpreadCostBlocks[0]
+                                                               : 0.0);
+        }
+        if (i == 0 || cost < best_cost) {
+            best = i;
+            best_cost = cost;
+        }
+    }
+    return std::move(plans[best]);
+}
+
 void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,
                     std::vector<double2>& pool, std::vector<TileOp>& out) {
     std::vector<int> local(size_t(n), -1);
@@ -963,34 +1164,30 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
     for (size_t i = begin; i < end; i++) widest = std::max(widest, int(ops[i].touched().size()));
     const int pinned = std::min(std::max(opt.pinned_low, 0), n);
     const int m = std::min(std::max(opt.m, widest + pinned), n);
+    if (n > 64) fail(kValueError, "tile passes take at most 64 qubits");
     Dag g;
     g.qs.resize(N);
+    g.mask.assign(N, 0);
     g.per_qubit.assign(n, {});
     for (size_t i = 0; i < N; i++) {
         g.qs[i] = ops[begin + i].touched();
-        for (auto q : g.qs[i]) g.per_qubit[q].push_back(i);
-    }
-    PlanState s;
-    s.head.assign(n, 0);
-    s.done.assign(N, 0);
-    while (s.first_open < N) {
-        // candidate seeds: the first `seeds` ready ops
-        std::vector<size_t> seeds;
-        for (size_t o = s.first_open; o < N && int(seeds.size()) < std::max(1, opt.seeds); o++)
-            if (!s.done[o] && ready(g, s, o)) seeds.push_back(o);
-        size_t best_seed = seeds[0], best_count = 0;
-        for (size_t sd : seeds) {
-            std::vector<char> inT;
-            size_t c = grow(g, s, sd, m, n, pinned, inT, nullptr);
-            if (c > best_count) {
-                best_count = c;
-                best_seed = sd;
-            }
+        for (auto q : g.qs[i]) {
+            g.per_qubit[q].push_back(i);
+            g.mask[i] |= uint64_t(1) << q;
         }
-        std::vector<char> inT;
-        std::vector<size_t> taken;
-        grow(g, s, best_seed, m, n, pinned, inT, &taken);
-        for (size_t o : taken) take(g, s, o);
+    }
+    const int beam = N > kPlanBeamMaxOps ? 1 : std::max(1, opt.beam);
+    // A seed's own qubits are always allowed; the cap applies to the rest.
+    TileShape sh{m, n, pinned, std::max(opt.spread_bit, 0), opt.max_spread >= 0 ? opt.max_spread : INT_MAX,
+                 std::max(opt.inflight_bits, 0)};
+    const std::vector<PassChoice> chosen = choose_passes(g, sh, std::max(1, opt.seeds), beam);
+    for (const PassChoice& pc : chosen) {
+        std::vector<char> inT(size_t(n), 0);
+        for (int q = 0; q < n; q++) inT[size_t(q)] = char((pc.T >> q) & 1);
+        std::vector<size_t> taken = pc.taken;
+        // Circuit order is a valid order for any set of ops, and the block
+        // fusion below starts each block at the first op left.
+        std::sort(taken.begin(), taken.end());
         // pad T to m qubits with the lowest free qubits (longer contiguous rows)
         int size = 0;
         for (int q = 0; q < n; q++) size += inT[q];

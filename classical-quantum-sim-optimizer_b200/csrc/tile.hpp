@@ -60,7 +60,24 @@ struct TilePlanOptions {
     // Qubits 0..pinned_low-1 belong to every tile, so each thread's run of
     // amplitudes in HBM is 2^pinned_low elements long (whole 32-byte sectors).
     int pinned_low = 0;
+    // Partial plans kept by the pass search (1: the single best pass each
+    // time).  Circuits of more than kPlanBeamMaxOps operations use 1.
+    int beam = 1;
+    // Tile qubits at or above spread_bit scatter the contiguous runs that the
+    // tiles in flight together read (tiles in flight differ in the lowest
+    // inflight_bits qubits outside the tile); a pass's spread, in quarters
+    // (4 per tile qubit from spread_bit + 4 up, 3 per tile qubit in
+    // [spread_bit, spread_bit + 4), less 12 per tile qubit that lengthens
+    // those runs), is at most max_spread (-1: no limit).  See kFusedSpreadBit.
+    int spread_bit = 0;
+    int max_spread = -1;
+    int inflight_bits = 9;
 };
+
+constexpr size_t kPlanBeamMaxOps = 50000;
+// Beam width of the prepared and per-call simulator plans (batched circuits
+// plan with 1: hundreds of circuits are planned per call).
+constexpr int kPlanBeam = 8;
 
 // Widest dense operation a tile pass applies on CUDA cores (register budget).
 constexpr int kTileMaxDense = 3;
@@ -71,7 +88,12 @@ inline bool tileable(const Operation& op) {
     return op.is_unitary() && !(op.type == Operation::Dense && op.qubits.size() > size_t(kTileMaxDense));
 }
 
-// Plans passes over ops[begin, end) (tileable operations only).
+// Plans passes over ops[begin, end) (tileable operations only).  Each pass is
+// grown from one of the first `seeds` ready operations by one of two rules
+// (add the ready operation needing the fewest new qubits; add the one whose new
+// qubits let the most operations in per qubit), a beam of `beam` partial plans
+// ranked by the operations covered keeps the best extensions, and the first
+// plan to cover the range wins.  A pass lists its operations in circuit order.
 std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
                                  const TilePlanOptions& opt, std::vector<double2>* pool);
 
@@ -92,6 +114,14 @@ std::vector<Operation> fuse_ops_lookahead(const std::vector<Operation>& ops, int
 // ---------------------------------------------------------------------------
 constexpr int kFusedM = 12;            // tile qubits of a fused pass
 constexpr int kFusedPinned = 2;        // low qubits in every fused tile (32-byte runs of complex64)
+// Fused passes keep their spread (TilePlanOptions) at most kFusedMaxSpread
+// quarters over qubits from kFusedSpreadBit (2^20 complex64 = 8 MiB) up; about
+// 2^9 tiles (148 CTAs x 4) are in flight.  Fitted to 450 single passes of three
+// blocks over 327 tile qubit sets at 30 and 32 qubits: spread <= 24 took
+// 0.95-1.17 of the median time, 25-28 1.29-1.44, above 28 1.29-1.76 (at 30
+// qubits the median is 11.4 ms; five sets fall on the wrong side of 24).
+constexpr int kFusedSpreadBit = 20;
+constexpr int kFusedMaxSpread = 24;
 constexpr int kFusedCols = 1 << (kFusedM - 5);
 constexpr int kFusedUHalves = 2 * 64 * 64;  // U_hi and U_lo images of one block (f16)
 
@@ -153,6 +183,33 @@ void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& t
 // and f16 hi/lo gate images (K-major, 128-byte swizzled operand layout).
 FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
                            std::vector<FusedBlock>& blocks, std::vector<uint16_t>& upool);
+
+// A fused pass with its own block descriptors and gate images (block offsets
+// relative to its own arrays).
+struct BuiltFusedPass {
+    TilePass src;
+    FusedPass fp;
+    std::vector<FusedBlock> blocks;
+    std::vector<uint16_t> upool;
+};
+
+// A pass's fixed cost (loads, stores, norms) in units of one block's: at 30
+// qubits a pass of b blocks took about 3 + b ms (1 block 3.96 ms, 5 blocks
+// 8.2-8.3 ms, 7 blocks 9.6-9.96 ms).
+constexpr double kFusedPassCostBlocks = 3.0;
+// The added cost of a pass whose spread exceeds kFusedMaxSpread by at most 4
+// quarters, and by more (at 30 qubits about +4 ms and +8 ms).
+constexpr double kFusedSpreadCostBlocks[2] = {4.0, 8.0};
+
+// Plans ops[begin, end) as fused passes (kFusedM tile qubits, kFusedPinned
+// pinned, beam kPlanBeam) under the spread cap kFusedMaxSpread, one less, and
+// none, where they can bind, builds every pass's blocks, and returns the plan of
+// lowest kFusedPassCostBlocks * passes + blocks + kFusedSpreadCostBlocks for
+// passes over the cap (the pass search follows ops covered, not blocks, so the
+// caps give different plans).  `base` supplies seeds; the other planning
+// fields are set here.
+std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                                       const TilePlanOptions& base);
 
 namespace k {
 // One fused pass over every tile of every state (complex64 only).  err: device

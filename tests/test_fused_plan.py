@@ -189,7 +189,44 @@ def test_fused_block_counts_for_30q_brickwork():
 
     plan = _core.fused_plan_dump(workloads.brickwork(30, 40, seed=0, measure=False).model_dump_json())
     blocks = sum(len(p["blocks"]) for p in plan["passes"])
-    assert len(plan["passes"]) < 40
-    # blocks chosen by a beam search over the 5-qubit sets that absorb the most
-    # operations (117 here; first-fit fusion gave 141)
-    assert blocks <= 120, blocks
+    # passes from a beam search over pass sequences, blocks from a beam search
+    # over the 5-qubit sets that absorb the most operations (first-fit fusion
+    # gave 141 blocks); the plan's estimated cost is 3 per pass + 1 per block
+    # (24 passes and 107 blocks here; 23 and 117 from one pass at a time by the
+    # fewest-new-qubits rule)
+    assert blocks <= 110, blocks
+    assert 3 * len(plan["passes"]) + blocks <= 180
+
+
+def _spread(qubits, spread_bit=20, pinned=2, inflight=9):
+    T = set(qubits)
+    high = sum(1 for q in T if q >= spread_bit)
+    run = outside = 0
+    for q in range(64):
+        if q in T:
+            run += q >= pinned
+        else:
+            outside += 1
+            if outside > inflight:
+                break
+    return high - 2 * run
+
+
+@pytest.mark.parametrize("name, cost_max", [("bw30", 180), ("qft30", 137), ("qft32", 161), ("hea26", 110)])
+def test_pass_search_and_spread_cap(name, cost_max):
+    """The lookahead growth rule and the beam over pass sequences (QFT at 30
+    qubits took 33 passes and 114 blocks, HEA at 26 qubits 21 and 82, with the
+    fewest-new-qubits rule alone), and no pass whose tiles scatter their runs
+    over more than the measured limit (spread <= 7 above qubit 20)."""
+    from dqsim import workloads
+
+    c = {"bw30": lambda: workloads.brickwork(30, 40, seed=0, measure=False),
+         "qft30": lambda: workloads.qft(30, seed=0),
+         "qft32": lambda: workloads.qft(32, seed=0),
+         "hea26": lambda: workloads.hea(26, 16, seed=0)}[name]()
+    plan = _core.fused_plan_dump(c.model_dump_json())
+    blocks = sum(len(p["blocks"]) for p in plan["passes"])
+    assert 3 * len(plan["passes"]) + blocks <= cost_max
+    assert max(_spread(p["qubits"]) for p in plan["passes"]) <= 7
+    # every operation lands in exactly one pass
+    assert sum(p["raw"] for p in plan["passes"]) == len(_core.compile_dump(c.model_dump_json()))
