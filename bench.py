@@ -69,8 +69,8 @@ def tensor_peak():
 # and lo*hi products of the 128 x 64 operand with the 64 x 64 real gate image.
 FUSED_FLOPS_PER_TILE_BLOCK = 3 * 2 * 128 * 64 * 64
 # DRAM bytes (read + write) per tile of one k_fused launch, from the ncu capture
-# of a 25-qubit pass (482.8 MB over 8192 tiles; traffic grows with the tiles).
-FUSED_TRAFFIC_PER_TILE = 482.760e6 / 8192
+# of a 25-qubit pass (477.9 MB over 8192 tiles; traffic grows with the tiles).
+FUSED_TRAFFIC_PER_TILE = 477.933e6 / 8192
 
 
 class ClockSampler:
