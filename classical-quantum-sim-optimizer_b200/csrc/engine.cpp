@@ -12,6 +12,8 @@
 #include <mutex>
 #include <thread>
 
+#include <unistd.h>
+
 #include "cost.hpp"
 
 namespace dq {
@@ -27,11 +29,13 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
-// Host worker threads shared by every parallel_for, started on first use.  A
-// call posts its job, works on it itself, then withdraws it and waits for the
-// workers still inside one of its items; a worker only ever waits for items
-// already running, so nested calls (an item that calls parallel_for) cannot
-// deadlock, and with no workers (e.g. after fork) the caller does every item.
+// Host worker threads shared by every parallel_for, started on first use and
+// never torn down (they idle on a condition variable until the process ends).
+// A call posts its job, works on it itself, then withdraws it and waits for
+// the workers still inside one of its items; a worker only ever waits for
+// items already running, so nested calls (an item that calls parallel_for)
+// cannot deadlock.  A forked child, which has none of the workers, runs its
+// calls on the calling thread.
 class WorkerPool {
   public:
     struct Job {
@@ -43,17 +47,12 @@ class WorkerPool {
         std::exception_ptr error;
     };
 
-    explicit WorkerPool(size_t workers) {
-        for (size_t w = 0; w < workers; w++) threads_.emplace_back([this] { loop(); });
+    explicit WorkerPool(size_t workers) : owner_(getpid()) {
+        for (size_t w = 0; w < workers; w++) std::thread([this] { loop(); }).detach();
     }
-    ~WorkerPool() {
-        {
-            std::lock_guard<std::mutex> l(mutex_);
-            stop_ = true;
-        }
-        wake_.notify_all();
-        for (auto& t : threads_) t.join();
-    }
+
+    // False in a process forked after the workers started.
+    bool usable() const { return getpid() == owner_; }
 
     void run(Job& job) {
         {
@@ -84,8 +83,7 @@ class WorkerPool {
     void loop() {
         std::unique_lock<std::mutex> l(mutex_);
         while (true) {
-            wake_.wait(l, [&] { return stop_ || !jobs_.empty(); });
-            if (stop_) return;
+            wake_.wait(l, [&] { return !jobs_.empty(); });
             Job* job = jobs_.front();
             if (job->next.load() >= job->count) {
                 jobs_.pop_front();
@@ -99,22 +97,22 @@ class WorkerPool {
         }
     }
 
+    const pid_t owner_;
     std::mutex mutex_;
     std::condition_variable wake_, idle_;
     std::deque<Job*> jobs_;
-    std::vector<std::thread> threads_;
-    bool stop_ = false;
 };
 
 WorkerPool& worker_pool() {
-    static WorkerPool pool(std::min<size_t>(std::max<size_t>(1, std::thread::hardware_concurrency()), 16) - 1);
-    return pool;
+    static WorkerPool* pool =
+        new WorkerPool(std::min<size_t>(std::max<size_t>(1, std::thread::hardware_concurrency()), 16) - 1);
+    return *pool;
 }
 
 }  // namespace
 
 void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
-    if (count <= 1) {
+    if (count <= 1 || !worker_pool().usable()) {
         for (size_t i = 0; i < count; i++) fn(i);
         return;
     }

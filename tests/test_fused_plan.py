@@ -244,3 +244,28 @@ def test_pass_search_and_spread_cap(name, cost_max):
         assert max(_spread(p["qubits"]) for p in plan["passes"]) <= 24
     # every operation lands in exactly one pass
     assert sum(p["raw"] for p in plan["passes"]) == len(_core.compile_dump(c.model_dump_json()))
+
+
+def _plan_in_child(text, queue):
+    plan = _core.fused_plan_dump(text)
+    queue.put((len(plan["passes"]), sum(len(p["blocks"]) for p in plan["passes"])))
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_planning_in_a_forked_child():
+    """Planning runs on pooled host workers; a child forked after the pool
+    started has none of them and plans on its calling thread, to the same plan."""
+    import multiprocessing as mp
+
+    from dqsim import workloads
+
+    text = workloads.brickwork(24, 12, seed=2, measure=False).model_dump_json()
+    plan = _core.fused_plan_dump(text)  # starts the pool in this process
+    expect = (len(plan["passes"]), sum(len(p["blocks"]) for p in plan["passes"]))
+    ctx = mp.get_context("fork")
+    queue = ctx.Queue()
+    child = ctx.Process(target=_plan_in_child, args=(text, queue))
+    child.start()
+    child.join(120)
+    assert child.exitcode == 0
+    assert queue.get(timeout=5) == expect
