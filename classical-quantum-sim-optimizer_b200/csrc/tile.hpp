@@ -202,12 +202,12 @@ constexpr double kFusedPassCostBlocks = 3.0;
 constexpr double kFusedSpreadCostBlocks[2] = {4.0, 8.0};
 
 // Plans ops[begin, end) as fused passes (kFusedM tile qubits, kFusedPinned
-// pinned, beam kPlanBeam) under the spread cap kFusedMaxSpread, one less, and
-// none, where they can bind, builds every pass's blocks, and returns the plan of
-// lowest kFusedPassCostBlocks * passes + blocks + kFusedSpreadCostBlocks for
-// passes over the cap (the pass search follows ops covered, not blocks, so the
-// caps give different plans).  `base` supplies seeds; the other planning
-// fields are set here.
+// pinned, beam kPlanBeam) under the spread cap kFusedMaxSpread and, where it
+// can bind, also with no cap and with a cap 4 quarters lower; builds every
+// pass's blocks and returns the plan of lowest kFusedPassCostBlocks * passes
+// + blocks + kFusedSpreadCostBlocks per pass over the cap (the pass search
+// follows ops covered, not blocks, so the caps give different plans).  `base`
+// supplies seeds; the other planning fields are set here.
 std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
                                        const TilePlanOptions& base);
 
