@@ -1112,39 +1112,54 @@ std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t
         caps.push_back(-1);
         caps.push_back(kFusedMaxSpread - 4);
     }
-    std::vector<std::vector<BuiltFusedPass>> plans(caps.size());
+    std::vector<std::vector<TilePass>> plans(caps.size());
     parallel_for(caps.size(), [&](size_t i) {
         TilePlanOptions oi = o;
         oi.max_spread = caps[i];
         std::vector<double2> unused;
-        std::vector<TilePass> ps = plan_tiles(ops, begin, end, n, oi, &unused);
-        std::vector<BuiltFusedPass>& plan = plans[i];
-        plan.resize(ps.size());
-        parallel_for(ps.size(), [&](size_t k) {
-            BuiltFusedPass& b = plan[k];
-            b.fp = build_fused_pass(ps[k].raw, ps[k].qubits, b.blocks, b.upool);
-            b.src = std::move(ps[k]);
-        });
+        plans[i] = plan_tiles(ops, begin, end, n, oi, &unused);
+    });
+    // The plans share passes (same tile qubits, same operations): each distinct
+    // pass is fused into blocks once, all of them on pooled workers.
+    std::map<std::pair<std::vector<int>, std::vector<size_t>>, size_t> slot_of;
+    std::vector<const TilePass*> distinct;
+    std::vector<std::vector<size_t>> slots(plans.size());
+    for (size_t i = 0; i < plans.size(); i++)
+        for (const TilePass& p : plans[i]) {
+            auto it = slot_of.emplace(std::make_pair(p.qubits, p.op_index), distinct.size()).first;
+            if (it->second == distinct.size()) distinct.push_back(&p);
+            slots[i].push_back(it->second);
+        }
+    std::vector<BuiltFusedPass> built(distinct.size());
+    parallel_for(distinct.size(), [&](size_t k) {
+        BuiltFusedPass& b = built[k];
+        b.fp = build_fused_pass(distinct[k]->raw, distinct[k]->qubits, b.blocks, b.upool);
     });
     const TileShape sh{kFusedM, n, kFusedPinned, kFusedSpreadBit, INT_MAX, o.inflight_bits};
     size_t best = 0;
     double best_cost = 0;
     for (size_t i = 0; i < plans.size(); i++) {
         double cost = kFusedPassCostBlocks * double(plans[i].size());
-        for (const BuiltFusedPass& b : plans[i]) {
+        for (size_t k = 0; k < plans[i].size(); k++) {
             uint64_t T = 0;
-            for (int q : b.src.qubits) T |= uint64_t(1) << q;
+            for (int q : plans[i][k].qubits) T |= uint64_t(1) << q;
             const int spread = sh.spread(T);
-            cost += b.fp.nblocks + (spread > kFusedMaxSpread + 4   ? kFusedSpreadCostBlocks[1]
-                                    : spread > kFusedMaxSpread ? kFusedSpreadCostBlocks[0]
-                                                               : 0.0);
+            cost += built[slots[i][k]].fp.nblocks + (spread > kFusedMaxSpread + 4   ? kFusedSpreadCostBlocks[1]
+                                                     : spread > kFusedMaxSpread ? kFusedSpreadCostBlocks[0]
+                                                                                : 0.0);
         }
         if (i == 0 || cost < best_cost) {
             best = i;
             best_cost = cost;
         }
     }
-    return std::move(plans[best]);
+    std::vector<BuiltFusedPass> out(plans[best].size());
+    for (size_t k = 0; k < out.size(); k++) {
+        const size_t slot = slots[best][k];
+        out[k] = built[slot];
+        out[k].src = std::move(plans[best][k]);
+    }
+    return out;
 }
 
 void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,
@@ -1204,6 +1219,7 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
         std::vector<Operation> pass_ops;
         for (size_t o : taken) pass_ops.push_back(ops[begin + o]);
         p.raw_ops = int(pass_ops.size());
+        for (size_t o : taken) p.op_index.push_back(begin + o);
         if (opt.keep_raw) {
             p.raw = std::move(pass_ops);
             passes.push_back(std::move(p));

@@ -43,6 +43,7 @@ struct TilePass {
     int op_begin = 0;         // index into the device op array
     int raw_ops = 0;          // unfused operations covered (for statistics)
     std::vector<Operation> raw;  // filled when TilePlanOptions::keep_raw
+    std::vector<size_t> op_index;  // the pass's operations: indices into the planned list, ascending
 };
 
 struct TilePlanOptions {
