@@ -412,17 +412,39 @@ __global__ void __launch_bounds__(256) k_scan_tiles(const V* __restrict__ in, do
     const uint64_t base = uint64_t(blockIdx.x) * kScanTile + uint64_t(threadIdx.x) * kScanItems;
     double v[kScanItems];
     double run = 0.0;
+    // A whole run of complex64 amplitudes is read as 16-byte vectors (two
+    // amplitudes each); the sums are the same, in the same order.
+    const bool full = base + kScanItems <= len;
+    bool done = false;
+    if constexpr (std::is_same<V, float2>::value) {
+        if (full && (reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+            const float4* p = reinterpret_cast<const float4*>(in + base);
+            float4 f[kScanItems / 2];
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        double e = 0.0;
-        if (base + i < len) {
-            if constexpr (std::is_same<V, double>::value)
-                e = in[base + i];
-            else
-                e = dev::norm2(in[base + i]);
+            for (int i = 0; i < kScanItems / 2; i++) f[i] = p[i];
+#pragma unroll
+            for (int i = 0; i < kScanItems / 2; i++) {
+                run += dev::norm2(make_float2(f[i].x, f[i].y));
+                v[2 * i] = run;
+                run += dev::norm2(make_float2(f[i].z, f[i].w));
+                v[2 * i + 1] = run;
+            }
+            done = true;
         }
-        run += e;
-        v[i] = run;
+    }
+    if (!done) {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            double e = 0.0;
+            if (base + i < len) {
+                if constexpr (std::is_same<V, double>::value)
+                    e = in[base + i];
+                else
+                    e = dev::norm2(in[base + i]);
+            }
+            run += e;
+            v[i] = run;
+        }
     }
     // inclusive warp scan of thread totals
     double t = run;
@@ -437,9 +459,15 @@ __global__ void __launch_bounds__(256) k_scan_tiles(const V* __restrict__ in, do
     double wprefix = 0.0;
     for (int i = 0; i < w; i++) wprefix += warp_tot[i];
     double excl = wprefix + t - run;
+    if (full && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        double2* px = reinterpret_cast<double2*>(x + base);
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++)
-        if (base + i < len) x[base + i] = v[i] + excl;
+        for (int i = 0; i < kScanItems / 2; i++) px[i] = make_double2(v[2 * i] + excl, v[2 * i + 1] + excl);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++)
+            if (base + i < len) x[base + i] = v[i] + excl;
+    }
     if (threadIdx.x == 255) {
         double tot = 0.0;
         for (int i = 0; i < 8; i++) tot += warp_tot[i];
