@@ -14,6 +14,26 @@ namespace {
 using clk = std::chrono::steady_clock;
 double since(clk::time_point t0) { return std::chrono::duration<double>(clk::now() - t0).count(); }
 
+// Sorts sampled outcomes ascending: LSD radix sort on 16-bit digits, only as
+// many passes as the largest value needs (std::sort below 4096 values).
+void sort_outcomes(std::vector<uint64_t>& v) {
+    if (v.size() < 4096) {
+        std::sort(v.begin(), v.end());
+        return;
+    }
+    uint64_t top = 0;
+    for (uint64_t x : v) top |= x;
+    std::vector<uint64_t> tmp(v.size());
+    std::vector<size_t> start(65537);
+    for (int shift = 0; shift < 64 && (top >> shift) != 0; shift += 16) {
+        std::fill(start.begin(), start.end(), size_t(0));
+        for (uint64_t x : v) start[((x >> shift) & 0xffff) + 1]++;
+        for (size_t d = 0; d < 65536; d++) start[d + 1] += start[d];
+        for (uint64_t x : v) tmp[start[(x >> shift) & 0xffff]++] = x;
+        v.swap(tmp);
+    }
+}
+
 // state_layout, shots.rs:22-31, for `amp` bytes per amplitude.
 void state_layout(uint64_t n, uint64_t amp, uint64_t* len, uint64_t* bytes) {
     if (n >= 64) fail(kMemoryError, "State dimension overflow");
@@ -234,15 +254,26 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 std::vector<uint64_t> h(shots);
                 cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
                 cuda_check(cudaStreamSynchronize(s), "stream synchronize");
-                std::sort(h.begin(), h.end());
+                sort_outcomes(h);
                 if (ncb <= 64) {
                     // Classical-register value of each distinct outcome, merged by value.
+                    // Where every cbit reads the sampled bit of its own position the
+                    // value is the outcome masked to those bits.
+                    bool same_bit = true;
+                    uint64_t same_mask = 0;
+                    for (auto& sh : shifts) {
+                        same_bit = same_bit && sh.first == sh.second;
+                        same_mask |= uint64_t(1) << sh.second;
+                    }
                     std::vector<std::pair<uint64_t, uint64_t>> kc;
                     for (size_t i = 0; i < h.size();) {
                         size_t j = i;
                         while (j < h.size() && h[j] == h[i]) j++;
                         uint64_t key = 0;
-                        for (auto& sh : shifts) key |= ((h[i] >> sh.second) & 1) << sh.first;
+                        if (same_bit)
+                            key = h[i] & same_mask;
+                        else
+                            for (auto& sh : shifts) key |= ((h[i] >> sh.second) & 1) << sh.first;
                         kc.emplace_back(key, uint64_t(j - i));
                         i = j;
                     }
