@@ -9,6 +9,7 @@
 #include <deque>
 #include <exception>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <thread>
 
@@ -135,6 +136,11 @@ void trim_pool() {
     }
 }
 
+// Live Device objects per ordinal: the default memory pool is shared by every
+// simulator on a device, so only the last one to go returns its cache.
+std::mutex g_devices_mu;
+std::map<int, int> g_devices_live;
+
 }  // namespace
 
 void DevMem::alloc(size_t b, const char* what) {
@@ -187,13 +193,15 @@ Device::Device(int ord) : ordinal(ord) {
     cuda_check(cudaSetDevice(ord), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     // Freed stream-ordered blocks stay cached in the device pool (statevector
-    // and sampling-table sized), returned on destruction or when a plain
-    // allocation runs out of memory.
+    // and sampling-table sized), returned when the device's last simulator is
+    // destroyed or when a plain allocation runs out of memory.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, ord) == cudaSuccess) {
         uint64_t keep = ~uint64_t(0);
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    std::lock_guard<std::mutex> l(g_devices_mu);
+    g_devices_live[ord]++;
 }
 
 Device::~Device() {
@@ -201,7 +209,12 @@ Device::~Device() {
         cudaSetDevice(ordinal);
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
-        trim_pool();
+        bool last = false;
+        {
+            std::lock_guard<std::mutex> l(g_devices_mu);
+            last = --g_devices_live[ordinal] == 0;
+        }
+        if (last) trim_pool();
     }
 }
 
