@@ -16,8 +16,14 @@ beside it.  The roofline is the fused kernel's tensor-pipe throughput (f16
 FLOPs it issues: three 128x64x64 products per block and tile).
 
 --impl reference times the CPU restatement of the reference's engine
-(oracle/, OpenMP on every host core) on a bounded sample of the same circuit:
-the first operations at 30 qubits, scaled by operation count.
+(oracle/, OpenMP on every host core) on complete circuits: every step is one
+whole simulate_shots call at 30 qubits (all operations, the FP64 marginal
+table and CDF, 10^5 seeded draws), nothing extrapolated.  One such circuit
+takes minutes, so the arm runs as many complete circuits as fit its wall-time
+budget (at least one, at most --steps, no warm-up: the reference allocates
+and first-touches a fresh state inside every call) and reports the count it
+ran.  It loads the circuit generators from their file alone, never the
+engine's library.
 
 --workload selects the other measured configurations (their own JSON line):
 qft (32-qubit QFT, complex64 fused vs complex128 plain), batch (512 uneven HEA
@@ -35,6 +41,8 @@ import sys
 import threading
 import time
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 PKG = ROOT / "classical-quantum-sim-optimizer_b200"
@@ -174,56 +182,103 @@ def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed, exec
     return sim, plan
 
 
-def cpu_reference_sample(circuit, budget_s, threads=None):
-    """Time the oracle's kernels on the first operations of the circuit at full size."""
+def load_workloads():
+    """The seeded circuit generators, loaded from their file alone (importing the dqsim package would load
+    the engine's library into the CPU-only arms)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("dqsim_workloads", PKG / "dqsim" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cpu_budget_mb(n):
+    """max_memory_mb for terminal sampling on the CPU restatement: state (16 B per amplitude) plus the
+    FP64 CDF, shots.rs:118-124."""
+    return ((16 << n) + (8 << n)) // (1 << 20) + 64
+
+
+def cpu_reference_sample(circuit, budget_s, shots, seed):
+    """Bounded CPU baseline at full size: the first operations of the circuit timed one by one on a fresh
+    state (the first includes first-touching it), the rest estimated from the timed ones' per-kind means,
+    and the marginal table, CDF and seeded draws timed in full."""
     from oracle import oracle
 
     L = oracle.lib()
-    if threads:
-        L.orc_set_num_threads(threads)
     n, _, ops = oracle.circuit_ops(circuit.model_dump_json())
-    unitary = [op for op in ops if op[0] not in ("measure", "reset", "cond")]
-    import numpy as np
+    prefix_end = next((i for i, op in enumerate(ops) if not oracle.is_unitary(op)), len(ops))
+    unitary = ops[:prefix_end]
+    qubits = sorted({op[1] for op in ops[prefix_end:]}, reverse=True)
 
-    t0 = time.perf_counter()
-    state = np.zeros(1 << n, dtype=np.complex128)
-    state[0] = 1.0
-    alloc_s = time.perf_counter() - t0
-    done = 0
-    t1 = time.perf_counter()
-    rng = oracle.ChaCha8Stream(0)
-    while done < len(unitary) and time.perf_counter() - t1 < budget_s:
+    def kind(op):
+        return f"{op[0]}{len(op[3]) if op[0] == 'one' else len(op[2]) if op[0] == 'x' else ''}"
+
+    t_start = time.perf_counter()
+    state = oracle.zero_state(n)
+    rng = oracle.ChaCha8Stream(seed)
+    per_kind, first_s, done = {}, 0.0, 0
+    while done < len(unitary) and (done < 2 or time.perf_counter() - t_start < budget_s):
+        t0 = time.perf_counter()
         oracle.apply_op(unitary[done], state, n, [], rng, True)
+        dt = time.perf_counter() - t0
+        if done == 0:
+            first_s = dt
+        else:
+            per_kind.setdefault(kind(unitary[done]), []).append(dt)
         done += 1
-    per_op = (time.perf_counter() - t1) / max(done, 1)
+    timed_s = first_s + sum(sum(v) for v in per_kind.values())
+    all_mean = sum(sum(v) for v in per_kind.values()) / max(1, sum(len(v) for v in per_kind.values()))
+    rest_s = 0.0
+    for op in unitary[done:]:
+        v = per_kind.get(kind(op))
+        rest_s += statistics.mean(v) if v else all_mean
+    t0 = time.perf_counter()
+    cdf = oracle.cdf_from_probs(oracle.marginal_probs(state, n, qubits))
     del state
-    return {"per_op_s": per_op, "ops_timed": done, "ops_total": len(unitary), "alloc_s": alloc_s,
-            "circuit_s": per_op * len(unitary), "threads": L.orc_num_threads(), "qubits": n}
+    draws = oracle.first_draws(seed, shots)
+    idx = np.minimum(np.searchsorted(cdf, draws, side="right"), len(cdf) - 1)
+    np.unique(idx, return_counts=True)
+    sample_s = time.perf_counter() - t0
+    del cdf
+    return {"circuit_s": timed_s + rest_s + sample_s, "ops_timed": done, "ops_total": len(unitary),
+            "sampling_s": sample_s, "threads": L.orc_num_threads(), "qubits": n,
+            "per_kind_ms": {k: 1e3 * statistics.mean(v) for k, v in per_kind.items()}}
 
 
 def run_reference(args):
+    """The reference arm: complete 30-qubit circuits through the CPU restatement's simulate_shots."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import dqsim
+    from oracle import oracle
 
-    circuit = dqsim.workloads.brickwork(args.qubits, args.depth, seed=args.seed, measure=True)
-    samples = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_reference_sample(circuit, args.cpu_budget / max(1, args.steps + args.warmup))
-        if i >= args.warmup:
-            samples.append(info["circuit_s"])
-    value = statistics.mean(samples)
+    circuit = load_workloads().brickwork(args.qubits, args.depth, seed=args.seed, measure=True)
+    threads = oracle.lib().orc_num_threads()
+    sim = oracle.OracleSimulator(seed=args.seed, max_memory_mb=cpu_budget_mb(args.qubits))
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max(1, args.steps):
+        t0 = time.perf_counter()
+        out = sim.simulate_shots_full(circuit, shots=args.shots)
+        times.append(time.perf_counter() - t0)
+        if out["strategy"] != "terminal_sampling" or sum(out["counts"].values()) != args.shots:
+            raise RuntimeError("the CPU restatement did not sample the circuit terminally")
+        if time.perf_counter() - t_start + 1.1 * max(times) > args.ref_budget:
+            break
+    value = statistics.mean(times)
+    sample = (f"full circuit: every one of the circuit's operations at {args.qubits} qubits, the FP64 marginal "
+              f"table and CDF and {args.shots} seeded draws per step (simulate_shots of the C restatement of "
+              f"src/engine.rs + shots.rs), {len(times)} complete circuit(s) timed, no extrapolation")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "higher_is_better": False,
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic",
+        "n_gpus": world, "steps": len(times), "warmup": 0, "ms_per_step": value * 1e3,
+        "requested": {"steps": args.steps, "warmup": args.warmup,
+                      "why": "one complete CPU circuit takes minutes; as many as fit the arm's budget are run"},
+        "runs_s": times, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic",
         "config": workload_config(args),
-        "cpu_baseline": {"value": value, "unit": "s", "cores": info["threads"], "kind": "port",
-                         "sample": f"first {info['ops_timed']} of {info['ops_total']} operations at "
-                                   f"{info['qubits']} qubits per step, scaled by operation count"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -273,8 +328,13 @@ def main():
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--shots", type=int, default=100000)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of timed CPU operations (cpu_baseline)")
+    ap.add_argument("--ref-budget", type=float, default=900.0,
+                    help="wall seconds the reference arm may spend on complete circuits (at least one runs)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--forms", default="fused,c64_cuda_core,c128_tiled,c128_per_gate",
+                    help="forms timed beside the fused one (profiling runs time the fused form alone)")
     ap.add_argument("--plain-steps", type=int, default=1)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -288,38 +348,55 @@ def main():
     peak, peak_kind = peaks()
     circuit = dqsim.workloads.brickwork(args.qubits, args.depth, seed=args.seed, measure=True)
 
+    forms = set(args.forms.split(","))
+    unknown = forms - {"fused", "c64_cuda_core", "c128_tiled", "c128_per_gate"}
+    if unknown or "fused" not in forms:
+        raise SystemExit(f"--forms: the fused form is required; unknown forms {sorted(unknown)}")
+    out_forms = {}
+    plan128 = sim128 = None
+
     # Plain complex128 form: the reference's arithmetic, one HBM pass per operation.
-    sim128, plan128 = time_form(dqsim, circuit, "complex128", local, 1, 0, args.shots, args.seed,
-                                execution="per_gate")
-    t128 = [plan128.run() for _ in range(args.plain_steps)]
-    plan128.run(record=True)
-    st128 = plan128.stats()
-    ms128 = statistics.mean(t128)
-    per_gate = st128.get("gate1q")
-    plain_kernel = None
-    if per_gate:
-        ach = per_gate["bytes"] / (per_gate["ms"] * 1e-3) / 1e9
-        plain_kernel = {"kernel": "gate1q (c128, per-gate)", "achieved": ach, "frac": ach / peak,
-                        "launches": per_gate["launches"]}
+    if "c128_per_gate" in forms:
+        sim128, plan128 = time_form(dqsim, circuit, "complex128", local, 1, 0, args.shots, args.seed,
+                                    execution="per_gate")
+        t128 = [plan128.run() for _ in range(args.plain_steps)]
+        plan128.run(record=True)
+        st128 = plan128.stats()
+        ms128 = statistics.mean(t128)
+        per_gate = st128.get("gate1q")
+        plain_kernel = None
+        if per_gate:
+            ach = per_gate["bytes"] / (per_gate["ms"] * 1e-3) / 1e9
+            plain_kernel = {"kernel": "gate1q (c128, per-gate)", "achieved": ach, "frac": ach / peak,
+                            "launches": per_gate["launches"]}
+        out_forms["complex128_per_gate"] = {**summarize(st128, ms128, peak), "dominant": plain_kernel}
+
+    def compare_plain(plan):
+        return plan.compare(plan128) if plan128 is not None else (None, None)
 
     # complex128 with shared-memory tile passes (same FP64 arithmetic, fused 4x4 within a pass).
-    simt, plant = time_form(dqsim, circuit, "complex128", local, 1, 1, args.shots, args.seed)
-    tt = [plant.run() for _ in range(args.plain_steps)]
-    plant.run(record=True)
-    stt = plant.stats()
-    mst = statistics.mean(tt)
-    tiled_fid, tiled_err = plant.compare(plan128)
-    del plant, simt
+    if "c128_tiled" in forms:
+        simt, plant = time_form(dqsim, circuit, "complex128", local, 1, 1, args.shots, args.seed)
+        tt = [plant.run() for _ in range(args.plain_steps)]
+        plant.run(record=True)
+        stt = plant.stats()
+        mst = statistics.mean(tt)
+        tiled_fid, tiled_err = compare_plain(plant)
+        out_forms["complex128_tiled"] = {**summarize(stt, mst, peak), "fidelity": tiled_fid,
+                                         "max_amp_err": tiled_err}
+        del plant, simt
 
     # complex64 on CUDA cores (13-qubit tiles, width-2 fusion).
-    simc, planc = time_form(dqsim, circuit, "complex64", local, 1, 1, args.shots, args.seed,
-                            tile_qubits=13, fusion_width=2)
-    tc = [planc.run() for _ in range(args.plain_steps)]
-    planc.run(record=True)
-    stc = planc.stats()
-    msc = statistics.mean(tc)
-    cc_fid, cc_err = planc.compare(plan128)
-    del planc, simc
+    if "c64_cuda_core" in forms:
+        simc, planc = time_form(dqsim, circuit, "complex64", local, 1, 1, args.shots, args.seed,
+                                tile_qubits=13, fusion_width=2)
+        tc = [planc.run() for _ in range(args.plain_steps)]
+        planc.run(record=True)
+        stc = planc.stats()
+        msc = statistics.mean(tc)
+        cc_fid, cc_err = compare_plain(planc)
+        out_forms["complex64_cuda_core"] = {**summarize(stc, msc, peak), "fidelity": cc_fid, "max_amp_err": cc_err}
+        del planc, simc
 
     # The chosen form: complex64 with fused 5-qubit blocks on tensor cores.
     sim64, plan64 = time_form(dqsim, circuit, "complex64", local, 1, args.warmup, args.shots, args.seed)
@@ -330,32 +407,46 @@ def main():
     ms = max_over_ranks(pg, local, statistics.mean(times))
     plan64.run(record=True)
     st64 = plan64.stats()
-    fidelity, max_err = plan64.compare(plan128)
+    fidelity, max_err = compare_plain(plan64)
     shape64 = plan64.shape()
     roof = fused_roofline(plan64, st64, args.qubits)
+    out_forms["complex64_fused"] = {**summarize(st64, ms, peak), "fidelity": fidelity, "max_amp_err": max_err,
+                                    "passes": shape64["passes"], "fused_blocks": shape64["fused_blocks"]}
+    if "complex128_per_gate" in out_forms:
+        out_forms["speedup_fused_vs_plain"] = out_forms["complex128_per_gate"]["s"] * 1e3 / ms
+    if "complex64_cuda_core" in out_forms:
+        out_forms["speedup_fused_vs_c64_cuda_core"] = out_forms["complex64_cuda_core"]["s"] * 1e3 / ms
     del plan128, sim128
 
-    # End to end through the public API: host JSON in, host counts out (median of three calls after the
-    # same warm-up count as the device timing; the first calls after start-up also warm the memory pool).
-    api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64", device=local)
-    for _ in range(max(1, args.warmup)):
-        api.simulate_shots(circuit, shots=args.shots)
-    e2e_runs = []
-    for _ in range(3):
-        t0 = time.perf_counter()
-        counts = api.simulate_shots(circuit, shots=args.shots)
-        e2e_runs.append(time.perf_counter() - t0)
-        assert sum(counts.values()) == args.shots
-    e2e_s = statistics.median(e2e_runs)
-    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": len(circuit.model_dump_json()),
-           "d2h_bytes_per_step": 8 * args.shots, "runs_s": e2e_runs}
+    # End to end through the public API: host JSON in, host counts out.  Five calls after the same warm-up
+    # count as the device timing (the first calls also fill the engine's memory pool); every call is
+    # reported with its host phase times.
+    e2e = None
+    if not args.no_e2e:
+        api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64",
+                                         device=local)
+        for _ in range(max(1, args.warmup)):
+            api.simulate_shots(circuit, shots=args.shots)
+        e2e_runs, e2e_phases = [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            counts = api.simulate_shots(circuit, shots=args.shots)
+            e2e_runs.append(time.perf_counter() - t0)
+            e2e_phases.append({k: round(v * 1e3, 3) for k, v in dqsim._core.last_call_phases(api).items()})
+            assert sum(counts.values()) == args.shots
+        e2e = {"value": statistics.median(e2e_runs), "unit": "s",
+               "h2d_bytes_per_step": len(circuit.model_dump_json()), "d2h_bytes_per_step": 8 * args.shots,
+               "runs_s": e2e_runs, "mean_s": statistics.mean(e2e_runs), "max_s": max(e2e_runs),
+               "phases_ms": e2e_phases}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        info = cpu_reference_sample(circuit, args.cpu_budget)
+        info = cpu_reference_sample(circuit, args.cpu_budget, args.shots, args.seed)
         cpu = {"value": info["circuit_s"], "unit": "s", "cores": info["threads"], "kind": "port",
                "sample": f"first {info['ops_timed']} of {info['ops_total']} operations at {info['qubits']} qubits "
-                         f"(OpenMP C restatement of src/engine.rs), scaled by operation count"}
+                         f"timed on a fresh state, the rest estimated from their per-kind means "
+                         f"({info['per_kind_ms']} ms), marginal table, CDF and {args.shots} draws timed in full "
+                         f"({info['sampling_s']:.2f} s); OpenMP C restatement of src/engine.rs + shots.rs"}
 
     value = (ms * 1e-3) / world
     # Every kernel of a step: the recorded classes plus the basis-state initialisation.
@@ -365,15 +456,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (f16x3 tensor products, f32 accumulate, FP64 reductions)",
         "data": "synthetic", "config": workload_config(args),
-        "forms": {
-            "complex64_fused": {**summarize(st64, ms, peak), "fidelity": fidelity, "max_amp_err": max_err,
-                                "passes": shape64["passes"], "fused_blocks": shape64["fused_blocks"]},
-            "complex64_cuda_core": {**summarize(stc, msc, peak), "fidelity": cc_fid, "max_amp_err": cc_err},
-            "complex128_per_gate": {**summarize(st128, ms128, peak), "dominant": plain_kernel},
-            "complex128_tiled": {**summarize(stt, mst, peak), "fidelity": tiled_fid, "max_amp_err": tiled_err},
-            "speedup_fused_vs_plain": ms128 / ms,
-            "speedup_fused_vs_c64_cuda_core": msc / ms,
-        },
+        "forms": out_forms,
         "roofline": roof,
         "hbm_peak": {"value": peak, "kind": peak_kind},
         "cpu_baseline": cpu,

@@ -613,6 +613,15 @@ int dq_sim_planner_log(dq_sim* sim, char** out_text) {
     });
 }
 
+int dq_sim_last_call_phases(dq_sim* sim, double* out, uint64_t n) {
+    return guard([&] {
+        need(sim, "sim");
+        need(out, "out");
+        if (n != uint64_t(kNumCallPhases)) fail(kValueError, "phase buffer must hold DQ_CALL_PHASES doubles");
+        sim->impl->last_call_phases(out);
+    });
+}
+
 int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit,
                        int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes) {
     return guard([&] {

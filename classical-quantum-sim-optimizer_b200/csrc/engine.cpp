@@ -126,20 +126,54 @@ void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
 
 namespace {
 
-// Returns the memory the current device's pool keeps cached to the driver.
-void trim_pool() {
-    int dev = 0;
-    cudaMemPool_t pool;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        cudaDeviceSynchronize();
-        cudaMemPoolTrimTo(pool, 0);
+// The engine's own stream-ordered memory pool per device: statevectors and
+// sampling tables come from it, and freed blocks stay cached in it (release
+// threshold: keep everything) so that repeated calls map no memory.  It is
+// separate from the device's default pool, whose settings and cache belong to
+// whatever else in the process uses cudaMallocAsync.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_devices_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+// Live Device objects per ordinal: the pool is shared by every simulator (and
+// result) on a device, so only the last one to go returns its cache.
+std::map<int, int> g_devices_live;
+
+cudaMemPool_t engine_pool(int dev) {
+    std::lock_guard<std::mutex> l(g_devices_mu);
+    if (dev < 0 || dev >= kMaxPoolDevices) fail(kValueError, "CUDA device ordinal out of range");
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        cuda_check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        uint64_t keep = ~uint64_t(0);
+        cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                   "memory pool release threshold");
+        g_pools[dev] = pool;
     }
+    return g_pools[dev];
 }
 
-// Live Device objects per ordinal: the default memory pool is shared by every
-// simulator on a device, so only the last one to go returns its cache.
-std::mutex g_devices_mu;
-std::map<int, int> g_devices_live;
+// Returns the memory the current device's engine pool keeps cached.  Blocks
+// freed on a stream return to the pool only once the stream reaches the free,
+// so `sync_device` first waits for the whole device (the out-of-memory path,
+// where another simulator's frees may still be pending).
+void trim_pool(bool sync_device) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxPoolDevices) return;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> l(g_devices_mu);
+        pool = g_pools[dev];
+    }
+    if (!pool) return;
+    if (sync_device) cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(pool, 0);
+}
 
 }  // namespace
 
@@ -149,7 +183,7 @@ void DevMem::alloc(size_t b, const char* what) {
     cudaError_t e = cudaMalloc(&p, b);
     if (e == cudaErrorMemoryAllocation) {  // memory cached by the stream-ordered pool: give it back, retry
         cudaGetLastError();
-        trim_pool();
+        trim_pool(true);
         e = cudaMalloc(&p, b);
     }
     if (e != cudaSuccess) p = nullptr;
@@ -160,11 +194,14 @@ void DevMem::alloc(size_t b, const char* what) {
 void DevMem::alloc_on(size_t b, cudaStream_t s, const char* what) {
     release();
     if (b == 0) b = 16;
-    cudaError_t e = cudaMallocAsync(&p, b, s);
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaMemPool_t pool = engine_pool(dev);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, b, pool, s);
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
-        trim_pool();
-        e = cudaMallocAsync(&p, b, s);
+        trim_pool(true);
+        e = cudaMallocFromPoolAsync(&p, b, pool, s);
     }
     if (e != cudaSuccess) p = nullptr;
     cuda_check(e, what);
@@ -192,14 +229,7 @@ Device::Device(int ord) : ordinal(ord) {
     if (ord < 0 || ord >= count) fail(kValueError, "CUDA device ordinal out of range");
     cuda_check(cudaSetDevice(ord), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    // Freed stream-ordered blocks stay cached in the device pool (statevector
-    // and sampling-table sized), returned when the device's last simulator is
-    // destroyed or when a plain allocation runs out of memory.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, ord) == cudaSuccess) {
-        uint64_t keep = ~uint64_t(0);
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
+    engine_pool(ord);
     std::lock_guard<std::mutex> l(g_devices_mu);
     g_devices_live[ord]++;
 }
@@ -214,7 +244,9 @@ Device::~Device() {
             std::lock_guard<std::mutex> l(g_devices_mu);
             last = --g_devices_live[ordinal] == 0;
         }
-        if (last) trim_pool();
+        // Every other Device on this ordinal has synchronised and destroyed its
+        // stream already, so the pool's pending frees have all completed.
+        if (last) trim_pool(false);
     }
 }
 

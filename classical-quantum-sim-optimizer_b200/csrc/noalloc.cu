@@ -1,16 +1,22 @@
 // Measurement of states the caller already holds on the device, with no
 // device allocation anywhere on the call path.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA stream is
-// being captured (an allocation there breaks the capture), hosts whose device
-// memory is owned and budgeted by their own allocator and that forbid side
-// allocations, and latency-bound loops that cannot pay for the device-wide
-// synchronisation cudaMalloc/cudaFree may trigger.  dq_measure_noalloc serves
-// them: the states (inputs and outputs) are the caller's device memory, and
-// the only scratch the measurement needs -- per-state seeds, draw counters,
-// outcomes, scales, branch partial sums and an error flag -- lives in one
-// file-scope __device__ array of fixed size, which every GPU that loads this
-// library holds until the process exits.
+// Some callers cannot call cudaMalloc: hosts whose device memory is owned and
+// budgeted by their own allocator and that forbid side allocations, and
+// latency-bound loops that cannot pay for the device-wide synchronisation
+// cudaMalloc/cudaFree may trigger.  dq_measure_noalloc serves them: the states
+// (inputs and outputs) are the caller's device memory, and the only scratch the
+// measurement needs -- per-state seeds, draw counters, outcomes, scales, branch
+// partial sums and an error flag -- lives in one file-scope __device__ array of
+// fixed size, which every GPU that loads this library holds until the process
+// exits.
+//
+// Ordering: the call issues its work on the legacy default stream and returns
+// only after that work has finished (the outcomes are read back into host
+// memory).  The legacy default stream does not wait for streams created
+// non-blocking, so work that writes the states on such a stream (or on any
+// stream of a per-thread-default-stream build) must be synchronised before the
+// call.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -55,7 +61,10 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // Measures `qubit` in each of num_states states of 2^num_qubits amplitudes
 // held back to back at `states` (caller's device memory), drawing from the
 // ChaCha8 stream seeds[i] at draw draw_index[i]; collapses (or resets) in
-// place and writes each outcome to outcomes[i] (host memory).
+// place and writes each outcome to outcomes[i] (host memory).  A state whose
+// norm is zero or not finite is left as it was with outcomes[i] = -1, and the
+// call then fails with RuntimeError; every other state of the call has been
+// measured and collapsed all the same, and its outcome is in outcomes[].
 void measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit, int reset,
                      const uint64_t* seeds, const uint64_t* draw_index, int* outcomes) {
     if (!states || !seeds || !draw_index || !outcomes) fail(kValueError, "null pointer argument");

@@ -165,6 +165,10 @@ uint64_t Simulator::next_seed() {
 ShotOutput Simulator::simulate_shots(const char* json, size_t len, uint64_t shots, bool profile, double* pre,
                                      double* fus) {
     auto total0 = clk::now();
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (double& v : phases_) v = 0.0;
+    }
     profile = profile || opt_.profile;
     Circuit c = parse_circuit(json, len);
     validate_circuit(c);
@@ -172,10 +176,13 @@ ShotOutput Simulator::simulate_shots(const char* json, size_t len, uint64_t shot
     auto f0 = clk::now();
     std::vector<Operation> plan = compile(c.instructions);
     double fusion = since(f0);
+    set_phase(kPhParse, preprocessing);
+    set_phase(kPhCompile, fusion);
     uint64_t seed = next_seed();
     auto s0 = clk::now();
     ShotOutput out = run_shots(plan, c.num_qubits(), c.num_cbits(), shots, seed, profile);
     double shots_total = since(s0);
+    set_phase(kPhTotal, since(total0));
     if (pre) *pre = preprocessing;
     if (fus) *fus = fusion;
     if (profile) write_shots_profile(out, preprocessing, fusion, shots_total, since(total0), shots);
@@ -234,19 +241,29 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
             dev_->activate();
             cudaStream_t s = dev_->stream;
             uint64_t kept_seed = seed;
+            clk::time_point mark = clk::now();
+            auto phase = [&](int i) {
+                const clk::time_point now = clk::now();
+                set_phase(i, std::chrono::duration<double>(now - mark).count());
+                mark = now;
+            };
             {
                 StateBatch st;
                 st.allocate(int(n), 1, ncb, c64, s);
                 k::Batch b = st.view(s, 1);
                 k::init_basis(b);
                 reset_bookkeeping(st, 1, {kept_seed}, s);
+                phase(kPhState);
                 Executor ex(ops, 0, prefix_end, exec_config(opt_, n));
+                phase(kPhPlan);
                 ex.run(b, nullptr);
+                phase(kPhRun);
                 DevMem cdf, tmp, idx;
                 const uint64_t clen = uint64_t(1) << kq;
                 cdf.alloc_on(clen * 8, s, "the sampling table");
                 double total = build_sums(b, qubits, cdf.as<double>(), clen, tmp);
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
+                phase(kPhSums);
                 st.amps.release();  // the state is no longer needed (shots.rs:150)
                 idx.alloc(shots * 8, "sampled outcomes");
                 k::sample_sums(s, cdf.as<double>(), tmp.as<double>(), clen, nullptr, total, false, seed, shots, true,
@@ -254,6 +271,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 std::vector<uint64_t> h(shots);
                 cuda_check(cudaMemcpyAsync(h.data(), idx.p, shots * 8, cudaMemcpyDeviceToHost, s), "read samples");
                 cuda_check(cudaStreamSynchronize(s), "stream synchronize");
+                phase(kPhSample);
                 sort_outcomes(h);
                 if (ncb <= 64) {
                     // Classical-register value of each distinct outcome, merged by value.
@@ -304,7 +322,9 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                         i = j;
                     }
                 }
+                phase(kPhKeys);
             }
+            phase(kPhRelease);
             out.strategy = "terminal_sampling";
             out.parallel_shots = 1;
             out.working_bytes = required;

@@ -52,6 +52,23 @@ struct ShotOutput {
     uint64_t prefix_ops = 0;
 };
 
+// Host wall time of the phases of the last simulate_shots call on a
+// simulator, in seconds (terminal sampling fills every phase; trajectories
+// fill parse, compile and total).  Phase order of dq_sim_last_call_phases.
+enum CallPhase : int {
+    kPhParse = 0,   // JSON parse and validation
+    kPhCompile,     // operation lowering and 1q fusion
+    kPhState,       // statevector allocation and |0...0> (enqueued)
+    kPhPlan,        // pass planning, fused blocks and gate images
+    kPhRun,         // uploads and kernel launches of the unitary prefix (enqueued)
+    kPhSums,        // probability running sums, waits for the prefix to finish
+    kPhSample,      // shot draws and the device-to-host copy of the outcomes
+    kPhKeys,        // sorting outcomes into distinct count keys
+    kPhRelease,     // freeing the call's device buffers
+    kPhTotal,
+    kNumCallPhases
+};
+
 struct ProfileData {
     bool present = false;
     ProfileAcc acc;
@@ -100,6 +117,10 @@ class Simulator {
         std::lock_guard<std::mutex> lk(mu_);
         planner_log_.push_back(line);
     }
+    void last_call_phases(double* out) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (int i = 0; i < kNumCallPhases; i++) out[i] = phases_[i];
+    }
     std::string planner_log() {
         std::lock_guard<std::mutex> lk(mu_);
         std::string s;
@@ -114,6 +135,11 @@ class Simulator {
     std::shared_ptr<Device> dev_;
     const CostModel* model_ = nullptr;
     std::vector<std::string> planner_log_;
+    double phases_[kNumCallPhases] = {};
+    void set_phase(int i, double v) {
+        std::lock_guard<std::mutex> lk(mu_);
+        phases_[i] = v;
+    }
     uint64_t next_seed();
     ShotOutput run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots, uint64_t seed,
                          bool profile);

@@ -574,6 +574,7 @@ _plan_planner = _sig("dq_plan_planner", [_P, ctypes.POINTER(ctypes.c_double), ct
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
 _plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
 _sim_log = _sig("dq_sim_planner_log", [_P, ctypes.POINTER(ctypes.c_char_p)])
+_sim_phases = _sig("dq_sim_last_call_phases", [_P, _P, _u64])
 _measure_noalloc = _sig("dq_measure_noalloc", [_P, ctypes.c_int, _u64, _u64, _u64, ctypes.c_int, _P, _P, _P])
 
 
@@ -670,6 +671,16 @@ def planner_log(simulator):
         return [_json.loads(line) for line in out.value.decode().splitlines() if line.strip()]
     finally:
         _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+CALL_PHASES = ("parse", "compile", "state", "plan", "run", "sums", "sample", "keys", "release", "total")
+
+
+def last_call_phases(simulator):
+    """Host seconds per phase of the simulator's last simulate_shots call (dq_sim_last_call_phases)."""
+    out = np.zeros(len(CALL_PHASES), dtype=np.float64)
+    _check(_sim_phases(simulator._h, out.ctypes.data, len(CALL_PHASES)))
+    return dict(zip(CALL_PHASES, out.tolist()))
 
 
 def measure_noalloc(states_ptr, precision, num_states, num_qubits, qubit, seeds, draw_index, reset=False):

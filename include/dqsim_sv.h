@@ -234,11 +234,23 @@ DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops,
 /* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
 DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
 
+/* Host wall time, in seconds, of the phases of the simulator's last
+ * simulate_shots call (no counterpart in the reference, whose shots profile
+ * records preprocessing, fusion and total times only, simulator.rs:25-37):
+ * out[0] parse and validation, [1] compile, [2] statevector allocation,
+ * [3] pass planning and gate images, [4] launching the unitary prefix,
+ * [5] probability running sums (waits for the prefix to finish), [6] shot
+ * draws and their copy to the host, [7] count keys, [8] freeing the call's
+ * device buffers, [9] the whole call.  Terminal sampling fills every phase;
+ * trajectories fill 0, 1 and 9. */
+#define DQ_CALL_PHASES 10
+DQ_API int dq_sim_last_call_phases(dq_sim* sim, double* out, uint64_t n);
+
 /* Measure without allocating.  No counterpart in the reference: it serves
- * callers that cannot call cudaMalloc -- code running while a CUDA stream is
- * being captured, hosts whose device memory belongs to their own budgeted
- * allocator, and latency-bound loops that cannot afford the device-wide
- * synchronisation an allocation may cause.  It measures `qubit` of each of
+ * callers that cannot call cudaMalloc -- hosts whose device memory belongs to
+ * their own budgeted allocator and that forbid side allocations, and
+ * latency-bound loops that cannot afford the device-wide synchronisation an
+ * allocation or a free may cause.  It measures `qubit` of each of
  * `num_states` states of 2^num_qubits amplitudes stored back to back at
  * `states` (the caller's device memory, complex128 or complex64 by
  * `precision`), drawing from ChaCha8 stream seeds[i] at draw draw_index[i]
@@ -247,10 +259,16 @@ DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
  * memory outcomes[i].  It calls no cudaMalloc, cudaFree or allocating
  * library routine: its scratch is a fixed 256 KiB __device__ array that
  * every GPU loading this library holds until exit, looked up on the first
- * call on each device (make that first call before any stream capture).
- * Requests whose scratch would exceed 256 KiB (about 15 states of 22+
- * qubits, thousands of small states) fail with DQ_VALUE_ERROR.  All calls
- * share that array: calls whose GPU work overlaps race on it. */
+ * call on each device.  Requests whose scratch would exceed 256 KiB (about
+ * 15 states of 22+ qubits, thousands of small states) fail with
+ * DQ_VALUE_ERROR.  All calls share that array: calls whose GPU work overlaps
+ * race on it.  The work runs on the legacy default stream and the call
+ * returns after it has finished; the legacy stream does not wait for
+ * non-blocking streams, so work that writes `states` on another stream must
+ * be synchronised before the call.  A state whose norm is zero or not finite
+ * is left unchanged with outcomes[i] = -1 and the call returns
+ * DQ_RUNTIME_ERROR; the other states of that call are measured and collapsed
+ * all the same, with their outcomes in outcomes[]. */
 DQ_API int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit,
                               int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes);
 

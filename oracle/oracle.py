@@ -10,7 +10,7 @@ Pinning: the reference is Rust/PyO3 and cannot be built in this environment, so
 this restatement is pinned by the known-answer tests in the reference's own
 test suites (src/engine.rs:509-779, src/gates.rs:302-378,
 src/monolithic/statevector/shots.rs:262-308,
-src/monolithic/statevector/validation.rs:196-382 and
+src/monolithic/statevector/validation.rs:14-200 and
 tests/test_statevector.py:53-347), ported in tests/test_oracle_*.py.  Exact
 seeded counts depend on rand_chacha's ChaCha8 stream, restated in sv_oracle.c;
 the block function is pinned against ChaCha20 from ``cryptography``, the seed
@@ -795,7 +795,9 @@ def marginal_probs(state, n, qubits):
 
 
 def cdf_from_probs(probs):
-    cdf = np.array(probs, dtype=np.float64)
+    """Running sums of `probs` normalised in place (shots.rs:137-149 turns the
+    marginal table itself into the CDF); None for a nonfinite or zero total."""
+    cdf = np.ascontiguousarray(probs, dtype=np.float64)
     if not lib().orc_cdf_inplace(_ptr(cdf), len(cdf)):
         return None
     return cdf
@@ -860,6 +862,7 @@ def run_shots(ops, n, ncb, shots, seed, budget, max_parallel_shots, sample_termi
             cdf = cdf_from_probs(marginal_probs(state, n, qubits))
             if cdf is None:
                 raise RuntimeError("Invalid state normalization when sampling")
+            del state  # shots.rs:150
             draws = first_draws(seed, shots)
             idx = np.searchsorted(cdf, draws, side="right")
             idx = np.minimum(idx, len(cdf) - 1)

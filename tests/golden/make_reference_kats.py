@@ -40,50 +40,50 @@ KATS = {
         {"ref": "src/engine.rs:698", "qubits": [2, 1, 0], "expected_x36": [float(i) for i in range(1, 9)]},
     ],
     "validation_accept": [
-        {"ref": "statevector/validation.rs:238-255",
+        {"ref": "statevector/validation.rs:56-73",
          "instructions": [inst("h", qubit=0), inst("cx", control=0, target=2), inst("measure", qubit=2, cbit=1),
                           cond(0, 3, 2, cond(1, 1, 1, inst("reset", qubit=0)))]},
-        {"ref": "statevector/validation.rs:311", "instructions": [gen("remote_cu1", [0, 1], [0.4])]},
-        {"ref": "statevector/validation.rs:312", "instructions": [gen("remote_rzz", [0, 1], [0.4])]},
-        {"ref": "statevector/validation.rs:313", "instructions": [gen("REMOTE_CX", [0, 2], [])]},
-        {"ref": "statevector/validation.rs:314", "instructions": [gen("remote_barrier", [0, 1, 2], [])]},
-        {"ref": "statevector/validation.rs:373-380", "cregs": regs(("c", 0, 64)),
+        {"ref": "statevector/validation.rs:129", "instructions": [gen("remote_cu1", [0, 1], [0.4])]},
+        {"ref": "statevector/validation.rs:130", "instructions": [gen("remote_rzz", [0, 1], [0.4])]},
+        {"ref": "statevector/validation.rs:131", "instructions": [gen("REMOTE_CX", [0, 2], [])]},
+        {"ref": "statevector/validation.rs:132", "instructions": [gen("remote_barrier", [0, 1, 2], [])]},
+        {"ref": "statevector/validation.rs:191-198", "cregs": regs(("c", 0, 64)),
          "instructions": [cond(0, 64, U64_MAX, inst("x", qubit=0))]},
     ],
     "validation_reject": [
-        {"ref": "statevector/validation.rs:260-263", "instructions": [inst("cx", control=0, target=3)]},
-        {"ref": "statevector/validation.rs:264-267", "instructions": [inst("cx", control=1, target=1)]},
-        {"ref": "statevector/validation.rs:268", "instructions": [inst("id", qubit=3)]},
-        {"ref": "statevector/validation.rs:269", "instructions": [inst("measure", qubit=0, cbit=3)]},
-        {"ref": "statevector/validation.rs:270", "instructions": [cond(0, 1, 1, inst("x", qubit=99))]},
-        {"ref": "statevector/validation.rs:274-280", "qregs": regs(("a", 0, 1), ("b", 2, 1)),
+        {"ref": "statevector/validation.rs:78-81", "instructions": [inst("cx", control=0, target=3)]},
+        {"ref": "statevector/validation.rs:82-85", "instructions": [inst("cx", control=1, target=1)]},
+        {"ref": "statevector/validation.rs:86", "instructions": [inst("id", qubit=3)]},
+        {"ref": "statevector/validation.rs:87", "instructions": [inst("measure", qubit=0, cbit=3)]},
+        {"ref": "statevector/validation.rs:88", "instructions": [cond(0, 1, 1, inst("x", qubit=99))]},
+        {"ref": "statevector/validation.rs:92-98", "qregs": regs(("a", 0, 1), ("b", 2, 1)),
          "instructions": [inst("x", qubit=1)]},
-        {"ref": "statevector/validation.rs:281-287", "qregs": regs(("q", 0, 12)),
+        {"ref": "statevector/validation.rs:99-105", "qregs": regs(("q", 0, 12)),
          "instructions": [inst("cx", control=0, target=12)]},
-        {"ref": "statevector/validation.rs:293", "qregs": regs(("a", USIZE_MAX, 1)), "instructions": []},
-        {"ref": "statevector/validation.rs:294", "qregs": regs(("a", 0, 2), ("b", 1, 2)), "instructions": []},
-        {"ref": "statevector/validation.rs:295", "qregs": regs(("a", 0, 64)), "instructions": []},
-        {"ref": "statevector/validation.rs:301-305", "cregs": regs(("c", 0, 3), ("overlap", 1, 1)),
+        {"ref": "statevector/validation.rs:111", "qregs": regs(("a", USIZE_MAX, 1)), "instructions": []},
+        {"ref": "statevector/validation.rs:112", "qregs": regs(("a", 0, 2), ("b", 1, 2)), "instructions": []},
+        {"ref": "statevector/validation.rs:113", "qregs": regs(("a", 0, 64)), "instructions": []},
+        {"ref": "statevector/validation.rs:119-123", "cregs": regs(("c", 0, 3), ("overlap", 1, 1)),
          "instructions": []},
-        {"ref": "statevector/validation.rs:319", "instructions": [gen("remote_cu1", [0, 1], [])]},
-        {"ref": "statevector/validation.rs:320", "instructions": [gen("remote_cx", [0], [])]},
-        {"ref": "statevector/validation.rs:321", "instructions": [gen("remote_epr", [0, 1, 2], [])]},
-        {"ref": "statevector/validation.rs:322", "instructions": [gen("remote_cz", [0, 1], [0.2])]},
-        {"ref": "statevector/validation.rs:323", "instructions": [gen("circuit-123", [0], [])]},
-        {"ref": "statevector/validation.rs:324", "instructions": [gen("remote_barrier", [1, 1], [])]},
-        {"ref": "statevector/validation.rs:325-327", "instructions": [inst("classical", name="opaque")]},
-        {"ref": "statevector/validation.rs:336-341",
+        {"ref": "statevector/validation.rs:137", "instructions": [gen("remote_cu1", [0, 1], [])]},
+        {"ref": "statevector/validation.rs:138", "instructions": [gen("remote_cx", [0], [])]},
+        {"ref": "statevector/validation.rs:139", "instructions": [gen("remote_epr", [0, 1, 2], [])]},
+        {"ref": "statevector/validation.rs:140", "instructions": [gen("remote_cz", [0, 1], [0.2])]},
+        {"ref": "statevector/validation.rs:141", "instructions": [gen("circuit-123", [0], [])]},
+        {"ref": "statevector/validation.rs:142", "instructions": [gen("remote_barrier", [1, 1], [])]},
+        {"ref": "statevector/validation.rs:143-145", "instructions": [inst("classical", name="opaque")]},
+        {"ref": "statevector/validation.rs:154-159",
          "instructions": [inst("u3", qubit=0, theta=0.0, phi=float("nan"), lam=0.0)]},
-        {"ref": "statevector/validation.rs:342-349",
+        {"ref": "statevector/validation.rs:160-167",
          "instructions": [inst("cu", control=0, target=1, theta=0.0, phi=0.0, lam=0.0, gamma=float("inf"))]},
-        {"ref": "statevector/validation.rs:350", "instructions": [gen("remote_rzz", [0, 1], [float("-inf")])]},
-        {"ref": "statevector/validation.rs:351-355",
+        {"ref": "statevector/validation.rs:168", "instructions": [gen("remote_rzz", [0, 1], [float("-inf")])]},
+        {"ref": "statevector/validation.rs:169-173",
          "instructions": [inst("u2", qubit=0, phi=1.7976931348623157e308, lam=1.7976931348623157e308)]},
-        {"ref": "statevector/validation.rs:364", "instructions": [cond(0, 0, 0, inst("x", qubit=0))]},
-        {"ref": "statevector/validation.rs:365", "instructions": [cond(0, 65, 0, inst("x", qubit=0))]},
-        {"ref": "statevector/validation.rs:366", "instructions": [cond(0, 1, 2, inst("x", qubit=0))]},
-        {"ref": "statevector/validation.rs:367", "instructions": [cond(2, 2, 0, inst("x", qubit=0))]},
-        {"ref": "statevector/validation.rs:368", "instructions": [cond(USIZE_MAX, 2, 0, inst("x", qubit=0))]},
+        {"ref": "statevector/validation.rs:182", "instructions": [cond(0, 0, 0, inst("x", qubit=0))]},
+        {"ref": "statevector/validation.rs:183", "instructions": [cond(0, 65, 0, inst("x", qubit=0))]},
+        {"ref": "statevector/validation.rs:184", "instructions": [cond(0, 1, 2, inst("x", qubit=0))]},
+        {"ref": "statevector/validation.rs:185", "instructions": [cond(2, 2, 0, inst("x", qubit=0))]},
+        {"ref": "statevector/validation.rs:186", "instructions": [cond(USIZE_MAX, 2, 0, inst("x", qubit=0))]},
     ],
     # tests/test_statevector.py:215-232 (ValueError before execution)
     "api_invalid": [

@@ -254,13 +254,13 @@ def _validate(instructions, qregs=None, cregs=None):
 
 @pytest.mark.parametrize("case", GOLDEN["validation_accept"])
 def test_validation_accepts(case):
-    # src/monolithic/statevector/validation.rs:238-331
+    # src/monolithic/statevector/validation.rs:56-149
     _validate(case["instructions"], case.get("qregs"), case.get("cregs"))
 
 
 @pytest.mark.parametrize("case", GOLDEN["validation_reject"])
 def test_validation_rejects(case):
-    # src/monolithic/statevector/validation.rs:257-381
+    # src/monolithic/statevector/validation.rs:75-199
     with pytest.raises(ValueError):
         _validate(case["instructions"], case.get("qregs"), case.get("cregs"))
 
