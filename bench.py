@@ -384,6 +384,17 @@ def main():
         tiled_fid, tiled_err = compare_plain(plant)
         out_forms["complex128_tiled"] = {**summarize(stt, mst, peak), "fidelity": tiled_fid,
                                          "max_amp_err": tiled_err}
+        tile = stt.get("tile")
+        if tile and tile["ms"] > 0:
+            # FP64 roofline of the tile kernel: its arithmetic over the device's FP64 FMA rate
+            # (measured by the library's own kernel).
+            fl = plant.flops()["cuda_core"]
+            fp64 = dqsim._core.device_fp64_tflops(local)
+            ach = fl / (tile["ms"] * 1e-3) / 1e12
+            out_forms["complex128_tiled"]["fp64_roofline"] = {
+                "kernel": "k_tile<double2>", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                "frac": ach / fp64, "peak_kind": "measured (dq_device_fp64_tflops)", "flops": fl,
+                "launches": tile["launches"]}
         del plant, simt
 
     # complex64 on CUDA cores (13-qubit tiles, width-2 fusion).

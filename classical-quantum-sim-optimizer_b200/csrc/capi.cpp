@@ -14,6 +14,7 @@
 using namespace dq;
 
 namespace dq {
+double fp64_fma_tflops(int device);
 void measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit, int reset,
                      const uint64_t* seeds, const uint64_t* draw_index, int* outcomes);
 }
@@ -592,6 +593,15 @@ int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int
     });
 }
 
+int dq_plan_flops(const dq_plan* p, double* cuda_core_flops, double* tensor_flops) {
+    return guard([&] {
+        need(p, "plan");
+        need(cuda_core_flops, "cuda_core_flops");
+        need(tensor_flops, "tensor_flops");
+        p->impl->flops(cuda_core_flops, tensor_flops);
+    });
+}
+
 int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops, uint64_t* fused_blocks) {
     return guard([&] {
         need(p, "plan");
@@ -610,6 +620,13 @@ int dq_sim_planner_log(dq_sim* sim, char** out_text) {
         if (!buf) throw std::bad_alloc();
         std::memcpy(buf, s.c_str(), s.size() + 1);
         *out_text = buf;
+    });
+}
+
+int dq_device_fp64_tflops(int device, double* tflops) {
+    return guard([&] {
+        need(tflops, "tflops");
+        *tflops = fp64_fma_tflops(device);
     });
 }
 

@@ -370,6 +370,62 @@ double Executor::step_bytes(size_t i, const k::Batch& b) const {
     }
 }
 
+namespace {
+// Real operations of a 2^k x 2^k complex matrix-vector product.
+double dense_flops(int k) {
+    const double d = double(1 << k);
+    return d * d * 6.0 + (d * d - d) * 2.0;
+}
+}  // namespace
+
+void Executor::arith_flops(const k::Batch& b, double* cuda_core, double* tensor) const {
+    const double amps = double(uint64_t(1) << b.n) * double(b.W);
+    double cc = 0.0, tc = 0.0;
+    for (const Step& s : steps_) {
+        if (s.fused >= 0) {
+            const FusedPass& p = fused_[size_t(s.fused)];
+            tc += double(p.nblocks) * (amps / double(1 << kFusedM)) * 3.0 * 2.0 * 128.0 * 64.0 * 64.0;
+            continue;
+        }
+        if (s.pass >= 0) {
+            const TilePass& p = passes_[size_t(s.pass)];
+            const int m = int(p.qubits.size());
+            const double tiles = amps / double(uint64_t(1) << m);
+            double per_tile = 0.0;
+            for (const TileOp& op : p.ops) {
+                const double items = double(uint64_t(1) << (m - op.nins));
+                switch (op.type) {
+                    case TileOp::kOne: per_tile += items * 28.0; break;
+                    case TileOp::kDiagEntry: per_tile += items * 6.0; break;
+                    case TileOp::kDiagFull: per_tile += double(uint64_t(1) << m) * 6.0; break;
+                    case TileOp::kDense: per_tile += double(uint64_t(1) << (m - op.k)) * dense_flops(op.k); break;
+                    default: break;  // X and swap move amplitudes only
+                }
+            }
+            cc += tiles * per_tile;
+            continue;
+        }
+        const double pairs = amps / 2.0 / double(uint64_t(1) << s.controls.size());
+        switch (s.type) {
+            case Operation::One: cc += pairs * 28.0; break;
+            case Operation::Diagonal: {
+                const int kq = int(s.qubits.size());
+                double e = 0;
+                for (auto& d : s.diag)
+                    if (!(d.x == 1.0 && d.y == 0.0)) e++;
+                cc += amps / double(1 << kq) * e * 6.0;
+                break;
+            }
+            case Operation::Dense: cc += amps / double(1 << s.qubits.size()) * dense_flops(int(s.qubits.size())); break;
+            case Operation::Measure:
+            case Operation::Reset: cc += amps * 5.0; break;  // |a|^2 sums, then one scale per kept amplitude
+            default: break;
+        }
+    }
+    *cuda_core = cc;
+    *tensor = tc;
+}
+
 Executor::Executor(const std::vector<Operation>& ops, size_t begin, size_t end, const ExecConfig& cfg) : cfg_(cfg) {
     size_t seg = begin;
     if (cfg_.fuse > kTileMaxDense) cfg_.fuse = kTileMaxDense;

@@ -27,15 +27,15 @@ void parallel_for(size_t count, const std::function<void(size_t)>& fn);
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
-    cudaStream_t stream = nullptr;  // set: stream-ordered block from the device's memory pool
+    cudaStream_t stream = nullptr;  // set: stream-ordered block from the engine's memory pool
     DevMem() = default;
     DevMem(const DevMem&) = delete;
     DevMem& operator=(const DevMem&) = delete;
     ~DevMem() { release(); }
     void alloc(size_t b, const char* what);
-    // Stream-ordered allocation: the block returns to the device pool when
-    // released, in order on stream s, so the next large buffer of the same
-    // size costs no driver mapping.
+    // Stream-ordered allocation from the engine's pool on this device: the
+    // block returns to the pool when released, in order on stream s, so the
+    // next large buffer of the same size costs no driver mapping.
     void alloc_on(size_t b, cudaStream_t s, const char* what);
     void ensure(size_t b, const char* what) {
         if (b > bytes) alloc(b, what);
@@ -139,6 +139,11 @@ class Executor {
     size_t steps() const { return steps_.size(); }
     // Algorithmic bytes one step moves for a batch (the roofline numerator).
     double step_bytes(size_t i, const k::Batch& b) const;
+    // Arithmetic of one run over a batch, for the FLOP rooflines: real
+    // floating-point operations on CUDA cores (a complex product counts 6, a
+    // complex sum 2; FP64 for complex128 states, FP32 for complex64) and the
+    // f16 tensor-core FLOPs the fused blocks issue.
+    void arith_flops(const k::Batch& b, double* cuda_core, double* tensor) const;
 
     size_t passes() const { return passes_.size() + fused_.size(); }
     size_t fused_blocks() const { return fused_blocks_host_.size(); }

@@ -37,6 +37,10 @@ class Plan {
         *used_learned = used_learned_ ? 1 : 0;
         *rejected = rejected_ ? 1 : 0;
     }
+    // Arithmetic of one run's operations (Executor::arith_flops).
+    void flops(double* cuda_core, double* tensor) const {
+        ex_->arith_flops(st_.view(nullptr, 1), cuda_core, tensor);
+    }
     size_t passes() const { return ex_ ? ex_->passes() : 0; }
     size_t tile_ops() const { return ex_ ? ex_->tile_ops() : 0; }
     size_t fused_blocks() const { return ex_ ? ex_->fused_blocks() : 0; }

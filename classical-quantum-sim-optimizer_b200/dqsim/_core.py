@@ -483,6 +483,12 @@ class PreparedCircuit:
         _check(_plan_planner(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(u), ctypes.byref(r)))
         return {"learned_ms": a.value, "greedy_ms": b.value, "used_learned": bool(u.value), "rejected": bool(r.value)}
 
+    def flops(self):
+        """Arithmetic of one run: CUDA-core real FLOPs and tensor-core f16 FLOPs (dq_plan_flops)."""
+        c, tc = ctypes.c_double(), ctypes.c_double()
+        _check(_plan_flops(self._h, ctypes.byref(c), ctypes.byref(tc)))
+        return {"cuda_core": c.value, "tensor": tc.value}
+
     def shape(self):
         p, t, f = _u64(), _u64(), _u64()
         _check(_plan_shape(self._h, ctypes.byref(p), ctypes.byref(t), ctypes.byref(f)))
@@ -573,8 +579,10 @@ _sim_set_cm = _sig("dq_sim_set_cost_model", [_P, _P])
 _plan_planner = _sig("dq_plan_planner", [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
 _plan_shape = _sig("dq_plan_shape", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_plan_flops = _sig("dq_plan_flops", [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)])
 _sim_log = _sig("dq_sim_planner_log", [_P, ctypes.POINTER(ctypes.c_char_p)])
 _sim_phases = _sig("dq_sim_last_call_phases", [_P, _P, _u64])
+_fp64_tflops = _sig("dq_device_fp64_tflops", [ctypes.c_int, ctypes.POINTER(ctypes.c_double)])
 _measure_noalloc = _sig("dq_measure_noalloc", [_P, ctypes.c_int, _u64, _u64, _u64, ctypes.c_int, _P, _P, _P])
 
 
@@ -681,6 +689,13 @@ def last_call_phases(simulator):
     out = np.zeros(len(CALL_PHASES), dtype=np.float64)
     _check(_sim_phases(simulator._h, out.ctypes.data, len(CALL_PHASES)))
     return dict(zip(CALL_PHASES, out.tolist()))
+
+
+def device_fp64_tflops(device=0):
+    """FP64 FMA throughput of a device in TFLOP/s, measured by the library's own kernel."""
+    out = ctypes.c_double()
+    _check(_fp64_tflops(int(device), ctypes.byref(out)))
+    return out.value
 
 
 def measure_noalloc(states_ptr, precision, num_states, num_qubits, qubit, seeds, draw_index, reset=False):

@@ -229,10 +229,23 @@ DQ_API int dq_cost_model_set_params(dq_cost_model* m, const float* in, uint64_t 
 DQ_API int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m);
 /* Planner outcome of a prepared circuit built while a model was attached. */
 DQ_API int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int* used_learned, int* rejected);
+/* Arithmetic of one run of the kept plan (no counterpart in the reference):
+ * real floating-point operations on CUDA cores (a complex product counts 6, a
+ * complex sum 2; FP64 for complex128 states, FP32 for complex64) and the f16
+ * tensor-core FLOPs of the fused blocks (three 128 x 64 x 64 products per
+ * block and 4096-amplitude tile).  The numerators of the FLOP rooflines. */
+DQ_API int dq_plan_flops(const dq_plan* p, double* cuda_core_flops, double* tensor_flops);
 /* Passes, CUDA-core tile operations and tensor-core fused blocks of the kept plan. */
 DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops, uint64_t* fused_blocks);
 /* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
 DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
+
+/* FP64 fused multiply-add throughput of CUDA device `device` in TFLOP/s,
+ * measured by a kernel of this library (eight independent FMA chains per
+ * thread, several blocks per SM, best of three timed launches).  No
+ * counterpart in the reference; it is the denominator of the complex128 tile
+ * kernel's FP64 roofline. */
+DQ_API int dq_device_fp64_tflops(int device, double* tflops);
 
 /* Host wall time, in seconds, of the phases of the simulator's last
  * simulate_shots call (no counterpart in the reference, whose shots profile
