@@ -9,6 +9,7 @@
 #include "batch.hpp"
 #include "cost.hpp"
 #include "plan.hpp"
+#include "portfolio.hpp"
 #include "simulator.hpp"
 
 using namespace dq;
@@ -473,11 +474,51 @@ int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items) {
 void dq_batch_free(dq_batch* b) { delete b; }
 
 int dq_cost_model_create(int device, uint64_t seed, dq_cost_model** out) {
+    return dq_cost_model_create_kind(device, seed, DQ_COST_TILE_OPS, out);
+}
+
+int dq_cost_model_create_kind(int device, uint64_t seed, int kind, dq_cost_model** out) {
     return guard([&] {
         need(out, "out");
         auto m = std::make_unique<dq_cost_model>();
-        m->impl = std::make_unique<CostModel>(device, seed);
+        m->impl = std::make_unique<CostModel>(device, seed, kind);
         *out = m.release();
+    });
+}
+
+int dq_cost_model_kind(const dq_cost_model* m, int* kind) {
+    return guard([&] {
+        need(m, "model");
+        need(kind, "kind");
+        *kind = m->impl->kind();
+    });
+}
+
+namespace {
+void give_text(const std::string& s, char** out_text) {
+    char* buf = static_cast<char*>(std::malloc(s.size() + 1));
+    if (!buf) throw std::bad_alloc();
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    *out_text = buf;
+}
+}  // namespace
+
+int dq_fused_portfolio(dq_sim* sim, const char* json, size_t len, int wide, int measure, const dq_cost_model* model,
+                       char** out_text) {
+    return guard([&] {
+        need(sim, "sim");
+        need(json, "json");
+        need(out_text, "out_text");
+        give_text(fused_portfolio_json(*sim->impl, json, len, wide != 0, measure != 0, model ? model->impl.get() : nullptr),
+                  out_text);
+    });
+}
+
+int dq_fused_random_passes(dq_sim* sim, int num_qubits, uint64_t count, uint64_t seed, int measure, char** out_text) {
+    return guard([&] {
+        need(sim, "sim");
+        need(out_text, "out_text");
+        give_text(fused_random_passes_json(*sim->impl, num_qubits, count, seed, measure != 0), out_text);
     });
 }
 

@@ -225,7 +225,42 @@ void fused_block_features(int gates, uint32_t local_mask, int nblocks, float* ou
     out[15] = 1.f;
 }
 
-CostModel::CostModel(int device, uint64_t seed) : device_(device) {
+void fused_pass_features(int n, uint64_t states, const std::vector<int>& tile_qubits, int nblocks, int gates,
+                         float* out) {
+    for (int i = 0; i < F; i++) out[i] = 0.f;
+    uint64_t T = 0;
+    for (int q : tile_qubits) T |= uint64_t(1) << q;
+    const int nb = std::max(1, nblocks);
+    out[0] = float(n) / 32.f;
+    out[1] = float(nblocks) / 8.f;
+    out[2] = 1.f / float(nb);
+    // Tile qubits by position (stride 8 B << q in the state), in bins of four
+    // from qubit 2 (qubits 0 and 1 are in every fused tile).
+    for (int q : tile_qubits)
+        if (q >= kFusedPinned) out[3 + std::min(7, (q - kFusedPinned) / 4)] += 0.25f;
+    int top = 0;
+    for (int q : tile_qubits) top += q >= n - 3 ? 1 : 0;
+    out[11] = float(top) / 3.f;
+    // The ingredients of the hand rule: tile qubits lengthening the runs that
+    // the ~2^9 tiles in flight read together, and where those runs end.
+    int run_bits = 0, outside = 0, c = n;
+    for (int q = 0; q < n; q++) {
+        if ((T >> q) & 1) {
+            run_bits += q >= kFusedPinned ? 1 : 0;
+        } else if (++outside > 9) {
+            c = q;
+            break;
+        }
+    }
+    out[12] = float(run_bits) / 8.f;
+    out[13] = float(c) / 32.f;
+    const FusedTma tma = fused_tma_plan(tile_qubits, n, states);
+    out[14] = tma.ok ? std::log2(float(tma.copies)) / 4.f : 1.25f;  // per-thread loads without TMA
+    out[15] = float(gates) / (16.f * float(nb));
+}
+
+CostModel::CostModel(int device, uint64_t seed, int kind) : device_(device), kind_(kind) {
+    if (kind != kCostTileOps && kind != kCostFusedPasses) fail(kValueError, "unknown cost model kind");
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaMalloc(&params_, sizeof(float) * (3 * size_t(kStored))), "cost model parameters");
@@ -373,6 +408,31 @@ double CostModel::predict_fused(const FusedPass& p) const {
     double total = 0;
     for (float v : y) total += std::exp(double(v));
     return total;
+}
+
+std::vector<double> CostModel::predict_passes_ms(const FusedPortfolio& pf, uint64_t states) const {
+    const size_t np = pf.built.size();
+    std::vector<double> ms(np, 0.0);
+    if (np == 0) return ms;
+    std::vector<float> X(np * F), y(np);
+    for (size_t i = 0; i < np; i++) {
+        const FusedPass& fp = pf.built[i].fp;
+        int gates = 0;
+        for (int g : fp.block_gates) gates += g;
+        fused_pass_features(pf.n, states, fp.qubits, fp.nblocks, gates, X.data() + i * F);
+    }
+    predict(X.data(), np, y.data());
+    const double tiles = double(states << (pf.n - kFusedM));
+    for (size_t i = 0; i < np; i++) ms[i] = std::exp(double(y[i])) * tiles * 1e-6;  // ns per tile -> ms
+    return ms;
+}
+
+std::vector<double> CostModel::predict_plans_ms(const FusedPortfolio& pf, uint64_t states) const {
+    const std::vector<double> pass_ms = predict_passes_ms(pf, states);
+    std::vector<double> plan_ms(pf.plans.size(), 0.0);
+    for (size_t i = 0; i < pf.plans.size(); i++)
+        for (size_t slot : pf.slots[i]) plan_ms[i] += pass_ms[slot];
+    return plan_ms;
 }
 
 }  // namespace dq

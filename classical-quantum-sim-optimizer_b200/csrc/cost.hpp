@@ -15,6 +15,16 @@
 // The planner asks it, per pass, which fusion width (CUDA cores) or the
 // tensor-core blocks is cheapest; the greedy plan stays the fallback and the
 // judge.
+//
+// A model of the second kind (kCostFusedPasses) prices whole tensor-core
+// passes instead: from a pass's tile qubits (where they sit in the state, the
+// hand rule's run and spread ingredients, its TMA box count), its block count
+// and gates per block and the state size, it predicts the log of the pass's
+// device time per tile.  Trained on passes the engine times itself (every
+// distinct pass of the candidate plans of recorded circuits, and seeded
+// random passes), it chooses which of the candidate fused plans to run in
+// place of the hand-fitted pass and spread constants; the hand rule's plan is
+// the fallback and the judge.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -38,10 +48,20 @@ void tile_op_features(const TileOp& op, int m, bool c64, float* out);
 // Features of one tensor-core block (local qubit mask, fused gates) in a
 // fused pass of `nblocks` blocks.
 void fused_block_features(int gates, uint32_t local_mask, int nblocks, float* out);
+// Features of one whole fused pass (kCostFusedPasses): its 12 tile qubits
+// over `states` states of n qubits, its block count and gates.
+void fused_pass_features(int n, uint64_t states, const std::vector<int>& tile_qubits, int nblocks, int gates,
+                         float* out);
+
+enum CostKind : int {
+    kCostTileOps = 0,      // CUDA-core tile operations and tensor-core blocks (fusion width per pass)
+    kCostFusedPasses = 1,  // whole tensor-core passes (which candidate fused plan runs)
+};
 
 class CostModel {
   public:
-    CostModel(int device, uint64_t seed);
+    CostModel(int device, uint64_t seed, int kind = kCostTileOps);
+    int kind() const { return kind_; }
     ~CostModel();
     void add_samples(const float* X, const float* y, size_t n);
     size_t num_samples() const { return y_.size(); }
@@ -62,10 +82,15 @@ class CostModel {
     double predict_ops(const std::vector<TileOp>& ops, int m, bool c64) const;
     // Sum of the predicted costs of a fused pass's blocks.
     double predict_fused(const FusedPass& p) const;
+    // Predicted device milliseconds of each distinct pass of a fused
+    // portfolio over `states` states (kCostFusedPasses), and of each plan.
+    std::vector<double> predict_passes_ms(const FusedPortfolio& pf, uint64_t states) const;
+    std::vector<double> predict_plans_ms(const FusedPortfolio& pf, uint64_t states) const;
     int device() const { return device_; }
 
   private:
     int device_;
+    int kind_ = kCostTileOps;
     bool trained_ = false;
     std::vector<float> X_, y_;
     void* params_ = nullptr;  // device: params, adam m, adam v

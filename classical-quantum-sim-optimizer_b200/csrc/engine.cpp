@@ -456,7 +456,28 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     o.model = cfg_.model;
     o.chosen_widths = &widths_;
     if (cfg_.fused && cfg_.c64 && cfg_.n >= kFusedM) {
-        std::vector<BuiltFusedPass> built = plan_fused(ops, begin, end, cfg_.n, o);
+        std::vector<BuiltFusedPass> built;
+        {
+            FusedPlanChoice ch;
+            FusedPortfolio pf = fused_portfolio(ops, begin, end, cfg_.n, o, fused_caps(cfg_.n, cfg_.pass_model != nullptr));
+            ch.caps = pf.caps;
+            ch.rule_cost = pf.rule_cost;
+            ch.rule_choice = ch.chosen = pf.rule_choice;
+            for (size_t i = 0; i < pf.plans.size(); i++) {
+                size_t nb = 0;
+                for (size_t slot : pf.slots[i]) nb += size_t(pf.built[slot].fp.nblocks);
+                ch.passes.push_back(pf.plans[i].size());
+                ch.blocks.push_back(nb);
+            }
+            if (cfg_.pass_model) {
+                // The learned pass-cost model picks the plan of least predicted time.
+                ch.predicted_ms = cfg_.pass_model->predict_plans_ms(pf, 1);
+                for (size_t i = 0; i < ch.predicted_ms.size(); i++)
+                    if (ch.predicted_ms[i] < ch.predicted_ms[ch.chosen]) ch.chosen = i;
+            }
+            built = take_fused_plan(pf, ch.chosen);
+            fused_choices_.push_back(std::move(ch));
+        }
         // With a trained cost model each pass runs on whichever executor it
         // predicts cheapest: tensor-core blocks (0) or CUDA-core tile operations
         // fused to width 1..kTileMaxDense.

@@ -125,6 +125,19 @@ struct ExecConfig {
     bool c64 = false;
     const CostModel* model = nullptr;  // learned fusion-width choice per pass
     bool fused = false;  // complex64: 5-qubit blocks on tcgen05 (12-qubit tiles)
+    // Learned pass-cost model: picks the fused plan of least predicted time
+    // from the wide portfolio (kCostFusedPasses models only).
+    const CostModel* pass_model = nullptr;
+};
+
+// How the fused plan of a segment was chosen: the portfolio's caps, the hand
+// rule's cost of each plan and its choice, and, with a pass-cost model, the
+// predicted milliseconds of each plan and the model's choice.
+struct FusedPlanChoice {
+    std::vector<int> caps;
+    std::vector<double> rule_cost, predicted_ms;
+    std::vector<size_t> passes, blocks;
+    size_t rule_choice = 0, chosen = 0;
 };
 
 // A compiled operation list lowered to launch descriptors, with every matrix
@@ -149,6 +162,7 @@ class Executor {
     size_t fused_blocks() const { return fused_blocks_host_.size(); }
     size_t raw_ops_in_passes() const;
     const std::vector<int>& chosen_widths() const { return widths_; }
+    const std::vector<FusedPlanChoice>& fused_choices() const { return fused_choices_; }
     size_t tile_ops() const { return tile_ops_host_.size(); }
     // Times every pass (CUDA events), shares each pass's time among its
     // operations by their clock64 cycles or equally among its tensor-core
@@ -185,6 +199,7 @@ class Executor {
     bool uploaded_ = false;
     ExecConfig cfg_;
     std::vector<int> widths_;
+    std::vector<FusedPlanChoice> fused_choices_;
     void lower(const Operation& op, std::vector<Condition>& conds);
     void lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end);
 };

@@ -1,5 +1,7 @@
 #include "plan.hpp"
 
+#include "cost.hpp"
+
 #include <algorithm>
 #include <cstdio>
 #include <string>
@@ -51,6 +53,7 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
         run(false);
         learned_ms_ = std::min(run(false), run(false));
         std::vector<int> widths = ex_->chosen_widths();
+        const std::vector<FusedPlanChoice> choices = ex_->fused_choices();
         rejected_ = learned_ms_ > greedy_ms_;
         if (rejected_) std::swap(ex_, learned);
         used_learned_ = !rejected_;
@@ -61,7 +64,26 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
                       "{\"qubits\": %llu, \"ops\": %llu, \"greedy_ms\": %.4f, \"learned_ms\": %.4f, \"rejected\": %s, ",
                       (unsigned long long)n_, (unsigned long long)ops_.size(), greedy_ms_, learned_ms_,
                       rejected_ ? "true" : "false");
-        sim.log_planner(std::string(buf) + "\"widths\": [" + w + "]}");
+        std::string line = std::string(buf) + "\"kind\": \"" +
+                           (model->kind() == kCostFusedPasses ? "fused_passes" : "tile_ops") + "\", \"widths\": [" + w +
+                           "], \"fused_plans\": [";
+        // Per planned segment: the candidate plans (spread cap, passes, blocks, hand-rule
+        // cost, predicted ms), the rule's choice and the model's.
+        for (size_t s = 0; s < choices.size(); s++) {
+            const FusedPlanChoice& c = choices[s];
+            line += s ? ", {" : "{";
+            line += "\"rule_choice\": " + std::to_string(c.rule_choice) + ", \"chosen\": " + std::to_string(c.chosen) +
+                    ", \"candidates\": [";
+            for (size_t i = 0; i < c.caps.size(); i++) {
+                std::snprintf(buf, sizeof buf,
+                              "%s{\"cap\": %d, \"passes\": %zu, \"blocks\": %zu, \"rule_cost\": %.2f, \"predicted_ms\": %.4f}",
+                              i ? ", " : "", c.caps[i], c.passes[i], c.blocks[i], c.rule_cost[i],
+                              i < c.predicted_ms.size() ? c.predicted_ms[i] : -1.0);
+                line += buf;
+            }
+            line += "]}";
+        }
+        sim.log_planner(line + "]}");
     }
 }
 

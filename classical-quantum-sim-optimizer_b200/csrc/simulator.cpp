@@ -1,5 +1,7 @@
 #include "simulator.hpp"
 
+#include "cost.hpp"
+
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -127,7 +129,10 @@ std::string json_double(double v) {
 
 ExecConfig exec_config(const Options& o, uint64_t n, bool force_per_gate, const CostModel* model) {
     ExecConfig c;
-    c.model = model;
+    if (model && model->kind() == kCostFusedPasses)
+        c.pass_model = model;
+    else
+        c.model = model;
     c.c64 = o.precision == Precision::C64;
     c.tiled = !force_per_gate && o.execution != 1;
     c.tile_m = o.tile_qubits > 0 ? o.tile_qubits : (c.c64 ? 13 : 12);

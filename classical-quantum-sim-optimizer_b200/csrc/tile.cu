@@ -1093,8 +1093,20 @@ TileOp lower_tile_op(const Operation& op, const std::vector<int>& local, std::ve
 
 }  // namespace
 
-std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
-                                       const TilePlanOptions& base) {
+std::vector<int> fused_caps(int n, bool wide) {
+    std::vector<int> caps{kFusedMaxSpread};
+    if (4 * (n - kFusedSpreadBit) - 4 > kFusedMaxSpread) {
+        caps.push_back(-1);
+        caps.push_back(kFusedMaxSpread - 4);
+        if (wide)
+            for (int c : {kFusedMaxSpread - 8, kFusedMaxSpread + 4, kFusedMaxSpread + 8})
+                if (c >= 0 && (c <= kFusedMaxSpread || 4 * (n - kFusedSpreadBit) - 4 > c)) caps.push_back(c);
+    }
+    return caps;
+}
+
+FusedPortfolio fused_portfolio(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                               const TilePlanOptions& base, const std::vector<int>& caps) {
     TilePlanOptions o = base;
     o.m = kFusedM;
     o.keep_raw = true;
@@ -1103,63 +1115,66 @@ std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t
     o.beam = kPlanBeam;
     o.model = nullptr;
     o.chosen_widths = nullptr;
-    // Where the cap can bind (the largest spread, every qubit from
-    // kFusedSpreadBit up in the tile, exceeds it) also plan with no cap (-1),
-    // the spread priced into the plan's cost instead, and with a cap one
-    // top qubit (4 quarters) lower.
-    std::vector<int> caps{kFusedMaxSpread};
-    if (4 * (n - kFusedSpreadBit) - 4 > kFusedMaxSpread) {
-        caps.push_back(-1);
-        caps.push_back(kFusedMaxSpread - 4);
-    }
-    std::vector<std::vector<TilePass>> plans(caps.size());
+    FusedPortfolio pf;
+    pf.n = n;
+    pf.caps = caps;
+    pf.plans.resize(caps.size());
     parallel_for(caps.size(), [&](size_t i) {
         TilePlanOptions oi = o;
         oi.max_spread = caps[i];
         std::vector<double2> unused;
-        plans[i] = plan_tiles(ops, begin, end, n, oi, &unused);
+        pf.plans[i] = plan_tiles(ops, begin, end, n, oi, &unused);
     });
     // The plans share passes (same tile qubits, same operations): each distinct
     // pass is fused into blocks once, all of them on pooled workers.
     std::map<std::pair<std::vector<int>, std::vector<size_t>>, size_t> slot_of;
     std::vector<const TilePass*> distinct;
-    std::vector<std::vector<size_t>> slots(plans.size());
-    for (size_t i = 0; i < plans.size(); i++)
-        for (const TilePass& p : plans[i]) {
+    pf.slots.resize(pf.plans.size());
+    for (size_t i = 0; i < pf.plans.size(); i++)
+        for (const TilePass& p : pf.plans[i]) {
             auto it = slot_of.emplace(std::make_pair(p.qubits, p.op_index), distinct.size()).first;
             if (it->second == distinct.size()) distinct.push_back(&p);
-            slots[i].push_back(it->second);
+            pf.slots[i].push_back(it->second);
         }
-    std::vector<BuiltFusedPass> built(distinct.size());
+    pf.built.resize(distinct.size());
     parallel_for(distinct.size(), [&](size_t k) {
-        BuiltFusedPass& b = built[k];
+        BuiltFusedPass& b = pf.built[k];
         b.fp = build_fused_pass(distinct[k]->raw, distinct[k]->qubits, b.blocks, b.upool);
     });
     const TileShape sh{kFusedM, n, kFusedPinned, kFusedSpreadBit, INT_MAX, o.inflight_bits};
-    size_t best = 0;
-    double best_cost = 0;
-    for (size_t i = 0; i < plans.size(); i++) {
-        double cost = kFusedPassCostBlocks * double(plans[i].size());
-        for (size_t k = 0; k < plans[i].size(); k++) {
+    pf.rule_cost.assign(pf.plans.size(), 0.0);
+    for (size_t i = 0; i < pf.plans.size(); i++) {
+        double cost = kFusedPassCostBlocks * double(pf.plans[i].size());
+        for (size_t k = 0; k < pf.plans[i].size(); k++) {
             uint64_t T = 0;
-            for (int q : plans[i][k].qubits) T |= uint64_t(1) << q;
+            for (int q : pf.plans[i][k].qubits) T |= uint64_t(1) << q;
             const int spread = sh.spread(T);
-            cost += built[slots[i][k]].fp.nblocks + (spread > kFusedMaxSpread + 4   ? kFusedSpreadCostBlocks[1]
-                                                     : spread > kFusedMaxSpread ? kFusedSpreadCostBlocks[0]
-                                                                                : 0.0);
+            cost += pf.built[pf.slots[i][k]].fp.nblocks + (spread > kFusedMaxSpread + 4   ? kFusedSpreadCostBlocks[1]
+                                                           : spread > kFusedMaxSpread ? kFusedSpreadCostBlocks[0]
+                                                                                      : 0.0);
         }
-        if (i == 0 || cost < best_cost) {
-            best = i;
-            best_cost = cost;
-        }
+        pf.rule_cost[i] = cost;
+        if (i == 0 || cost < pf.rule_cost[pf.rule_choice]) pf.rule_choice = i;
     }
-    std::vector<BuiltFusedPass> out(plans[best].size());
+    return pf;
+}
+
+std::vector<BuiltFusedPass> take_fused_plan(FusedPortfolio& pf, size_t i) {
+    std::vector<BuiltFusedPass> out(pf.plans[i].size());
     for (size_t k = 0; k < out.size(); k++) {
-        const size_t slot = slots[best][k];
-        out[k] = built[slot];
-        out[k].src = std::move(plans[best][k]);
+        const size_t slot = pf.slots[i][k];
+        out[k].fp = pf.built[slot].fp;
+        out[k].blocks = pf.built[slot].blocks;
+        out[k].upool = pf.built[slot].upool;
+        out[k].src = std::move(pf.plans[i][k]);
     }
     return out;
+}
+
+std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                                       const TilePlanOptions& base) {
+    FusedPortfolio pf = fused_portfolio(ops, begin, end, n, base, fused_caps(n, false));
+    return take_fused_plan(pf, pf.rule_choice);
 }
 
 void lower_pass_ops(const std::vector<Operation>& raw, const std::vector<int>& tile_qubits, int n, int width,

@@ -202,13 +202,38 @@ constexpr double kFusedPassCostBlocks = 3.0;
 // quarters, and by more (at 30 qubits about +4 ms and +8 ms).
 constexpr double kFusedSpreadCostBlocks[2] = {4.0, 8.0};
 
-// Plans ops[begin, end) as fused passes (kFusedM tile qubits, kFusedPinned
-// pinned, beam kPlanBeam) under the spread cap kFusedMaxSpread and, where it
-// can bind, also with no cap and with a cap 4 quarters lower; builds every
-// pass's blocks and returns the plan of lowest kFusedPassCostBlocks * passes
-// + blocks + kFusedSpreadCostBlocks per pass over the cap (the pass search
-// follows ops covered, not blocks, so the caps give different plans).  `base`
-// supplies seeds; the other planning fields are set here.
+// The candidate fused plans of ops[begin, end): one per spread cap (-1: no
+// cap), each planned with kFusedM tile qubits, kFusedPinned pinned and beam
+// kPlanBeam.  The plans share passes (same tile qubits, same operations), so
+// each distinct pass is fused into blocks once.  `rule_cost` prices each plan
+// by the hand-fitted rule: kFusedPassCostBlocks * passes + blocks +
+// kFusedSpreadCostBlocks per pass over kFusedMaxSpread; `rule_choice` is the
+// cheapest (the first on ties).
+struct FusedPortfolio {
+    int n = 0;
+    std::vector<int> caps;
+    std::vector<std::vector<TilePass>> plans;  // per cap: its passes (raw operations kept)
+    std::vector<std::vector<size_t>> slots;    // per cap: each pass's index in `built`
+    std::vector<BuiltFusedPass> built;         // distinct passes (their src left empty)
+    std::vector<double> rule_cost;
+    size_t rule_choice = 0;
+};
+
+// Spread caps of the portfolio.  The default set: kFusedMaxSpread and, where
+// it can bind (every qubit from kFusedSpreadBit up in the tile exceeds it),
+// also no cap and a cap 4 quarters lower.  The wide set, planned when a
+// learned pass-cost model chooses among the plans, adds caps from 8 quarters
+// below to 8 above.
+std::vector<int> fused_caps(int n, bool wide);
+FusedPortfolio fused_portfolio(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
+                               const TilePlanOptions& base, const std::vector<int>& caps);
+// The passes of plan i (each with its source pass), moved out of the portfolio.
+std::vector<BuiltFusedPass> take_fused_plan(FusedPortfolio& pf, size_t i);
+
+// Plans ops[begin, end) as fused passes: the default portfolio's rule choice
+// (the pass search follows ops covered, not blocks, so the caps give
+// different plans).  `base` supplies seeds; the other planning fields are set
+// here.
 std::vector<BuiltFusedPass> plan_fused(const std::vector<Operation>& ops, size_t begin, size_t end, int n,
                                        const TilePlanOptions& base);
 

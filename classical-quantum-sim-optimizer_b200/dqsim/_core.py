@@ -564,7 +564,12 @@ BATCH_SEED_STRIDE = 0x9E3779B97F4A7C15
 
 MLP_FEATURES = 16
 MLP_PARAMS = 5315
-_cm_create = _sig("dq_cost_model_create", [ctypes.c_int, _u64, ctypes.POINTER(_P)])
+_cm_create = _sig("dq_cost_model_create_kind", [ctypes.c_int, _u64, ctypes.c_int, ctypes.POINTER(_P)])
+_cm_kind = _sig("dq_cost_model_kind", [_P, ctypes.POINTER(ctypes.c_int)])
+_fused_portfolio = _sig("dq_fused_portfolio", [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _P,
+                                               ctypes.POINTER(ctypes.c_char_p)])
+_fused_random = _sig("dq_fused_random_passes", [_P, ctypes.c_int, _u64, _u64, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_char_p)])
 _cm_free = _sig("dq_cost_model_free", [_P], None)
 _cm_add = _sig("dq_cost_model_add_samples", [_P, _P, _P, _u64])
 _cm_record = _sig("dq_cost_model_record", [_P, _P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_u64)])
@@ -593,13 +598,28 @@ def _f32(a, cols=None):
     return a
 
 
-class CostModel:
-    """The planner's learned cost model (dq_cost_model_*): MLP 16-64-64-1, trained on device."""
+COST_KINDS = {"tile_ops": 0, "fused_passes": 1}
 
-    def __init__(self, device=0, seed=0):
+
+class CostModel:
+    """The planner's learned cost model (dq_cost_model_*): MLP 16-64-64-1, trained on device.
+
+    kind "tile_ops" prices CUDA-core tile operations and tensor-core blocks (it picks each pass's fusion
+    width); kind "fused_passes" prices whole tensor-core passes (it picks which candidate fused plan runs).
+    """
+
+    def __init__(self, device=0, seed=0, kind="tile_ops"):
+        if kind not in COST_KINDS:
+            raise ValueError(f"kind must be one of {sorted(COST_KINDS)}")
         h = _P()
-        _check(_cm_create(int(device), _as_u64(seed, "seed"), ctypes.byref(h)))
+        _check(_cm_create(int(device), _as_u64(seed, "seed"), COST_KINDS[kind], ctypes.byref(h)))
         self._h = h
+
+    @property
+    def kind(self):
+        k = ctypes.c_int()
+        _check(_cm_kind(self._h, ctypes.byref(k)))
+        return {v: n for n, v in COST_KINDS.items()}[k.value]
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -662,6 +682,42 @@ class CostModel:
     def params(self, value):
         p = _f32(value).reshape(-1)
         _check(_cm_set(self._h, p.ctypes.data_as(_P), p.shape[0]))
+
+
+def _take_text(out):
+    try:
+        return out.value.decode()
+    finally:
+        _string_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+def fused_portfolio(simulator, circuit, wide=True, measure=False, model=None):
+    """The candidate fused plans of a circuit's unitary prefix (dq_fused_portfolio) as a dict: per plan its
+    spread cap, hand-rule cost and pass indices; per distinct pass its tile qubits, blocks, gates and
+    features, with measure=True its device milliseconds and with a fused-pass model its prediction."""
+    import json as _json
+
+    text = _circuit_json(circuit)
+    out = ctypes.c_char_p()
+    _check(_fused_portfolio(simulator._h, text, len(text), 1 if wide else 0, 1 if measure else 0,
+                            None if model is None else model._h, ctypes.byref(out)))
+    return _json.loads(_take_text(out))
+
+
+def fused_random_passes(simulator, num_qubits, count, seed=0, measure=True):
+    """Seeded random fused passes with features and device milliseconds (dq_fused_random_passes)."""
+    import json as _json
+
+    out = ctypes.c_char_p()
+    _check(_fused_random(simulator._h, int(num_qubits), _as_u64(count, "count"), _as_u64(seed, "seed"),
+                         1 if measure else 0, ctypes.byref(out)))
+    return _json.loads(_take_text(out))
+
+
+def fused_pass_targets(passes, num_qubits):
+    """Training targets of the fused-pass model: log of each pass's device nanoseconds per tile."""
+    tiles = float(1 << (int(num_qubits) - 12))
+    return np.log(np.array([p["ms"] for p in passes], dtype=np.float64) * 1e6 / tiles).astype(np.float32)
 
 
 def set_cost_model(simulator, model):

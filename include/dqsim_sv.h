@@ -214,6 +214,18 @@ typedef struct dq_cost_model dq_cost_model;
 #define DQ_MLP_FEATURES 16
 #define DQ_MLP_PARAMS 5315 /* 5313 weights and biases + target mean and std */
 DQ_API int dq_cost_model_create(int device, uint64_t seed, dq_cost_model** out);
+/* Model kinds.  DQ_COST_TILE_OPS: the model above (tile-local operations and
+ * tensor-core blocks; picks each pass's fusion width).  DQ_COST_FUSED_PASSES:
+ * prices whole tensor-core passes from their tile qubits, block count, gates
+ * per block and the state size (log device nanoseconds per tile); attached to
+ * a complex64 simulator it picks, among the candidate fused plans of a wider
+ * set of spread caps, the one of least predicted time, in place of the
+ * hand-fitted pass and spread constants.  A prepared circuit then times that
+ * plan against the hand rule's and keeps the faster (rejections logged). */
+#define DQ_COST_TILE_OPS 0
+#define DQ_COST_FUSED_PASSES 1
+DQ_API int dq_cost_model_create_kind(int device, uint64_t seed, int kind, dq_cost_model** out);
+DQ_API int dq_cost_model_kind(const dq_cost_model* m, int* kind);
 DQ_API void dq_cost_model_free(dq_cost_model* m);
 DQ_API int dq_cost_model_add_samples(dq_cost_model* m, const float* features, const float* log_cycles, uint64_t n);
 DQ_API int dq_cost_model_record(dq_cost_model* m, dq_sim* sim, const char* json, size_t json_len, uint64_t* added);
@@ -227,6 +239,22 @@ DQ_API int dq_cost_model_gradients(const dq_cost_model* m, const float* features
 DQ_API int dq_cost_model_get_params(const dq_cost_model* m, float* out, uint64_t len);
 DQ_API int dq_cost_model_set_params(dq_cost_model* m, const float* in, uint64_t len);
 DQ_API int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m);
+/* The candidate fused plans of a circuit's unitary prefix as JSON text (no
+ * counterpart in the reference): per plan its spread cap, the hand rule's
+ * cost and its passes; per distinct pass its tile qubits, blocks, gates and
+ * DQ_COST_FUSED_PASSES features, with measure != 0 its device milliseconds
+ * (one k_fused launch on a complex64 state of the circuit's size on the
+ * simulator's device) and with a model its predicted milliseconds.  wide != 0
+ * plans the learned planner's wider set of caps.  Free with dq_string_free. */
+DQ_API int dq_fused_portfolio(dq_sim* sim, const char* json, size_t json_len, int wide, int measure,
+                              const dq_cost_model* model, char** out_text);
+/* `count` seeded random fused passes over num_qubits qubits (14..34): random
+ * tile qubits (qubits 0 and 1 plus ten drawn uniformly, low- or high-weighted,
+ * or as one window) and 1..10 clusters of random one- and two-qubit gates,
+ * with features and, with measure != 0, device milliseconds, as JSON text.
+ * Training data of the DQ_COST_FUSED_PASSES model. */
+DQ_API int dq_fused_random_passes(dq_sim* sim, int num_qubits, uint64_t count, uint64_t seed, int measure,
+                                  char** out_text);
 /* Planner outcome of a prepared circuit built while a model was attached. */
 DQ_API int dq_plan_planner(const dq_plan* p, double* learned_ms, double* greedy_ms, int* used_learned, int* rejected);
 /* Arithmetic of one run of the kept plan (no counterpart in the reference):
