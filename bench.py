@@ -583,85 +583,45 @@ def run_cases(args):
 
 
 def run_learned(args):
-    """Cost model trained on this engine's recorded timings (brickwork and QFT, 24..30 qubits),
-    then learned vs greedy plans on held-out depth-40 brickwork at 26, 30 and 33 qubits."""
+    """Learned fused-pass cost model: trained on the device on passes this engine times itself (seeded random
+    passes at 24-32 qubits and every distinct pass of the candidate plans of brickwork and QFT circuits of
+    24-30 qubits), then, on held-out circuits (depth-40 brickwork at 26, 30 and 33 qubits, QFT at 32), the plan
+    it picks against the hand rule's: each prepared circuit A/B-times the two and keeps the faster."""
     import dqsim
-    from dqsim import _core
+    from dqsim import _core, pass_costs
 
-    model = _core.CostModel(seed=args.seed)
     rec = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
     t0 = time.perf_counter()
-    for n in (24, 26, 28, 30):
-        for s in range(2):
-            model.record(rec, dqsim.workloads.brickwork(n, 40, seed=1000 + 10 * n + s, measure=False))
-        model.record(rec, dqsim.workloads.qft(n, seed=2000 + n))
+    rows = pass_costs.record(rec, seed=args.seed)
     record_s = time.perf_counter() - t0
-    samples = model.num_samples
-    mse = model.train(epochs=60, lr=2e-3)
+    del rec
+    t0 = time.perf_counter()
+    model, mse = pass_costs.train(rows, seed=args.seed)
+    train_s = time.perf_counter() - t0
     results = []
-    for n in (26, 30, 33):
-        circuit = dqsim.workloads.brickwork(n, 40, seed=9000 + n, measure=False)
+    for kind, n, seed in pass_costs.HELD_OUT:
+        circuit = pass_costs.circuit(kind, n, seed)
         sim = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
         _core.set_cost_model(sim, model)
         learned = _core.PreparedCircuit(sim, circuit)
         info = learned.planner()
         log = _core.planner_log(sim)[-1]
-        greedy_sim = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
-        greedy = _core.PreparedCircuit(greedy_sim, circuit)
-        tl = min(learned.run() for _ in range(2))
-        tg = min(greedy.run() for _ in range(2))
+        greedy = _core.PreparedCircuit(dqsim.StatevectorSimulator(seed=1, precision="complex64",
+                                                                  max_memory_mb=1 << 20), circuit)
+        tl = min(learned.run() for _ in range(3))
+        tg = min(greedy.run() for _ in range(3))
         fid, err = learned.compare(greedy)
-        row = {"qubits": n, "greedy_ms": tg, "kept_ms": tl, "ab_greedy_ms": info["greedy_ms"],
-               "ab_learned_ms": info["learned_ms"], "rejected": info["rejected"],
-               "per_pass_choice": log.get("widths"), "fidelity_vs_greedy": fid, "max_amp_err_vs_greedy": err}
-        if n <= 30:
-            _, ref = time_form(dqsim, circuit, "complex128", 0, 1, 0, 0, 1)
-            row["fidelity_vs_c128"] = learned.compare(ref)[0]
-            del ref
-        results.append(row)
+        seg = log["fused_plans"][0] if log.get("fused_plans") else {}
+        results.append({"circuit": f"{kind}-{n}q-seed{seed}", "greedy_ms": tg, "kept_ms": tl, "gain": tg / tl,
+                        "ab_greedy_ms": info["greedy_ms"], "ab_learned_ms": info["learned_ms"],
+                        "rejected": info["rejected"], "rule_choice": seg.get("rule_choice"),
+                        "model_choice": seg.get("chosen"), "candidates": seg.get("candidates"),
+                        "fidelity_vs_greedy": fid, "max_amp_err_vs_greedy": err})
         _core.set_cost_model(sim, None)
         del learned, greedy
-    # CUDA-core tiles in complex128: the model picks each pass's fusion width (1, 2 or 3)
-    # against the greedy fixed width 2, trained on passes recorded at all three widths.
-    model128 = _core.CostModel(seed=args.seed + 1)
-    t0 = time.perf_counter()
-    for fw in (1, 2, 3):
-        rec = dqsim.StatevectorSimulator(seed=1, precision="complex128", execution="tiled", fusion_width=fw,
-                                         max_memory_mb=1 << 20)
-        for n in (22, 24, 26):
-            model128.record(rec, dqsim.workloads.brickwork(n, 20, seed=3000 + 10 * n + fw, measure=False))
-            model128.record(rec, dqsim.workloads.qft(n, seed=4000 + n + fw))
-    record128_s = time.perf_counter() - t0
-    samples128 = model128.num_samples
-    mse128 = model128.train(epochs=60, lr=2e-3)
-    results128 = []
-    for n in (26, 30):
-        for kind, circuit in (("brickwork-d40", dqsim.workloads.brickwork(n, 40, seed=9100 + n, measure=False)),
-                              ("qft", dqsim.workloads.qft(n, seed=9200 + n))):
-            sim = dqsim.StatevectorSimulator(seed=1, execution="tiled", max_memory_mb=1 << 20)
-            _core.set_cost_model(sim, model128)
-            learned = _core.PreparedCircuit(sim, circuit)
-            info = learned.planner()
-            log = _core.planner_log(sim)[-1]
-            greedy = _core.PreparedCircuit(dqsim.StatevectorSimulator(seed=1, execution="tiled",
-                                                                      max_memory_mb=1 << 20), circuit)
-            tl = min(learned.run() for _ in range(2))
-            tg = min(greedy.run() for _ in range(2))
-            fid, err = learned.compare(greedy)
-            widths = log.get("widths") or []
-            results128.append({"circuit": kind, "qubits": n, "greedy_ms": tg, "kept_ms": tl,
-                               "ab_greedy_ms": info["greedy_ms"], "ab_learned_ms": info["learned_ms"],
-                               "rejected": info["rejected"], "gain": tg / tl,
-                               "widths_chosen": {str(w): widths.count(w) for w in sorted(set(widths))},
-                               "fidelity_vs_greedy": fid, "max_amp_err_vs_greedy": err})
-            _core.set_cost_model(sim, None)
-            del learned, greedy
-    print(json.dumps({"workload": "learned-vs-greedy", "samples": samples, "record_s": record_s,
-                      "train_mse": mse, "results": results,
-                      "rejection_rate": sum(r["rejected"] for r in results) / len(results),
-                      "complex128_tiles": {"samples": samples128, "record_s": record128_s, "train_mse": mse128,
-                                           "results": results128,
-                                           "rejection_rate": sum(r["rejected"] for r in results128) / len(results128)}}))
+    print(json.dumps({"workload": "learned-fused-planner-vs-hand-rule", "samples": int(len(rows["ms"])),
+                      "record_s": record_s, "train_s": train_s, "train_mse": mse, "results": results,
+                      "rejection_rate": sum(r["rejected"] for r in results) / len(results)}))
     return 0
 
 

@@ -514,6 +514,19 @@ int dq_fused_portfolio(dq_sim* sim, const char* json, size_t len, int wide, int 
     });
 }
 
+int dq_fused_pass_features(int num_qubits, const int* tile_qubits, int nblocks, int gates, float* out) {
+    return guard([&] {
+        need(tile_qubits, "tile_qubits");
+        need(out, "out");
+        if (num_qubits < kFusedM || num_qubits > 63) fail(kValueError, "num_qubits must be between 12 and 63");
+        std::vector<int> tq(tile_qubits, tile_qubits + kFusedM);
+        for (size_t i = 0; i < tq.size(); i++)
+            if (tq[i] < 0 || tq[i] >= num_qubits || (i && tq[i] <= tq[i - 1]))
+                fail(kValueError, "tile qubits must be 12 ascending qubits of the state");
+        fused_pass_features(num_qubits, 1, tq, nblocks, gates, out);
+    });
+}
+
 int dq_fused_random_passes(dq_sim* sim, int num_qubits, uint64_t count, uint64_t seed, int measure, char** out_text) {
     return guard([&] {
         need(sim, "sim");
@@ -661,6 +674,27 @@ int dq_sim_planner_log(dq_sim* sim, char** out_text) {
         if (!buf) throw std::bad_alloc();
         std::memcpy(buf, s.c_str(), s.size() + 1);
         *out_text = buf;
+    });
+}
+
+int dq_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
+    return guard([&] {
+        need(free_bytes, "free_bytes");
+        need(total_bytes, "total_bytes");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+            cudaGetLastError();
+            fail(kValueError, "CUDA device ordinal out of range");
+        }
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        size_t f = 0, tot = 0;
+        const cudaError_t e = cudaMemGetInfo(&f, &tot);
+        cudaSetDevice(prev);
+        cuda_check(e, "cudaMemGetInfo");
+        *free_bytes = f;
+        *total_bytes = tot;
     });
 }
 

@@ -17,6 +17,7 @@
 #include <random>
 
 #include "cost.hpp"
+#include "engine.hpp"
 
 namespace dq {
 namespace {
@@ -149,10 +150,11 @@ std::string fused_portfolio_json(Simulator& sim, const char* json, size_t len, b
 
 std::string fused_random_passes_json(Simulator& sim, int n, uint64_t count, uint64_t seed, bool measure) {
     if (n < kFusedM + 2 || n > 34) fail(kValueError, "random fused passes take 14 to 34 qubits");
-    if (count == 0) fail(kValueError, "count must be positive");
-    std::mt19937_64 rng(seed);
+    if (count == 0 || count > 4096) fail(kValueError, "count must be between 1 and 4096");
     std::vector<BuiltFusedPass> passes(static_cast<size_t>(count));
-    for (uint64_t c = 0; c < count; c++) {
+    // Each pass draws from its own stream (seed, index), so passes build on pooled workers.
+    parallel_for(passes.size(), [&](size_t c) {
+        std::mt19937_64 rng(seed * 0x9E3779B97F4A7C15ull + uint64_t(c));
         // Tile qubits: 0 and 1, then ten more drawn by one of four shapes.
         std::vector<int> pool;
         for (int q = kFusedPinned; q < n; q++) pool.push_back(q);
@@ -176,7 +178,7 @@ std::string fused_random_passes_json(Simulator& sim, int n, uint64_t count, uint
             }
         }
         std::sort(T.begin(), T.end());
-        // Gates: 1..10 clusters of up to 12 one- and two-qubit gates on five tile qubits each.
+        // Gates: 1..10 clusters of 4..12 one- and two-qubit gates on five tile qubits each.
         const int clusters = 1 + int(rng() % 10);
         std::vector<Operation> ops;
         for (int b = 0; b < clusters; b++) {
@@ -192,19 +194,19 @@ std::string fused_random_passes_json(Simulator& sim, int n, uint64_t count, uint
                     op.m = random_u3(rng);
                 } else {
                     const int a = five[rng() % 5];
-                    int t = five[rng() % 5];
-                    while (t == a) t = five[rng() % 5];
+                    int tq = five[rng() % 5];
+                    while (tq == a) tq = five[rng() % 5];
                     op.type = Operation::X;
-                    op.target = uint64_t(t);
+                    op.target = uint64_t(tq);
                     op.controls.push_back({uint64_t(a), true});
                 }
                 ops.push_back(op);
             }
         }
-        BuiltFusedPass& bp = passes[size_t(c)];
+        BuiltFusedPass& bp = passes[c];
         bp.src.qubits = T;
         bp.fp = build_fused_pass(ops, T, bp.blocks, bp.upool);
-    }
+    });
     std::vector<double> ms(passes.size(), -1.0);
     if (measure) {
         PassTimer timer(sim, n);

@@ -714,6 +714,19 @@ def fused_random_passes(simulator, num_qubits, count, seed=0, measure=True):
     return _json.loads(_take_text(out))
 
 
+_fused_features = _sig("dq_fused_pass_features", [ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, _P])
+
+
+def fused_pass_features(num_qubits, tile_qubits, blocks, gates):
+    """The fused-pass cost model's features of one pass (dq_fused_pass_features)."""
+    tq = np.ascontiguousarray(np.asarray(tile_qubits, dtype=np.int32).reshape(-1))
+    if tq.shape[0] != 12:
+        raise ValueError("a fused pass has 12 tile qubits")
+    out = np.empty(MLP_FEATURES, dtype=np.float32)
+    _check(_fused_features(int(num_qubits), tq.ctypes.data_as(_P), int(blocks), int(gates), out.ctypes.data_as(_P)))
+    return out
+
+
 def fused_pass_targets(passes, num_qubits):
     """Training targets of the fused-pass model: log of each pass's device nanoseconds per tile."""
     tiles = float(1 << (int(num_qubits) - 12))
@@ -745,6 +758,16 @@ def last_call_phases(simulator):
     out = np.zeros(len(CALL_PHASES), dtype=np.float64)
     _check(_sim_phases(simulator._h, out.ctypes.data, len(CALL_PHASES)))
     return dict(zip(CALL_PHASES, out.tolist()))
+
+
+_device_memory = _sig("dq_device_memory", [ctypes.c_int, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+
+
+def device_memory(device=0):
+    """Free and total bytes of a CUDA device (dq_device_memory)."""
+    f, t = _u64(), _u64()
+    _check(_device_memory(int(device), ctypes.byref(f), ctypes.byref(t)))
+    return {"free": f.value, "total": t.value}
 
 
 def device_fp64_tflops(device=0):

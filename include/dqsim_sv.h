@@ -248,7 +248,11 @@ DQ_API int dq_sim_set_cost_model(dq_sim* sim, dq_cost_model* m);
  * plans the learned planner's wider set of caps.  Free with dq_string_free. */
 DQ_API int dq_fused_portfolio(dq_sim* sim, const char* json, size_t json_len, int wide, int measure,
                               const dq_cost_model* model, char** out_text);
-/* `count` seeded random fused passes over num_qubits qubits (14..34): random
+/* The DQ_COST_FUSED_PASSES features (DQ_MLP_FEATURES floats) of a fused
+ * pass: its 12 ascending tile qubits over one state of num_qubits qubits, its
+ * block count and the gates fused into its blocks.  Host-only. */
+DQ_API int dq_fused_pass_features(int num_qubits, const int* tile_qubits, int nblocks, int gates, float* out);
+/* `count` (1..4096) seeded random fused passes over num_qubits qubits (14..34): random
  * tile qubits (qubits 0 and 1 plus ten drawn uniformly, low- or high-weighted,
  * or as one window) and 1..10 clusters of random one- and two-qubit gates,
  * with features and, with measure != 0, device milliseconds, as JSON text.
@@ -267,6 +271,11 @@ DQ_API int dq_plan_flops(const dq_plan* p, double* cuda_core_flops, double* tens
 DQ_API int dq_plan_shape(const dq_plan* p, uint64_t* passes, uint64_t* tile_ops, uint64_t* fused_blocks);
 /* Planner decisions of a simulator, one JSON object per line; free with dq_string_free. */
 DQ_API int dq_sim_planner_log(dq_sim* sim, char** out_text);
+
+/* Free and total memory of CUDA device `device`, in bytes (cudaMemGetInfo).
+ * No counterpart in the reference; the device backends' resource preflight
+ * (ml/circuit.py:201-217 checks host memory for complex128 states) reads it. */
+DQ_API int dq_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
 
 /* FP64 fused multiply-add throughput of CUDA device `device` in TFLOP/s,
  * measured by a kernel of this library (eight independent FMA chains per
