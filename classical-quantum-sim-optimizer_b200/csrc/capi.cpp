@@ -7,6 +7,7 @@
 
 #include "../../include/dqsim_sv.h"
 #include "batch.hpp"
+#include "blocks.hpp"
 #include "cost.hpp"
 #include "plan.hpp"
 #include "portfolio.hpp"
@@ -28,6 +29,9 @@ struct dq_batch {
 };
 struct dq_cost_model {
     std::unique_ptr<CostModel> impl;
+};
+struct dq_blocks {
+    std::unique_ptr<BlockContext> impl;
 };
 
 struct dq_sim {
@@ -718,6 +722,97 @@ int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_
                        int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes) {
     return guard([&] {
         measure_noalloc(states, precision, num_states, num_qubits, qubit, reset, seeds, draw_index, outcomes);
+    });
+}
+
+int dq_blocks_create(int device, int precision, dq_blocks** out) {
+    return guard([&] {
+        need(out, "out");
+        if (precision != DQ_COMPLEX128 && precision != DQ_COMPLEX64)
+            fail(kValueError, "precision must be DQ_COMPLEX128 or DQ_COMPLEX64");
+        auto b = std::make_unique<dq_blocks>();
+        b->impl = std::make_unique<BlockContext>(device, precision == DQ_COMPLEX64);
+        *out = b.release();
+    });
+}
+
+void dq_blocks_destroy(dq_blocks* ctx) { delete ctx; }
+
+int dq_blocks_sync(dq_blocks* ctx) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->sync();
+    });
+}
+
+int dq_block_apply_one_qubit(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t target, const double* matrix,
+                             const uint64_t* ctl_qubits, const uint8_t* ctl_values, size_t num_controls) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->apply_one_qubit(state, num_qubits, target, matrix, ctl_qubits, ctl_values, num_controls, false);
+    });
+}
+
+int dq_block_apply_x(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t target, const uint64_t* ctl_qubits,
+                     const uint8_t* ctl_values, size_t num_controls) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->apply_one_qubit(state, num_qubits, target, nullptr, ctl_qubits, ctl_values, num_controls, true);
+    });
+}
+
+int dq_block_apply_swap(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t a, uint64_t b,
+                        const uint64_t* ctl_qubits, const uint8_t* ctl_values, size_t num_controls) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->apply_swap(state, num_qubits, a, b, ctl_qubits, ctl_values, num_controls);
+    });
+}
+
+int dq_block_apply_diagonal(dq_blocks* ctx, void* state, uint64_t num_qubits, const uint64_t* qubits, size_t k,
+                            const double* diagonal) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->apply_diagonal(state, num_qubits, qubits, k, diagonal);
+    });
+}
+
+int dq_block_apply_dense(dq_blocks* ctx, void* state, uint64_t num_qubits, const uint64_t* qubits, size_t k,
+                         const double* matrix) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->apply_dense(state, num_qubits, qubits, k, matrix);
+    });
+}
+
+int dq_block_measure(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t qubit, double draw, int* outcome) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(outcome, "outcome");
+        *outcome = ctx->impl->measure(state, num_qubits, qubit, draw);
+    });
+}
+
+int dq_block_merge(dq_blocks* ctx, const void* left, uint64_t left_qubits, const void* right, uint64_t right_qubits,
+                   void* out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->merge(left, left_qubits, right, right_qubits, out);
+    });
+}
+
+int dq_block_probabilities(dq_blocks* ctx, const void* state, uint64_t num_qubits, const uint64_t* qubits, size_t k,
+                           double* out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->probabilities(state, num_qubits, qubits, k, out);
+    });
+}
+
+int dq_block_running_sums(dq_blocks* ctx, const void* state, uint64_t num_qubits, double* out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        ctx->impl->running_sums(state, num_qubits, out);
     });
 }
 

@@ -734,6 +734,49 @@ void measure_t(const Batch& b, int qubit, int64_t cbit, bool reset, const CondLi
     check_launch("collapse");
 }
 
+template <typename V>
+void measure_draw_t(const Batch& b, int qubit, double draw, int* outcome_host) {
+    const int pbits = std::max(0, std::min(10, b.n - 12));
+    const int P = 1 << pbits;
+    k_prob2<V><<<P, kThreads, 0, b.stream>>>(static_cast<const V*>(b.amps), b.n, b.n - pbits, P, uint64_t(1) << qubit,
+                                            b.partial, CondList{}, b.cbits, b.cwords);
+    check_launch("prob2");
+    std::vector<double> part(size_t(P) * 2);
+    cudaError_t e = cudaMemcpyAsync(part.data(), b.partial, part.size() * 8, cudaMemcpyDeviceToHost, b.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
+    if (e != cudaSuccess) fail(kCudaError, std::string("branch sums: ") + cudaGetErrorString(e));
+    // The branch sums in the order k_measure_finalize adds them.
+    double p0 = 0.0, p1 = 0.0;
+    for (int c = 0; c < P; c++) {
+        p0 += part[size_t(c) * 2];
+        p1 += part[size_t(c) * 2 + 1];
+    }
+    const double total = p0 + p1;
+    if (!(std::isfinite(total) && total > 0.0)) fail(kRuntimeError, "Cannot measure a state with nonfinite or zero norm");
+    const int o = draw < p1 / total ? 1 : 0;  // engine.rs:405
+    const double scale = 1.0 / std::sqrt(o ? p1 : p0);
+    e = cudaMemcpyAsync(b.outcome, &o, sizeof(int), cudaMemcpyHostToDevice, b.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.scale, &scale, sizeof(double), cudaMemcpyHostToDevice, b.stream);
+    if (e != cudaSuccess) fail(kCudaError, std::string("measurement upload: ") + cudaGetErrorString(e));
+    const uint64_t items = uint64_t(1) << (b.n - 1);
+    k_collapse<V><<<blocks_for(items, kThreads * kIPT), kThreads, 0, b.stream>>>(static_cast<V*>(b.amps), b.n, items,
+                                                                                  qubit, b.outcome, b.scale, 0);
+    check_launch("collapse");
+    // The host values above must not change before the copies read them.
+    e = cudaStreamSynchronize(b.stream);
+    if (e != cudaSuccess) fail(kCudaError, std::string("collapse: ") + cudaGetErrorString(e));
+    *outcome_host = o;
+}
+
+// out[i * 2^nl + j] = left[j] * right[i]: the state of the merged block whose
+// low nl qubits are the left block's (src/distributed/pblock/model.rs:216-230).
+template <typename V>
+__global__ void k_kron(const V* __restrict__ left, int nl, const V* __restrict__ right, uint64_t len,
+                       V* __restrict__ out) {
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x)
+        out[g] = dev::cmul(left[g & ((uint64_t(1) << nl) - 1)], right[g >> nl]);
+}
+
 unsigned stream_grid(uint64_t len) {
     uint64_t b = (len + 255) / 256;
     return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(b, 148 * 32)));
@@ -775,6 +818,26 @@ void measure(const Batch& b, int qubit, int64_t cbit, bool reset, const CondList
         measure_t<float2>(b, qubit, cbit, reset, cond);
     else
         measure_t<double2>(b, qubit, cbit, reset, cond);
+}
+
+void measure_draw(const Batch& b, int qubit, double draw, int* outcome) {
+    if (b.W != 1) fail(kValueError, "a measurement with a given draw takes one state");
+    if (b.c64)
+        measure_draw_t<float2>(b, qubit, draw, outcome);
+    else
+        measure_draw_t<double2>(b, qubit, draw, outcome);
+}
+
+void kron(cudaStream_t s, bool c64, const void* left, int nl, const void* right, int nr, void* out) {
+    const uint64_t len = uint64_t(1) << (nl + nr);
+    if (c64)
+        k_kron<float2><<<stream_grid(len), 256, 0, s>>>(static_cast<const float2*>(left), nl,
+                                                         static_cast<const float2*>(right), len, static_cast<float2*>(out));
+    else
+        k_kron<double2><<<stream_grid(len), 256, 0, s>>>(static_cast<const double2*>(left), nl,
+                                                          static_cast<const double2*>(right), len,
+                                                          static_cast<double2*>(out));
+    check_launch("kron");
 }
 
 void init_basis(const Batch& b) {

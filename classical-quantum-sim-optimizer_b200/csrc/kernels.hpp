@@ -61,6 +61,13 @@ void dense(const Batch& b, const std::vector<int>& qubits, const double2* dmatri
 // sums, a ChaCha8 draw per state, collapse (engine.rs:367-426).  cbit < 0: no write.
 void measure(const Batch& b, int qubit, int64_t cbit, bool reset, const dev::CondList& cond);
 
+// Measure one qubit of one state with a draw the caller supplies (uniform in
+// [0, 1)): branch sums, outcome = draw < p1 / (p0 + p1), collapse; the outcome
+// is returned to the host (the stream is synchronised).  engine.rs:367-426.
+void measure_draw(const Batch& b, int qubit, double draw, int* outcome);
+// out[i * 2^nl + j] = left[j] * right[i] (the merged block of two blocks).
+void kron(cudaStream_t s, bool c64, const void* left, int nl, const void* right, int nr, void* out);
+
 // Set each state to |0...0>.
 void init_basis(const Batch& b);
 // Copy one state into all W states of the batch.

@@ -770,6 +770,95 @@ def device_memory(device=0):
     return {"free": f.value, "total": t.value}
 
 
+_U8P = ctypes.POINTER(ctypes.c_uint8)
+_blocks_create = _sig("dq_blocks_create", [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)])
+_blocks_destroy = _sig("dq_blocks_destroy", [_P], None)
+_blocks_sync = _sig("dq_blocks_sync", [_P])
+_block_one = _sig("dq_block_apply_one_qubit", [_P, _P, _u64, _u64, _P, _P, _P, ctypes.c_size_t])
+_block_x = _sig("dq_block_apply_x", [_P, _P, _u64, _u64, _P, _P, ctypes.c_size_t])
+_block_swap = _sig("dq_block_apply_swap", [_P, _P, _u64, _u64, _u64, _P, _P, ctypes.c_size_t])
+_block_diag = _sig("dq_block_apply_diagonal", [_P, _P, _u64, _P, ctypes.c_size_t, _P])
+_block_dense = _sig("dq_block_apply_dense", [_P, _P, _u64, _P, ctypes.c_size_t, _P])
+_block_measure = _sig("dq_block_measure", [_P, _P, _u64, _u64, ctypes.c_double, ctypes.POINTER(ctypes.c_int)])
+_block_merge = _sig("dq_block_merge", [_P, _P, _u64, _P, _u64, _P])
+_block_probs = _sig("dq_block_probabilities", [_P, _P, _u64, _P, ctypes.c_size_t, _P])
+_block_sums = _sig("dq_block_running_sums", [_P, _P, _u64, _P])
+
+
+def _ptr_arg(p):
+    return ctypes.c_void_p(int(p))
+
+
+class BlockContext:
+    """Dense P-block blocks on the device (dq_blocks_* / dq_block_*).
+
+    Blocks are device buffers the caller owns (e.g. CUDA tensors' data_ptr()), of 2^n complex128 or complex64
+    amplitudes little-endian in the block's local qubits; calls run in order on the context's stream.
+    """
+
+    def __init__(self, device=0, precision="complex128"):
+        prec = PRECISIONS[str(precision).lower()]
+        h = _P()
+        _check(_blocks_create(int(device), prec, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _blocks_destroy(h)
+            self._h = None
+
+    @staticmethod
+    def _controls(controls):
+        q = np.ascontiguousarray([c[0] for c in controls], dtype=np.uint64)
+        v = np.ascontiguousarray([1 if c[1] else 0 for c in controls], dtype=np.uint8)
+        return q, v
+
+    def apply_one_qubit(self, state, n, target, matrix, controls=()):
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(4))
+        q, v = self._controls(controls)
+        _check(_block_one(self._h, _ptr_arg(state), n, target, m.ctypes.data_as(_P), q.ctypes.data_as(_P),
+                          v.ctypes.data_as(_P), len(controls)))
+
+    def apply_x(self, state, n, target, controls=()):
+        q, v = self._controls(controls)
+        _check(_block_x(self._h, _ptr_arg(state), n, target, q.ctypes.data_as(_P), v.ctypes.data_as(_P),
+                        len(controls)))
+
+    def apply_swap(self, state, n, a, b, controls=()):
+        q, v = self._controls(controls)
+        _check(_block_swap(self._h, _ptr_arg(state), n, a, b, q.ctypes.data_as(_P), v.ctypes.data_as(_P),
+                           len(controls)))
+
+    def apply_diagonal(self, state, n, qubits, diagonal):
+        q = np.ascontiguousarray(qubits, dtype=np.uint64)
+        d = np.ascontiguousarray(np.asarray(diagonal, dtype=np.complex128).reshape(-1))
+        _check(_block_diag(self._h, _ptr_arg(state), n, q.ctypes.data_as(_P), q.shape[0], d.ctypes.data_as(_P)))
+
+    def apply_dense(self, state, n, qubits, matrix):
+        q = np.ascontiguousarray(qubits, dtype=np.uint64)
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(-1))
+        _check(_block_dense(self._h, _ptr_arg(state), n, q.ctypes.data_as(_P), q.shape[0], m.ctypes.data_as(_P)))
+
+    def measure(self, state, n, qubit, draw):
+        out = ctypes.c_int()
+        _check(_block_measure(self._h, _ptr_arg(state), n, qubit, float(draw), ctypes.byref(out)))
+        return out.value
+
+    def merge(self, left, left_qubits, right, right_qubits, out):
+        _check(_block_merge(self._h, _ptr_arg(left), left_qubits, _ptr_arg(right), right_qubits, _ptr_arg(out)))
+
+    def probabilities(self, state, n, qubits, out):
+        q = np.ascontiguousarray(list(qubits or []), dtype=np.uint64)
+        _check(_block_probs(self._h, _ptr_arg(state), n, q.ctypes.data_as(_P), q.shape[0], _ptr_arg(out)))
+
+    def running_sums(self, state, n, out):
+        _check(_block_sums(self._h, _ptr_arg(state), n, _ptr_arg(out)))
+
+    def sync(self):
+        _check(_blocks_sync(self._h))
+
+
 def device_fp64_tflops(device=0):
     """FP64 FMA throughput of a device in TFLOP/s, measured by the library's own kernel."""
     out = ctypes.c_double()

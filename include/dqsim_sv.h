@@ -322,6 +322,54 @@ DQ_API int dq_sim_last_call_phases(dq_sim* sim, double* out, uint64_t n);
 DQ_API int dq_measure_noalloc(void* states, int precision, uint64_t num_states, uint64_t num_qubits, uint64_t qubit,
                               int reset, const uint64_t* seeds, const uint64_t* draw_index, int* outcomes);
 
+/* Dense blocks of the P-block backend on the device.  The reference's
+ * P-block model (src/distributed/pblock/model.rs) holds the state as
+ * independent dense blocks and runs every gate, merge and measurement on one
+ * block with the src/engine.rs kernels; these entry points are the calls it
+ * makes, on blocks the caller keeps in device memory (2^num_qubits complex128
+ * or complex64 amplitudes by the context's precision, little-endian in the
+ * block's local qubits, qubits[0] the MSB of a matrix or probability index).
+ * A context owns a stream: its calls run in order on it, asynchronously except
+ * dq_block_measure (which returns the outcome) and dq_blocks_sync; the block
+ * bookkeeping (which qubits a block holds, when to merge) stays with the
+ * caller, as in model.rs. */
+typedef struct dq_blocks dq_blocks;
+DQ_API int dq_blocks_create(int device, int precision, dq_blocks** out);
+DQ_API void dq_blocks_destroy(dq_blocks* ctx);
+DQ_API int dq_blocks_sync(dq_blocks* ctx);
+/* engine::apply_one_qubit (model.rs:322-324): matrix is 2x2 row-major complex
+ * as 8 doubles (re, im); controls are (qubit, value) pairs. */
+DQ_API int dq_block_apply_one_qubit(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t target,
+                                    const double* matrix, const uint64_t* ctl_qubits, const uint8_t* ctl_values,
+                                    size_t num_controls);
+/* engine::apply_x (model.rs:320). */
+DQ_API int dq_block_apply_x(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t target,
+                            const uint64_t* ctl_qubits, const uint8_t* ctl_values, size_t num_controls);
+/* engine::apply_swap (model.rs:370). */
+DQ_API int dq_block_apply_swap(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t a, uint64_t b,
+                               const uint64_t* ctl_qubits, const uint8_t* ctl_values, size_t num_controls);
+/* engine::apply_diagonal (model.rs:415): k <= 5 qubits, 2^k complex entries as doubles. */
+DQ_API int dq_block_apply_diagonal(dq_blocks* ctx, void* state, uint64_t num_qubits, const uint64_t* qubits, size_t k,
+                                   const double* diagonal);
+/* engine::DenseLayout::apply (model.rs:429): k <= 5 qubits, row-major 2^k x 2^k complex. */
+DQ_API int dq_block_apply_dense(dq_blocks* ctx, void* state, uint64_t num_qubits, const uint64_t* qubits, size_t k,
+                                const double* matrix);
+/* engine::measure_qubit (model.rs:484-486) with the caller's draw in [0, 1):
+ * outcome = draw < p1 / (p0 + p1), the block collapsed and renormalised. */
+DQ_API int dq_block_measure(dq_blocks* ctx, void* state, uint64_t num_qubits, uint64_t qubit, double draw,
+                            int* outcome);
+/* The merge of two blocks (model.rs:199-248): out[i * 2^left_qubits + j] =
+ * left[j] * right[i], the left block's qubits becoming the low ones. */
+DQ_API int dq_block_merge(dq_blocks* ctx, const void* left, uint64_t left_qubits, const void* right,
+                          uint64_t right_qubits, void* out);
+/* engine::marginal_probs over `qubits` (k = 0: every amplitude's |a|^2) into
+ * device memory `out` (2^k doubles). */
+DQ_API int dq_block_probabilities(dq_blocks* ctx, const void* state, uint64_t num_qubits, const uint64_t* qubits,
+                                  size_t k, double* out);
+/* The running sums of a block's squared magnitudes that P-block sampling
+ * draws from (model.rs:583-608), into device memory `out` (2^num_qubits doubles). */
+DQ_API int dq_block_running_sums(dq_blocks* ctx, const void* state, uint64_t num_qubits, double* out);
+
 /* Host-only helpers (no device work): parse, validate and compile a circuit
  * exactly as read_circuit + compile do (simulator.rs:204-211,
  * execution.rs:368-416), returning the operation list as JSON text with
