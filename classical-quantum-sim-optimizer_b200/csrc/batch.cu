@@ -13,6 +13,8 @@ namespace dq {
 namespace {
 
 constexpr int kBatchThreads = 256;
+// Side streams the fused circuits of a batch run on.
+constexpr size_t kSideStreams = 16;
 // Spin limit of one dependency wait: 2^24 polls of >= 256 ns, several seconds.
 constexpr uint64_t kMaxSpins = uint64_t(1) << 24;
 
@@ -324,20 +326,35 @@ BatchRun::BatchRun(Simulator& sim, const std::vector<std::string>& texts, uint64
         for (auto& kv : mapping) c.cbit_map.emplace_back(kv.first, kv.second);
         c.tile_m = tuning.tile_m > 0 ? tuning.tile_m : (c64_ ? 13 : 12);
         c.fuse = tuning.fuse > 0 ? tuning.fuse : 2;
+        c.depth = tuning.depth;
         auto tuned = tuning.per_n.find(c.n);
-        if (tuning.tile_m <= 0 && tuned != tuning.per_n.end()) {
-            c.tile_m = tuned->second.first;
-            c.fuse = tuned->second.second;
+        if (tuning.tile_m <= 0 && tuning.fuse <= 0 && tuned != tuning.per_n.end()) {
+            c.tile_m = tuned->second.tile_m;
+            c.fuse = tuned->second.fuse;
+            c.depth = tuned->second.depth;
         }
-        TilePlanOptions po;
-        po.m = c.tile_m;
-        po.fuse = std::min(c.fuse, kTileMaxDense);
-        po.c64 = c64_;
-        std::vector<TilePass> passes = plan_tiles(ops, 0, prefix, int(c.n), po, &pool_host_);
-        for (auto& p : passes) {
-            p.op_begin = int(ops_host_.size());
-            ops_host_.insert(ops_host_.end(), p.ops.begin(), p.ops.end());
-            max_m_ = std::max(max_m_, int(p.qubits.size()));
+        std::vector<TilePass> passes;
+        if (c.fuse == 5 && c64_ && c.n >= uint64_t(kFusedM)) {
+            // Tensor-core fused passes, run by an executor of their own on a side stream.
+            ExecConfig cfg;
+            cfg.tiled = true;
+            cfg.fused = true;
+            cfg.c64 = true;
+            cfg.n = int(c.n);
+            c.fused = std::make_unique<Executor>(ops, 0, prefix, cfg);
+        } else {
+            if (c.fuse == 5) c.fuse = 2;  // no tensor-core form below 12 qubits or in complex128
+            TilePlanOptions po;
+            po.m = c.tile_m;
+            po.fuse = std::min(c.fuse, kTileMaxDense);
+            po.c64 = c64_;
+            po.max_pass_ops = c.depth;
+            passes = plan_tiles(ops, 0, prefix, int(c.n), po, &pool_host_);
+            for (auto& p : passes) {
+                p.op_begin = int(ops_host_.size());
+                ops_host_.insert(ops_host_.end(), p.ops.begin(), p.ops.end());
+                max_m_ = std::max(max_m_, int(p.qubits.size()));
+            }
         }
         c.state_off = off;
         off += uint64_t(1) << c.n;
@@ -369,10 +386,12 @@ BatchRun::BatchRun(Simulator& sim, const std::vector<std::string>& texts, uint64
             for (int i = 0; i < r.m; i++) r.q[i] = tp.qubits[i];
             pass_recs_.push_back(r);
             item += tiles;
+            tile_bytes_ += 2.0 * (c64_ ? 8.0 : 16.0) * double(uint64_t(1) << r.n);
         }
     }
     total_items_ = item;
     if (max_m_ > 14) fail(kValueError, "tile too large");
+    if (max_m_ == 0) max_m_ = 5;  // every circuit runs fused passes: the persistent kernel gets no items
 
     dev_ = sim.ensure_device();
     std::lock_guard<std::mutex> lk(dev_->mu);
@@ -407,6 +426,33 @@ BatchRun::BatchRun(Simulator& sim, const std::vector<std::string>& texts, uint64
                "upload");
     cuda_check(cudaMemcpyAsync(circ_off_.p, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, s), "upload");
     cuda_check(cudaMemcpyAsync(seeds_.p, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, s), "upload");
+    // Fused circuits: executors prepared (pools uploaded, scratch sized) so that
+    // runs allocate nothing and can be captured; longest first onto the least
+    // loaded side stream.
+    std::vector<size_t> order;
+    for (size_t ci = 0; ci < circuits_.size(); ci++)
+        if (circuits_[ci].fused) order.push_back(ci);
+    auto cost = [&](size_t ci) {
+        return double(uint64_t(1) << circuits_[ci].n) * double(circuits_[ci].fused->fused_blocks() + 3);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+    if (!order.empty()) {
+        const size_t nside = std::min<size_t>(kSideStreams, order.size());
+        std::vector<double> load(nside, 0.0);
+        for (size_t ci : order) {
+            const size_t j = size_t(std::min_element(load.begin(), load.end()) - load.begin());
+            circuits_[ci].stream = int(j);
+            load[j] += cost(ci);
+        }
+        side_.resize(nside, nullptr);
+        join_.resize(nside, nullptr);
+        for (size_t j = 0; j < nside; j++) {
+            cuda_check(cudaStreamCreateWithFlags(&side_[j], cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaEventCreateWithFlags(&join_[j], cudaEventDisableTiming), "cudaEventCreate");
+        }
+        cuda_check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+        for (size_t ci : order) circuits_[ci].fused->prepare(circuit_view(circuits_[ci], s));
+    }
     const size_t smem = (S << max_m_);
     // Largest carveout: the occupancy query that sizes the persistent grid must
     // match what the launch gets, since every CTA has to be resident at once.
@@ -428,6 +474,75 @@ BatchRun::BatchRun(Simulator& sim, const std::vector<std::string>& texts, uint64
 
 BatchRun::~BatchRun() {
     if (graph_) cudaGraphExecDestroy(graph_);
+    if (dev_) {
+        dev_->activate();
+        for (cudaStream_t st : side_) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        for (cudaEvent_t e : join_) cudaEventDestroy(e);
+        if (fork_) cudaEventDestroy(fork_);
+    }
+}
+
+k::Batch BatchRun::circuit_view(const Circ& c, cudaStream_t s) const {
+    k::Batch b;
+    b.stream = s;
+    b.c64 = c64_;
+    b.amps = static_cast<unsigned char*>(amps_.p) + c.state_off * (c64_ ? 8 : 16);
+    b.n = int(c.n);
+    b.W = 1;
+    b.err = err_.as<int>();
+    return b;
+}
+
+size_t BatchRun::passes() const {
+    size_t total = pass_recs_.size();
+    for (const Circ& c : circuits_)
+        if (c.fused) total += c.fused->passes();
+    return total;
+}
+
+size_t BatchRun::fused_circuits() const {
+    size_t total = 0;
+    for (const Circ& c : circuits_) total += c.fused ? 1 : 0;
+    return total;
+}
+
+void BatchRun::work(double* bytes, double* tensor_flops, double* cuda_core_flops) const {
+    double by = tile_bytes_, tf = 0.0, cf = 0.0;
+    for (size_t i = 0; i < pass_recs_.size(); i++) {
+        const PassRec& r = pass_recs_[i];
+        double per_tile = 0.0;
+        for (int k = 0; k < r.nops; k++) {
+            const TileOp& op = ops_host_[size_t(r.op_begin + k)];
+            const double items = double(uint64_t(1) << (r.m - op.nins));
+            switch (op.type) {
+                case TileOp::kOne: per_tile += items * 28.0; break;
+                case TileOp::kDiagEntry: per_tile += items * 6.0; break;
+                case TileOp::kDiagFull: per_tile += double(uint64_t(1) << r.m) * 6.0; break;
+                case TileOp::kDense: {
+                    const double d = double(1 << op.k);
+                    per_tile += double(uint64_t(1) << (r.m - op.k)) * (d * d * 6.0 + (d * d - d) * 2.0);
+                    break;
+                }
+                default: break;
+            }
+        }
+        cf += per_tile * double(uint64_t(1) << (r.n - r.m));
+    }
+    for (const Circ& c : circuits_) {
+        if (!c.fused) continue;
+        const k::Batch b = circuit_view(c, nullptr);
+        double cc = 0.0, tc = 0.0;
+        c.fused->arith_flops(b, &cc, &tc);
+        cf += cc;
+        tf += tc;
+        by += double(c.fused->passes()) * 2.0 * 8.0 * double(uint64_t(1) << c.n);
+    }
+    *bytes = by;
+    *tensor_flops = tf;
+    *cuda_core_flops = cf;
 }
 
 void BatchRun::enqueue() {
@@ -443,6 +558,14 @@ void BatchRun::enqueue() {
         k_first_amp<float2><<<(count + 127) / 128, 128, 0, s>>>(amps_.as<float2>(), offs, count);
     else
         k_first_amp<double2><<<(count + 127) / 128, 128, 0, s>>>(amps_.as<double2>(), offs, count);
+    if (!side_.empty()) {
+        // Fused circuits on the side streams, beside the persistent kernel.
+        cuda_check(cudaEventRecord(fork_, s), "fork");
+        for (cudaStream_t st : side_) cuda_check(cudaStreamWaitEvent(st, fork_, 0), "fork");
+        for (const Circ& c : circuits_)
+            if (c.fused) c.fused->run(circuit_view(c, side_[size_t(c.stream)]), nullptr);
+        for (size_t j = 0; j < side_.size(); j++) cuda_check(cudaEventRecord(join_[j], side_[j]), "join");
+    }
     const size_t smem = (S << max_m_);
     int per_sm = 0;
     if (c64_)
@@ -465,6 +588,7 @@ void BatchRun::enqueue() {
                                                               head_.as<unsigned long long>(), total_items_,
                                                               err_.as<int>());
     }
+    for (cudaEvent_t e : join_) cuda_check(cudaStreamWaitEvent(s, e, 0), "join");
     const unsigned sgrid = unsigned(std::min<uint64_t>((total_amps_ + 255) / 256, 148 * 32));
     if (c64_)
         k_arena_norm2<float2><<<sgrid, 256, 0, s>>>(amps_.as<float2>(), probs_.as<double>(), total_amps_);
@@ -583,17 +707,34 @@ TuneResult autotune_tile(Simulator& sim, const std::string& json, bool c64) {
         auto it = cache.find({n, c64 ? 1 : 0});
         if (it != cache.end()) return it->second;
     }
-    TuneResult best{c64 ? 13 : 12, 2, 1e30};
+    auto time_shape = [&](int m, int fuse, int depth) {
+        BatchTuning t;
+        t.tile_m = m;
+        t.fuse = fuse;
+        t.depth = depth;
+        BatchRun run(sim, {json}, 0, t);
+        run.run(false);
+        double ms = 1e30;
+        for (int r = 0; r < 3; r++) ms = std::min(ms, run.run(false));
+        return ms;
+    };
+    TuneResult best{c64 ? 13 : 12, 2, 0, 1e30};
+    // Tile qubits and fusion width, passes as deep as they grow ...
     const int ms_max = c64 ? 14 : 13;
-    for (int m = std::max(5, std::min<int>(10, int(n))); m <= std::min<int>(ms_max, int(n)); m++) {
+    for (int m = std::max(5, std::min<int>(10, int(n))); m <= std::min<int>(ms_max, int(n)); m++)
         for (int fuse = 1; fuse <= 3; fuse++) {
-            BatchTuning t{m, fuse};
-            BatchRun run(sim, {json}, 0, t);
-            run.run(false);
-            double ms = 1e30;
-            for (int r = 0; r < 3; r++) ms = std::min(ms, run.run(false));
-            if (ms < best.ms) best = {m, fuse, ms};
+            const double ms = time_shape(m, fuse, 0);
+            if (ms < best.ms) best = {m, fuse, 0, ms};
         }
+    // ... then the shared-memory pass depth of the best shape ...
+    for (int depth : {12, 24, 48}) {
+        const double ms = time_shape(best.tile_m, best.fuse, depth);
+        if (ms < best.ms) best = {best.tile_m, best.fuse, depth, ms};
+    }
+    // ... and the tensor-core fused passes (complex64, 12 qubits or more).
+    if (c64 && n >= uint64_t(kFusedM)) {
+        const double ms = time_shape(kFusedM, 5, 0);
+        if (ms < best.ms) best = {kFusedM, 5, 0, ms};
     }
     std::lock_guard<std::mutex> lk(mu);
     cache[{n, c64 ? 1 : 0}] = best;

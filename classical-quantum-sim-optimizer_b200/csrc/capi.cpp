@@ -403,7 +403,9 @@ int dq_batch_create(dq_sim* sim, const char* const* jsons, const size_t* lens, u
             texts.emplace_back(jsons[i], lens[i]);
         }
         BatchTuning t;
-        if (autotune) {
+        if (autotune < 0 || autotune > 2) fail(kValueError, "autotune must be 0, 1 or 2");
+        if (autotune == 2) t.fuse = 5;  // tensor-core fused passes wherever they apply
+        if (autotune == 1) {
             const bool c64 = sim->impl->options().precision == Precision::C64;
             std::map<uint64_t, size_t> first;
             for (size_t i = 0; i < texts.size(); i++) {
@@ -413,7 +415,7 @@ int dq_batch_create(dq_sim* sim, const char* const* jsons, const size_t* lens, u
             }
             for (auto& kv : first) {
                 TuneResult r = autotune_tile(*sim->impl, texts[kv.second], c64);
-                t.per_n[kv.first] = {r.tile_m, r.fuse};
+                t.per_n[kv.first] = BatchShape{r.tile_m, r.fuse, r.depth};
             }
         }
         auto b = std::make_unique<dq_batch>();
@@ -472,6 +474,19 @@ int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items) {
         need(b, "batch");
         if (passes) *passes = b->impl->passes();
         if (items) *items = b->impl->items();
+    });
+}
+
+int dq_batch_work(const dq_batch* b, double* bytes, double* tensor_flops, double* cuda_core_flops,
+                  uint64_t* fused_circuits) {
+    return guard([&] {
+        need(b, "batch");
+        double by = 0, tf = 0, cf = 0;
+        b->impl->work(&by, &tf, &cf);
+        if (bytes) *bytes = by;
+        if (tensor_flops) *tensor_flops = tf;
+        if (cuda_core_flops) *cuda_core_flops = cf;
+        if (fused_circuits) *fused_circuits = b->impl->fused_circuits();
     });
 }
 

@@ -698,32 +698,44 @@ void Executor::lower(const Operation& op, std::vector<Condition>& conds) {
     steps_.push_back(std::move(s));
 }
 
-void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
-    if (!uploaded_) {
-        if (!pool_host_.empty()) {
-            pool_.alloc(pool_host_.size() * sizeof(double2), "gate matrices");
-            cuda_check(cudaMemcpyAsync(pool_.p, pool_host_.data(), pool_host_.size() * sizeof(double2),
-                                       cudaMemcpyHostToDevice, b.stream),
-                       "upload gate matrices");
-        }
-        if (!tile_ops_host_.empty()) {
-            tile_ops_.alloc(tile_ops_host_.size() * sizeof(TileOp), "tile operations");
-            cuda_check(cudaMemcpyAsync(tile_ops_.p, tile_ops_host_.data(), tile_ops_host_.size() * sizeof(TileOp),
-                                       cudaMemcpyHostToDevice, b.stream),
-                       "upload tile operations");
-        }
-        if (!fused_blocks_host_.empty()) {
-            fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
-            upool_.alloc(upool_host_.size() * sizeof(uint16_t), "fused block gate images");
-            cuda_check(cudaMemcpyAsync(fused_blocks_.p, fused_blocks_host_.data(),
-                                       fused_blocks_host_.size() * sizeof(FusedBlock), cudaMemcpyHostToDevice, b.stream),
-                       "upload fused blocks");
-            cuda_check(cudaMemcpyAsync(upool_.p, upool_host_.data(), upool_host_.size() * sizeof(uint16_t),
-                                       cudaMemcpyHostToDevice, b.stream),
-                       "upload gate images");
-        }
-        uploaded_ = true;
+void Executor::prepare(const k::Batch& b) {
+    if (!fused_.empty()) {
+        norm_tiles_.ensure((size_t(b.W) << (b.n - kFusedM)) * 8, "fused tile norms");
+        norm_states_.ensure(size_t(b.W) * size_t(k::fused_norm_parts(b.n)) * 8, "fused state norms");
+        k::fused_configure();
     }
+    upload(b.stream);
+}
+
+void Executor::upload(cudaStream_t stream) {
+    if (uploaded_) return;
+    if (!pool_host_.empty()) {
+        pool_.alloc(pool_host_.size() * sizeof(double2), "gate matrices");
+        cuda_check(cudaMemcpyAsync(pool_.p, pool_host_.data(), pool_host_.size() * sizeof(double2),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload gate matrices");
+    }
+    if (!tile_ops_host_.empty()) {
+        tile_ops_.alloc(tile_ops_host_.size() * sizeof(TileOp), "tile operations");
+        cuda_check(cudaMemcpyAsync(tile_ops_.p, tile_ops_host_.data(), tile_ops_host_.size() * sizeof(TileOp),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload tile operations");
+    }
+    if (!fused_blocks_host_.empty()) {
+        fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
+        upool_.alloc(upool_host_.size() * sizeof(uint16_t), "fused block gate images");
+        cuda_check(cudaMemcpyAsync(fused_blocks_.p, fused_blocks_host_.data(),
+                                   fused_blocks_host_.size() * sizeof(FusedBlock), cudaMemcpyHostToDevice, stream),
+                   "upload fused blocks");
+        cuda_check(cudaMemcpyAsync(upool_.p, upool_host_.data(), upool_host_.size() * sizeof(uint16_t),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload gate images");
+    }
+    uploaded_ = true;
+}
+
+void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
+    upload(b.stream);
     std::vector<uint64_t> host_cbits;
     bool norm_pending = false;  // a fused pass left a norm the next fused pass divides out
     for (size_t si = 0; si < steps_.size(); si++) {

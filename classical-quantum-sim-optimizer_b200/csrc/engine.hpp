@@ -149,6 +149,10 @@ class Executor {
     Executor(const std::vector<Operation>& ops, size_t begin, size_t end, const ExecConfig& cfg = ExecConfig());
     // Launch every step on the batch (asynchronously unless `profile`).
     void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr);
+    // Uploads the matrix pools and sizes the scratch a run over batches like
+    // `b` needs, so that later runs allocate nothing and copy nothing from the
+    // host (they can then be captured into a CUDA graph).
+    void prepare(const k::Batch& b);
     size_t steps() const { return steps_.size(); }
     // Algorithmic bytes one step moves for a batch (the roofline numerator).
     double step_bytes(size_t i, const k::Batch& b) const;
@@ -200,6 +204,7 @@ class Executor {
     ExecConfig cfg_;
     std::vector<int> widths_;
     std::vector<FusedPlanChoice> fused_choices_;
+    void upload(cudaStream_t stream);
     void lower(const Operation& op, std::vector<Condition>& conds);
     void lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end);
 };

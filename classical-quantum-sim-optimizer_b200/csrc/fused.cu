@@ -686,6 +686,22 @@ void set_fused_fault(uint64_t withhold_step, double wait_ms) {
     g_fault = f;
 }
 
+void fused_configure() {
+    static std::mutex mu;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!configured[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fused, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     int(cudaSharedmemCarveoutMaxShared));
+        if (e != cudaSuccess) fail(kCudaError, std::string("fused pass setup: ") + cudaGetErrorString(e));
+        configured[dev & 63] = true;
+    }
+}
+
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev, int* err,
                 const double* in_norm, double* tile_norm) {
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
@@ -705,17 +721,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     fq.tma = fused_tma_plan(p.qubits, b.n, b.W);
     fq.fault = g_fault;
     if (fq.tma.ok && !encode_tile_map(fq.tma, b.amps, b.W << b.n, &tile_map)) fq.tma.ok = 0;
-    static bool configured[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!configured[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fused, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     int(cudaSharedmemCarveoutMaxShared));
-        if (e != cudaSuccess) fail(kCudaError, std::string("fused pass setup: ") + cudaGetErrorString(e));
-        configured[dev & 63] = true;
-    }
+    fused_configure();
     // One CTA per SM, persistent over groups of kGroups tiles.
     const uint64_t total = b.W << (b.n - kFusedM);
     const uint64_t grid = std::min<uint64_t>((total + kGroups - 1) / kGroups, uint64_t(sm_count()));

@@ -830,6 +830,7 @@ void untake(const Dag& g, PlanState& s, const std::vector<size_t>& taken) {
 // per tile qubit that lengthens the runs (those in [pinned, c)).
 struct TileShape {
     int m, n, pinned, spread_bit, max_spread, inflight_bits;
+    size_t max_ops = 0;  // operations per pass (0: no limit)
     int spread(uint64_t T) const {
         if (spread_bit >= 64) return 0;
         const uint64_t hi = T >> spread_bit;
@@ -906,10 +907,11 @@ size_t grow(const Dag& g, PlanState& s, size_t seed, const TileShape& sh, bool l
         size = __builtin_popcountll(T);
         closure(g, s, T, taken, x.work);
     }
-    const size_t total = taken.size();
     untake(g, s, taken);
     s.first_open = first_open;
-    return total;
+    // A depth limit keeps the first operations taken (a dependency-closed prefix).
+    if (sh.max_ops && taken.size() > sh.max_ops) taken.resize(sh.max_ops);
+    return taken.size();
 }
 
 // One pass of a plan: its tile qubits (before padding) and the ops it takes.
@@ -1209,7 +1211,7 @@ std::vector<TilePass> plan_tiles(const std::vector<Operation>& ops, size_t begin
     const int beam = N > kPlanBeamMaxOps ? 1 : std::max(1, opt.beam);
     // A seed's own qubits are always allowed; the cap applies to the rest.
     TileShape sh{m, n, pinned, std::max(opt.spread_bit, 0), opt.max_spread >= 0 ? opt.max_spread : INT_MAX,
-                 std::max(opt.inflight_bits, 0)};
+                 std::max(opt.inflight_bits, 0), size_t(std::max(opt.max_pass_ops, 0))};
     const std::vector<PassChoice> chosen = choose_passes(g, sh, std::max(1, opt.seeds), beam);
     for (const PassChoice& pc : chosen) {
         std::vector<char> inT(size_t(n), 0);

@@ -73,6 +73,9 @@ struct TilePlanOptions {
     int spread_bit = 0;
     int max_spread = -1;
     int inflight_bits = 9;
+    // Shared-memory pass depth: at most this many operations per pass (0: no
+    // limit).  Shallower passes cost more passes but less work per tile item.
+    int max_pass_ops = 0;
 };
 
 constexpr size_t kPlanBeamMaxOps = 50000;
@@ -253,6 +256,8 @@ void fused_state_norm(const Batch& b, const double* tile_norm, double* norm);
 // sums fused_state_norm left (FP64 scale).
 void fused_renormalize(const Batch& b, const double* norm);
 size_t fused_smem_bytes();
+// Sets the fused kernel's shared-memory attributes on the current device (once).
+void fused_configure();
 // Failure-path tests: gate images of fused steps >= withhold_step are never
 // fetched, and every bounded wait of the fused kernel gives up after wait_ms
 // (<= 0: the default of about 2 s).  ~0 restores normal operation.

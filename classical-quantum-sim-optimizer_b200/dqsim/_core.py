@@ -507,24 +507,30 @@ _batch_counts = _sig("dq_batch_counts", [_P, _u64, ctypes.POINTER(_P)])
 _batch_zz = _sig("dq_batch_expect_zz", [_P, _P, _u64])
 _batch_sv = _sig("dq_batch_statevector", [_P, _u64, _P, _u64])
 _batch_info = _sig("dq_batch_info", [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
+_batch_work = _sig("dq_batch_work", [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_u64)])
 _batch_free = _sig("dq_batch_free", [_P], None)
 
 
 class BatchedCircuits:
-    """Many terminal-measurement circuits of uneven sizes in one persistent launch (dq_batch_*).
+    """Many terminal-measurement circuits of uneven sizes in one CUDA graph (dq_batch_*): a persistent
+    tile kernel, and tensor-core fused passes on side streams where the autotuner picks them.
 
     Seeds: circuit i samples with seed + i * 0x9E3779B97F4A7C15 (mod 2^64), shot t
     of it with ChaCha8 seed_from_u64(that + t), as a single simulate_shots call would.
     """
 
-    def __init__(self, simulator, circuits, shots=1024, autotune=False):
+    def __init__(self, simulator, circuits, shots=1024, autotune=False, tensor_cores=False):
+        """autotune=True times candidate shapes per qubit count (tensor-core passes among them);
+        tensor_cores=True runs every complex64 circuit of 12 or more qubits as tensor-core fused passes."""
         texts = [_circuit_json(c) for c in circuits]
         self._keep = [ctypes.create_string_buffer(t, len(t)) for t in texts]
         ptrs = (ctypes.c_void_p * len(texts))(*[ctypes.cast(b, ctypes.c_void_p) for b in self._keep])
         lens = (ctypes.c_size_t * len(texts))(*[len(t) for t in texts])
         h = _P()
         _check(_batch_create(simulator._h, ctypes.cast(ptrs, _P), ctypes.cast(lens, _P), len(texts),
-                             _as_u64(shots, "shots"), 1 if autotune else 0, ctypes.byref(h)))
+                             _as_u64(shots, "shots"), 2 if tensor_cores else (1 if autotune else 0),
+                             ctypes.byref(h)))
         self._h = h
         self._sim = simulator
         self.size = len(texts)
@@ -558,6 +564,12 @@ class BatchedCircuits:
         out = np.empty(1 << n, dtype=np.complex128)
         _check(_batch_sv(self._h, i, out.ctypes.data_as(_P), 2 * out.shape[0]))
         return out
+
+    def work(self):
+        """One run's algorithmic HBM bytes, tensor and CUDA-core FLOPs, and tensor-core circuits."""
+        b, tf, cf, fc = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), _u64()
+        _check(_batch_work(self._h, ctypes.byref(b), ctypes.byref(tf), ctypes.byref(cf), ctypes.byref(fc)))
+        return {"bytes": b.value, "tensor_flops": tf.value, "cuda_core_flops": cf.value, "fused_circuits": fc.value}
 
 
 BATCH_SEED_STRIDE = 0x9E3779B97F4A7C15

@@ -187,8 +187,12 @@ DQ_API void dq_plan_free(dq_plan* p);
  * samples each (per-shot ChaCha8 streams as shots.rs:153-158) and reduced to
  * <Z0 Z1>.  No counterpart in the reference, which runs one circuit per call;
  * each circuit's counts follow the reference's terminal-sampling semantics
- * (shots.rs:93-176).  autotune != 0 times candidate tile shapes and fusion
- * widths per qubit count first.  A run can replay a captured CUDA graph. */
+ * (shots.rs:93-176).  autotune = 1 times, per qubit count, candidate tile
+ * shapes, fusion widths and shared-memory pass depths of the persistent
+ * kernel and (complex64, 12 qubits or more) tensor-core fused passes, which
+ * run on side streams beside it; autotune = 2 takes the tensor-core fused
+ * passes wherever they apply without timing; 0 keeps the default tile shape.
+ * A run can replay a captured CUDA graph. */
 typedef struct dq_batch dq_batch;
 DQ_API int dq_batch_create(dq_sim* sim, const char* const* jsons, const size_t* json_lens, uint64_t count,
                            uint64_t shots, int autotune, dq_batch** out);
@@ -197,6 +201,12 @@ DQ_API int dq_batch_counts(const dq_batch* b, uint64_t index, dq_counts** out);
 DQ_API int dq_batch_expect_zz(const dq_batch* b, double* out, uint64_t count);
 DQ_API int dq_batch_statevector(const dq_batch* b, uint64_t index, double* out, uint64_t out_len);
 DQ_API int dq_batch_info(const dq_batch* b, uint64_t* passes, uint64_t* items);
+/* One run's work: algorithmic HBM bytes of its passes (each pass reads and
+ * writes its circuit's state once), tensor-core f16 FLOPs of the fused blocks,
+ * real CUDA-core FLOPs of the tile operations, and how many circuits run as
+ * tensor-core fused passes (the rest run in the persistent tile kernel). */
+DQ_API int dq_batch_work(const dq_batch* b, double* bytes, double* tensor_flops, double* cuda_core_flops,
+                         uint64_t* fused_circuits);
 DQ_API void dq_batch_free(dq_batch* b);
 
 /* Learned fusion cost model (no counterpart in the reference): a 16-64-64-1

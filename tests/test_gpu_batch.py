@@ -1,4 +1,5 @@
-"""Batched uneven circuits in one persistent launch (and its CUDA graph replay)."""
+"""Batched uneven circuits: one persistent launch, tensor-core fused passes on side streams, and the CUDA
+graph replay of both."""
 
 import numpy as np
 import pytest
@@ -83,3 +84,29 @@ def test_batch_rejects_mid_circuit_measurement():
     sim = dqsim.StatevectorSimulator(seed=1)
     with pytest.raises(ValueError):
         _core.BatchedCircuits(sim, [c], shots=16)
+
+
+def test_tensor_core_batch_matches_oracle_and_replays_identically():
+    """Complex64 circuits of 12 or more qubits as tensor-core fused passes on side streams (the smaller ones in
+    the persistent kernel), captured in one graph: states, <Z0 Z1> and counts against the oracle."""
+    cs = circuits(14, 4, 8, 18)
+    sim = dqsim.StatevectorSimulator(seed=21, precision="complex64", max_memory_mb=1 << 14)
+    b = _core.BatchedCircuits(sim, cs, shots=512, tensor_cores=True)
+    w = b.work()
+    assert w["fused_circuits"] == sum(1 for c in cs if c.num_qubits >= 12) > 0
+    assert w["tensor_flops"] > 0 and w["bytes"] > 0
+    b.run(use_graph=False)
+    zz = b.expect_zz()
+    direct = [b.counts(i) for i in range(len(cs))]
+    for i, c in enumerate(cs):
+        n = c.num_qubits
+        unitary = workloads.TransportCircuit(n, [x for x in c.data["instructions"] if x["kind"] != "measure"])
+        want = o.OracleSimulator(seed=1).simulate(unitary).statevector
+        got = b.statevector(i, n)
+        assert abs(np.vdot(got, want)) ** 2 >= 1 - 1e-6
+        assert abs(zz[i] - zz_of(want)) <= 1e-5
+        assert sum(direct[i].values()) == 512
+    for _ in range(2):
+        b.run(use_graph=True)
+    assert [b.counts(i) for i in range(len(cs))] == direct
+    np.testing.assert_array_equal(b.expect_zz(), zz)
