@@ -339,10 +339,13 @@ DQ_API int dq_measure_noalloc(void* states, int precision, uint64_t num_states, 
  * makes, on blocks the caller keeps in device memory (2^num_qubits complex128
  * or complex64 amplitudes by the context's precision, little-endian in the
  * block's local qubits, qubits[0] the MSB of a matrix or probability index).
- * A context owns a stream: its calls run in order on it, asynchronously except
- * dq_block_measure (which returns the outcome) and dq_blocks_sync; the block
- * bookkeeping (which qubits a block holds, when to merge) stays with the
- * caller, as in model.rs. */
+ * A context owns a non-blocking stream: its calls run in order on it,
+ * asynchronously except dq_block_measure (which returns the outcome) and
+ * dq_blocks_sync.  It does not wait for other streams, so work that writes a
+ * block elsewhere must be synchronised before the call, and a block must stay
+ * allocated until the context's stream has used it.  The block bookkeeping
+ * (which qubits a block holds, when to merge) stays with the caller, as in
+ * model.rs. */
 typedef struct dq_blocks dq_blocks;
 DQ_API int dq_blocks_create(int device, int precision, dq_blocks** out);
 DQ_API void dq_blocks_destroy(dq_blocks* ctx);

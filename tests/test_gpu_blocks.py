@@ -25,9 +25,13 @@ TOL = 1e-12
 
 
 def dev(a):
+    """A device copy, complete before it returns: the block context runs on a non-blocking stream of its own,
+    which does not wait for torch's stream."""
     import torch
 
-    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+    t = torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+    torch.cuda.synchronize()
+    return t
 
 
 def host(t):
@@ -98,8 +102,10 @@ def test_merge_is_the_product_state_and_measurement_matches():
     rng = np.random.default_rng(3)
     ctx = _core.BlockContext()
     left, right = rand_state(rng, 3), rand_state(rng, 4)
+    tl, tr = dev(left), dev(right)  # kept alive until the context's stream has read them
     out = torch.empty(1 << 7, dtype=torch.complex128, device="cuda")
-    ctx.merge(dev(left).data_ptr(), 3, dev(right).data_ptr(), 4, out.data_ptr())
+    torch.cuda.synchronize()
+    ctx.merge(tl.data_ptr(), 3, tr.data_ptr(), 4, out.data_ptr())
     ctx.sync()
     # model.rs:216-230: chunk i of the merged state is the left block times right[i].
     assert np.max(np.abs(host(out) - np.kron(right, left))) <= TOL
@@ -121,6 +127,7 @@ def test_probabilities_and_running_sums():
     s = rand_state(rng, n)
     t = dev(s)
     probs = torch.empty(1 << n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
     ctx.probabilities(t.data_ptr(), n, None, probs.data_ptr())
     sums = torch.empty(1 << n, dtype=torch.float64, device="cuda")
     ctx.running_sums(t.data_ptr(), n, sums.data_ptr())
@@ -146,10 +153,12 @@ def test_pblock_bookkeeping_on_device_blocks_matches_the_statevector():
     for wires in ((0, 1), (2, 3)):
         b = torch.zeros(4, dtype=torch.complex128, device="cuda")
         b[0] = 1
+        torch.cuda.synchronize()
         ctx.apply_one_qubit(b.data_ptr(), 2, 0, h)
         ctx.apply_x(b.data_ptr(), 2, 1, [(0, True)])
         blocks[wires] = b
     merged = torch.empty(16, dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
     ctx.merge(blocks[(0, 1)].data_ptr(), 2, blocks[(2, 3)].data_ptr(), 2, merged.data_ptr())
     local = [0, 1, 2, 3]  # wire of each local qubit after the merge
     ctx.apply_x(merged.data_ptr(), 4, local.index(2), [(local.index(1), True)])
