@@ -77,8 +77,10 @@ def tensor_peak():
 # and lo*hi products of the 128 x 64 operand with the 64 x 64 real gate image.
 FUSED_FLOPS_PER_TILE_BLOCK = 3 * 2 * 128 * 64 * 64
 # DRAM bytes (read + write) per tile of one k_fused launch, from the ncu capture
-# of a 25-qubit pass (477.9 MB over 8192 tiles; traffic grows with the tiles).
-FUSED_TRAFFIC_PER_TILE = 477.933e6 / 8192
+# of the first pass of the 28-qubit depth-40 brickwork (2 GiB complex64 state,
+# 16x the L2): 2.147771 GB read + 2.088167 GB written over 2^16 tiles.  Traffic
+# grows with the tiles, so a 30-qubit launch moves 2^18 times this.
+FUSED_TRAFFIC_PER_TILE = (2.147771e9 + 2.088167e9) / 65536
 
 
 class ClockSampler:
@@ -313,7 +315,7 @@ def fused_roofline(plan, stats, n):
             "unit": "TFLOP/s", "frac": achieved / burst, "frac_of_sustained": achieved / sustained,
             "peak_kind": kind, "flops": flops, "launches": fused["launches"],
             "hbm_gbs": fused["bytes"] / (fused["ms"] * 1e-3) / 1e9,
-            "traffic": FUSED_TRAFFIC_PER_TILE * tiles, "traffic_unit": "bytes per launch (scaled from 25 qubits)",
+            "traffic": FUSED_TRAFFIC_PER_TILE * tiles, "traffic_unit": "bytes per launch (scaled from 28 qubits)",
             "algorithmic_bytes_per_launch": 16.0 * tiles * 4096}
 
 
