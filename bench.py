@@ -338,6 +338,8 @@ def main():
     ap.add_argument("--forms", default="fused,c64_cuda_core,c128_tiled,c128_per_gate",
                     help="forms timed beside the fused one (profiling runs time the fused form alone)")
     ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--learned-rows", default="",
+                    help="--workload learned: train on these recorded pass rows (.npz) instead of recording anew")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -624,11 +626,15 @@ def run_learned(args):
     import dqsim
     from dqsim import _core, pass_costs
 
-    rec = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
     t0 = time.perf_counter()
-    rows = pass_costs.record(rec, seed=args.seed)
+    if args.learned_rows:
+        # Rows this engine recorded earlier (tests/golden/make_fused_pass_costs.py writes them).
+        rows = dict(np.load(args.learned_rows))
+    else:
+        rec = dqsim.StatevectorSimulator(seed=1, precision="complex64", max_memory_mb=1 << 20)
+        rows = pass_costs.record(rec, seed=args.seed)
+        del rec
     record_s = time.perf_counter() - t0
-    del rec
     t0 = time.perf_counter()
     model, mse = pass_costs.train(rows, seed=args.seed)
     train_s = time.perf_counter() - t0
@@ -654,6 +660,7 @@ def run_learned(args):
         _core.set_cost_model(sim, None)
         del learned, greedy
     print(json.dumps({"workload": "learned-fused-planner-vs-hand-rule", "samples": int(len(rows["ms"])),
+                      "rows_from": args.learned_rows or "recorded in this run",
                       "record_s": record_s, "train_s": train_s, "train_mse": mse, "results": results,
                       "rejection_rate": sum(r["rejected"] for r in results) / len(results)}))
     return 0
