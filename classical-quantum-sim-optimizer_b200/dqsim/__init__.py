@@ -41,21 +41,6 @@ __all__ = [
 ]
 
 
-class QASMImportError(ValueError):
-    """Raised by the OpenQASM helpers, which need Qiskit (not part of this engine)."""
+from .qasm import ImportedCircuit, QASMImportError, from_qiskit, load_qasm, parse_qasm  # noqa: E402
 
-
-class ImportedCircuit:  # pragma: no cover - placeholder for the reference's qasm transport
-    def __init__(self, *args, **kwargs):
-        raise NotImplementedError("OpenQASM import is not provided by the B200 statevector engine")
-
-
-def from_qiskit(*args, **kwargs):
-    raise NotImplementedError("OpenQASM import is not provided by the B200 statevector engine")
-
-
-def load_qasm(*args, **kwargs):
-    raise NotImplementedError("OpenQASM import is not provided by the B200 statevector engine")
-
-
-__all__ += ["ImportedCircuit", "QASMImportError", "from_qiskit", "load_qasm"]
+__all__ += ["ImportedCircuit", "QASMImportError", "from_qiskit", "load_qasm", "parse_qasm"]
