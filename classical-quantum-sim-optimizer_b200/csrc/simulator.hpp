@@ -95,6 +95,18 @@ class Result {
     void pauli_xz(uint64_t x, uint64_t z, double* re, double* im) const;
 };
 
+// A circuit text this simulator ran through simulate_shots: its compiled
+// operations and, once a terminal-sampling call has planned it, the executor
+// of its unitary prefix (passes, fused blocks and gate images on the device).
+// A call with the byte-identical text reuses both, skipping parse, validation,
+// compilation and planning, which give the same result for the same text.
+struct ShotPlan {
+    std::string json;
+    std::vector<Operation> ops;
+    uint64_t n = 0, ncb = 0;
+    std::unique_ptr<Executor> prefix;
+};
+
 class Simulator {
   public:
     explicit Simulator(const Options& o);
@@ -109,7 +121,12 @@ class Simulator {
         return dev_;
     }
     // Learned fusion planner (not owned; detach before the model is freed).
-    void set_cost_model(const CostModel* m) { model_ = m; }
+    // Plans cached before it changed no longer apply.
+    void set_cost_model(const CostModel* m) {
+        std::lock_guard<std::mutex> lk(mu_);
+        model_ = m;
+        plans_.clear();
+    }
     const CostModel* cost_model() const { return model_; }
     // Planner decisions: one JSON object per prepared circuit that compared
     // a learned plan with the greedy one (rejections included).
@@ -136,13 +153,16 @@ class Simulator {
     const CostModel* model_ = nullptr;
     std::vector<std::string> planner_log_;
     double phases_[kNumCallPhases] = {};
+    // Most recently used first; at most kShotPlans entries.
+    static constexpr size_t kShotPlans = 4;
+    std::vector<std::shared_ptr<ShotPlan>> plans_;
     void set_phase(int i, double v) {
         std::lock_guard<std::mutex> lk(mu_);
         phases_[i] = v;
     }
     uint64_t next_seed();
     ShotOutput run_shots(const std::vector<Operation>& ops, uint64_t n, uint64_t ncb, uint64_t shots, uint64_t seed,
-                         bool profile);
+                         bool profile, ShotPlan* plan = nullptr);
 };
 
 // Writes dqsim_profiles/statevector_shots_profile_<unix_ns>.json

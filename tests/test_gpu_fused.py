@@ -107,3 +107,24 @@ def test_fused_trajectories_and_sampling():
     ref.run()
     fid, err = plan.compare(ref)
     assert fid >= 1 - 1e-6 and err <= 1e-5
+
+
+def test_repeated_calls_reuse_the_compiled_plan():
+    """A simulator keeps the compiled operations and prefix executor of the circuit texts it ran: a repeated
+    call skips parse, compile and planning and gives the counts a fresh simulator gives; other texts are
+    planned on their own."""
+    c = brickwork(14, 6, seed=3, measure=True)
+    sim = dqsim.StatevectorSimulator(seed=5, precision="complex64")
+    first = sim.simulate_shots(c, 4000)
+    ph1 = _core.last_call_phases(sim)
+    again = sim.simulate_shots(c, 4000)
+    ph2 = _core.last_call_phases(sim)
+    assert again == first
+    assert ph1["parse"] > 0 and ph2["parse"] == 0 and ph2["compile"] == 0
+    assert dqsim.StatevectorSimulator(seed=5, precision="complex64").simulate_shots(c, 4000) == first
+    for s in range(6):  # more texts than the cache holds, then the first again
+        other = brickwork(14, 6, seed=10 + s, measure=True)
+        assert sim.simulate_shots(other, 500) == dqsim.StatevectorSimulator(
+            seed=5, precision="complex64").simulate_shots(other, 500)
+    assert sim.simulate_shots(c, 4000) == first
+    assert _core.last_call_phases(sim)["parse"] > 0  # evicted, so planned again
