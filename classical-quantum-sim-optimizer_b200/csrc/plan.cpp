@@ -48,15 +48,31 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
         // Learned plan vs the greedy fixed-width plan: the faster one is kept,
         // and a learned plan slower than greedy is rejected and logged.
         auto learned = std::make_unique<Executor>(ops_, 0, end, lc);
+        // A fused-pass model that picks, in every segment, the plan of the hand rule's
+        // own cap has chosen the very same plan (the planner is deterministic): nothing
+        // to compare, so it is neither timed again nor counted as a rejection.
+        bool same = lc.pass_model != nullptr && learned->fused_choices().size() == ex_->fused_choices().size() &&
+                    learned->chosen_widths() == ex_->chosen_widths();
+        for (size_t s = 0; same && s < learned->fused_choices().size(); s++) {
+            const FusedPlanChoice& a = learned->fused_choices()[s];
+            const FusedPlanChoice& b = ex_->fused_choices()[s];
+            same = a.caps[a.chosen] == b.caps[b.chosen];
+        }
         greedy_ms_ = std::min(run(false), run(false));
-        std::swap(ex_, learned);
-        run(false);
-        learned_ms_ = std::min(run(false), run(false));
-        std::vector<int> widths = ex_->chosen_widths();
-        const std::vector<FusedPlanChoice> choices = ex_->fused_choices();
-        rejected_ = learned_ms_ > greedy_ms_;
-        if (rejected_) std::swap(ex_, learned);
-        used_learned_ = !rejected_;
+        std::vector<int> widths = learned->chosen_widths();
+        const std::vector<FusedPlanChoice> choices = learned->fused_choices();
+        if (same) {
+            learned_ms_ = greedy_ms_;
+            rejected_ = false;
+            used_learned_ = true;
+        } else {
+            std::swap(ex_, learned);
+            run(false);
+            learned_ms_ = std::min(run(false), run(false));
+            rejected_ = learned_ms_ > greedy_ms_;
+            if (rejected_) std::swap(ex_, learned);
+            used_learned_ = !rejected_;
+        }
         std::string w;
         for (size_t i = 0; i < widths.size(); i++) w += (i ? "," : "") + std::to_string(widths[i]);
         char buf[256];
@@ -64,7 +80,7 @@ Plan::Plan(Simulator& sim, const char* json, size_t len, uint64_t shots) : opt_(
                       "{\"qubits\": %llu, \"ops\": %llu, \"greedy_ms\": %.4f, \"learned_ms\": %.4f, \"rejected\": %s, ",
                       (unsigned long long)n_, (unsigned long long)ops_.size(), greedy_ms_, learned_ms_,
                       rejected_ ? "true" : "false");
-        std::string line = std::string(buf) + "\"kind\": \"" +
+        std::string line = std::string(buf) + "\"same_plan\": " + (same ? "true" : "false") + ", \"kind\": \"" +
                            (model->kind() == kCostFusedPasses ? "fused_passes" : "tile_ops") + "\", \"widths\": [" + w +
                            "], \"fused_plans\": [";
         // Per planned segment: the candidate plans (spread cap, passes, blocks, hand-rule

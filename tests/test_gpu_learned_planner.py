@@ -1,0 +1,66 @@
+"""The learned fused-pass planner against the hand rule, on a fixed recorded dataset.
+
+tests/golden/fused_pass_costs_b200.npz holds k_fused timings this engine
+recorded on a B200 (tests/golden/make_fused_pass_costs.py): seeded random
+passes at 24-32 qubits and every distinct pass of the candidate plans of
+depth-40 brickwork and QFT circuits of 24-30 qubits.
+tests/golden/fused_pass_portfolios_b200.json holds the held-out circuits'
+candidate plans (brickwork at 26, 30 and 33 qubits, QFT at 32) with every
+pass's recorded time.  The model is trained on the device from the recorded
+rows alone (no new timing, so the outcome does not depend on the machine that
+runs the test); then, for each held-out circuit, the plan it predicts fastest
+must have a recorded time no worse than the hand rule's plan, and for at least
+one circuit a recorded time lower by at least 2%.
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from dqsim import pass_costs
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def load():
+    rows = dict(np.load(GOLDEN / "fused_pass_costs_b200.npz"))
+    held = json.loads((GOLDEN / "fused_pass_portfolios_b200.json").read_text())["held_out"]
+    return rows, held
+
+
+@pytest.fixture(scope="module")
+def trained():
+    rows, held = load()
+    model, mse = pass_costs.train(rows, seed=0)
+    return model, mse, held
+
+
+def test_model_fits_the_recorded_passes(trained):
+    model, mse, held = trained
+    assert mse < 0.1, mse  # in units of the targets' variance
+    # Held-out passes (never trained on): predicted vs recorded milliseconds.
+    rel = []
+    for h in held:
+        pf = h["portfolio"]
+        rows = pass_costs.portfolio_rows(pf)
+        pred = np.exp(model.predict(pass_costs.features(rows)).astype(np.float64)) * 2.0 ** (pf["n"] - 12) * 1e-6
+        rel.extend(np.abs(pred - rows["ms"]) / rows["ms"])
+    assert np.median(rel) < 0.15, np.median(rel)
+
+
+def test_learned_choice_beats_the_hand_rule_on_recorded_times(trained):
+    model, _, held = trained
+    gains = []
+    for h in held:
+        pf = h["portfolio"]
+        recorded = pass_costs.plan_ms(pf, [p["ms"] for p in pf["passes"]])
+        predicted = pass_costs.predicted_plan_ms(model, pf)
+        learned = int(np.argmin(predicted))
+        rule = pf["rule_choice"]
+        # Never worse than the hand rule's plan by more than the recorded timings' noise.
+        assert recorded[learned] <= recorded[rule] * 1.01, (h["kind"], h["n"], recorded, learned, rule)
+        gains.append(recorded[rule] / recorded[learned])
+    assert max(gains) >= 1.02, gains
