@@ -48,9 +48,12 @@ namespace k {
 namespace {
 
 constexpr int kGroups = 4;                               // tiles in flight per CTA (one per group)
-constexpr int kGroupWarps = 4;
+constexpr int kGroupWarps = 4;                           // 4 or 8: warps w and w + 4 share a TMEM lane quarter
 constexpr int kGroupThreads = 32 * kGroupWarps;
 constexpr int kThreads = kGroups * kGroupThreads;
+constexpr int kPairIters = 2048 / kGroupThreads;         // 16-byte amplitude pairs per thread and tile
+constexpr uint32_t kRowStep = uint32_t(kGroupThreads) / 32u;  // rows of 64 amplitudes between a thread's pairs
+constexpr int kHPerWarp = 16 / kGroupWarps;              // readback quarters (8 outputs each) per warp
 constexpr uint32_t kTmemCols = 512;                      // one 128-column accumulator per group
 constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part of a tile (4096 x 4 B)
 constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
@@ -71,7 +74,7 @@ static_assert(kOffDesc % 16 == 0 && kDescBytes % 16 == 0, "bulk copies need 16-b
 static_assert(kOffU % 1024 == 0 && kOffBar % 8 == 0 && kOffWsum % 8 == 0, "operand and mbarrier alignment");
 static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
 static_assert(kUBytes == kFusedUHalves * 2, "gate image size");
-static_assert(kGroupWarps == 4, "a group's warps cover the four TMEM lane quarters");
+static_assert(kGroupWarps == 4 || kGroupWarps == 8, "a group's warps cover the four TMEM lane quarters evenly");
 
 // mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
 constexpr uint32_t kBarUFull = 0;                     // [kUBufs] gate image of buffer b landed (expect_tx)
@@ -315,8 +318,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t pair_out = io[128 + ((2 * gt) & 63)];
     const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
     const uint32_t prow = uint32_t((2 * gt) >> 6);
-    const uint32_t col = uint32_t(gw * 32 + lane);        // readback: TMEM lane = tile column
-    const uint32_t taddr = tmem + ((uint32_t(gw) * 32u) << 16) + 128u * uint32_t(g);
+    const uint32_t col = uint32_t((gw & 3) * 32 + lane);  // readback: TMEM lane = tile column
+    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 128u * uint32_t(g);
+    const int h0 = (gw >> 2) * kHPerWarp;                 // this warp's first readback quarter
     const uint64_t desc_x = make_desc_sw128(smem_addr(x));
     double scale = 1.0;
     uint64_t scale_state = ~uint64_t(0);
@@ -354,9 +358,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const float2* __restrict__ src = s + tile_base(tt, n, fq);
 #pragma unroll
-        for (int k = 0; k < 16; k++)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(x + (2u * gt + 256u * k) * 8u)),
-                         "l"(src + (pair_lo | hi_tab[prow + 4 * k]))
+        for (int k = 0; k < kPairIters; k++)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                             smem_addr(x + (2u * gt + 2u * kGroupThreads * k) * 8u)),
+                         "l"(src + (pair_lo | hi_tab[prow + kRowStep * k]))
                          : "memory");
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -391,13 +396,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             group_sync(g);  // the group's copies of this tile have landed
         }
         {
-            float4 v[16];
+            float4 v[kPairIters];
 #pragma unroll
-            for (int k = 0; k < 16; k++) v[k] = *reinterpret_cast<const float4*>(x + (2u * gt + 256u * k) * 8u);
+            for (int k = 0; k < kPairIters; k++)
+                v[k] = *reinterpret_cast<const float4*>(x + (2u * gt + 2u * kGroupThreads * k) * 8u);
             group_sync(g);  // raw tile read: the split may overwrite it
 #pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const uint32_t hi_part = io[64 + prow + 4 * k];
+            for (int k = 0; k < kPairIters; k++) {
+                const uint32_t hi_part = io[64 + prow + kRowStep * k];
                 put_split2(x, pair_even ^ hi_part,
                            mul2(pack2(__float_as_uint(v[k].x), __float_as_uint(v[k].y)), fs2));
                 put_split2(x, pair_odd ^ hi_part,
@@ -468,8 +474,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % kTBufs) * kDescBytes);
             const uint32_t cpart = nb[32 + col];
 #pragma unroll
-            for (int h = 0; h < 4; h++) {
+            for (int hh = 0; hh < kHPerWarp; hh++) {
                 // Outputs 8h..8h+7: columns 16h.. (hi*hi + lo*hi) plus 64 + 16h.. (hi*lo).
+                const int h = h0 + hh;
                 uint32_t r[16], q[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
@@ -515,9 +522,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         float2* __restrict__ gp = s + base;
 #pragma unroll 8
-        for (int k = 0; k < 16; k++)  // 16-byte pairs: adjacent stage slots, adjacent in HBM
-            *reinterpret_cast<float4*>(gp + (pair_lo | hi_tab[prow + 4 * k])) =
-                *reinterpret_cast<const float4*>(x + (pair_out ^ io[192 + prow + 4 * k]));
+        for (int k = 0; k < kPairIters; k++)  // 16-byte pairs: adjacent stage slots, adjacent in HBM
+            *reinterpret_cast<float4*>(gp + (pair_lo | hi_tab[prow + kRowStep * k])) =
+                *reinterpret_cast<const float4*>(x + (pair_out ^ io[192 + prow + kRowStep * k]));
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;
