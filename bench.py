@@ -175,6 +175,17 @@ def max_over_ranks(pg, local, value):
     return float(t.item())
 
 
+def sum_over_ranks(pg, local, value):
+    if pg is None:
+        return value
+    import torch
+
+    device = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
 def time_form(dqsim, circuit, precision, local, steps, warmup, shots, seed, execution="auto", **kw):
     sim = dqsim.StatevectorSimulator(seed=seed, max_memory_mb=1 << 20, precision=precision, device=local,
                                      execution=execution, **kw)
@@ -510,31 +521,41 @@ def run_qft(args):
 def run_batch(args):
     """512 uneven HEA circuits (12..22 qubits, depth 4..16), 1024 shots and <Z0 Z1> each, in one CUDA graph
     (autotuned per qubit count: persistent tile kernel or tensor-core fused passes on side streams), vs a
-    per-circuit complex128 per-gate loop on the device and the CPU restatement on a sample of the circuits."""
+    per-circuit complex128 per-gate loop on the device and the CPU restatement on a sample of the circuits.
+    With N ranks every rank runs its longest-processing-time share of the circuits on its own GPU (no
+    data-path collective); the batch time is the maximum over ranks and <Z0 Z1> merges in one all-reduce."""
     import dqsim
+    from dqsim import sharding
     from oracle import oracle
 
+    world, rank, local, pg = dist_setup(args)
     peak, peak_kind = peaks()
-    circuits = dqsim.workloads.hea_batch(512, seed=args.seed)
-    sim = dqsim.StatevectorSimulator(seed=args.seed, precision="complex64", max_memory_mb=1 << 16)
+    all_circuits = dqsim.workloads.hea_batch(512, seed=args.seed)
+    mine, circuits = sharding.shard(all_circuits, world, rank)
+    sim = dqsim.StatevectorSimulator(seed=args.seed, precision="complex64", max_memory_mb=1 << 16, device=local)
     t0 = time.perf_counter()
     batch = dqsim._core.BatchedCircuits(sim, circuits, shots=1024, autotune=True)
     setup_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         batch.run()
+    barrier(pg)
     ms = [batch.run() for _ in range(args.steps)]
     zz = batch.expect_zz()
     work = batch.work()
-    batch_ms = statistics.mean(ms)
+    batch_ms = max_over_ranks(pg, local, statistics.mean(ms))
+    zz_all = sharding.merge_values(pg, mine, zz, len(all_circuits),
+                                   device=f"cuda:{local}" if pg is not None and pg.get_backend() == "nccl" else "cpu")
+    work = {k: (sum_over_ranks(pg, local, v) if k != "fused_circuits" else int(sum_over_ranks(pg, local, v)))
+            for k, v in work.items()}
     burst, _, tkind = tensor_peak()
     roof = {"bound": "hbm", "achieved": work["bytes"] / (batch_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
             "peak_kind": peak_kind, "algorithmic_bytes": work["bytes"],
             "tensor_tflops": work["tensor_flops"] / (batch_ms * 1e-3) / 1e12, "tensor_peak": burst,
             "cuda_core_tflops": work["cuda_core_flops"] / (batch_ms * 1e-3) / 1e12}
-    roof["frac"] = roof["achieved"] / peak
-    roof["tensor_frac"] = roof["tensor_tflops"] / burst
+    roof["frac"] = roof["achieved"] / (peak * world)  # whole-job rates against N GPUs' peaks
+    roof["tensor_frac"] = roof["tensor_tflops"] / (burst * world)
     sim128 = dqsim.StatevectorSimulator(seed=args.seed, precision="complex128", max_memory_mb=1 << 16,
-                                        execution="per_gate")
+                                        execution="per_gate", device=local)
     loop_ms, zz_err = 0.0, 0.0
     t1 = time.perf_counter()
     for i, c in enumerate(circuits):
@@ -548,32 +569,41 @@ def run_batch(args):
             zz_err = max(zz_err, abs(float(np.dot(p, sign)) - float(zz[i])))
         del plan
     loop_wall = time.perf_counter() - t1
-    # CPU restatement on a bounded sample: whole simulate_shots calls on circuits taken in a seeded order
-    # until the budget is spent, scaled to the batch by amplitude-operations (2^n x gates per circuit).
-    rng = np.random.default_rng(args.seed)
-    order = rng.permutation(len(circuits))
-    weight = [(1 << c.num_qubits) * len(c.data["instructions"]) for c in circuits]
-    cpu_s, cpu_w, done = 0.0, 0, 0
-    osim = oracle.OracleSimulator(seed=args.seed, max_memory_mb=1 << 16)
-    t2 = time.perf_counter()
-    for i in order:
-        if time.perf_counter() - t2 > args.cpu_budget and done >= 4:
-            break
-        t3 = time.perf_counter()
-        osim.simulate_shots(circuits[int(i)], shots=1024)
-        cpu_s += time.perf_counter() - t3
-        cpu_w += weight[int(i)]
-        done += 1
-    cpu_total = cpu_s * sum(weight) / cpu_w
-    print(json.dumps({"workload": f"hea-batch-512-seed{args.seed}", "batch_ms": batch_ms, "runs_ms": ms,
-                      "batch_setup_s": setup_s, "passes": batch.passes, "work_items": batch.items,
-                      "fused_circuits": work["fused_circuits"], "roofline": roof,
-                      "per_circuit_c128_device_ms": loop_ms, "per_circuit_c128_wall_s": loop_wall,
-                      "speedup_device": loop_ms / batch_ms, "zz_max_err_first16": zz_err,
-                      "cpu_baseline": {"value": cpu_total, "unit": "s", "cores": oracle.lib().orc_num_threads(),
-                                       "kind": "port",
-                                       "sample": f"{done} of {len(circuits)} circuits through simulate_shots "
-                                                 f"(1024 shots) in {cpu_s:.1f} s, scaled by 2^n x gates"}}))
+    loop_ms = max_over_ranks(pg, local, loop_ms)
+    zz_err = max_over_ranks(pg, local, zz_err)
+    cpu = None
+    if world == 1:
+        # CPU restatement on a bounded sample: whole simulate_shots calls on circuits taken in a seeded order
+        # until the budget is spent, scaled to the batch by amplitude-operations (2^n x gates per circuit).
+        rng = np.random.default_rng(args.seed)
+        order = rng.permutation(len(circuits))
+        weight = [sharding.circuit_weight(c) for c in circuits]
+        cpu_s, cpu_w, done = 0.0, 0, 0
+        osim = oracle.OracleSimulator(seed=args.seed, max_memory_mb=1 << 16)
+        t2 = time.perf_counter()
+        for i in order:
+            if time.perf_counter() - t2 > args.cpu_budget and done >= 4:
+                break
+            t3 = time.perf_counter()
+            osim.simulate_shots(circuits[int(i)], shots=1024)
+            cpu_s += time.perf_counter() - t3
+            cpu_w += weight[int(i)]
+            done += 1
+        cpu = {"value": cpu_s * sum(weight) / cpu_w, "unit": "s", "cores": oracle.lib().orc_num_threads(),
+               "kind": "port", "sample": f"{done} of {len(circuits)} circuits through simulate_shots "
+                                         f"(1024 shots) in {cpu_s:.1f} s, scaled by 2^n x gates"}
+    passes = int(sum_over_ranks(pg, local, batch.passes))
+    if rank == 0:
+        print(json.dumps({"workload": f"hea-batch-512-seed{args.seed}", "n_gpus": world,
+                          "scaling": "strong", "batch_ms": batch_ms, "runs_ms": ms,
+                          "circuits_per_s": len(all_circuits) / (batch_ms * 1e-3),
+                          "batch_setup_s": setup_s, "passes": passes, "work_items": batch.items,
+                          "fused_circuits": work["fused_circuits"], "roofline": roof,
+                          "per_circuit_c128_device_ms": loop_ms, "per_circuit_c128_wall_s": loop_wall,
+                          "speedup_device": loop_ms / batch_ms, "zz_max_err_first16": zz_err,
+                          "zz_checksum": sum(zz_all), "cpu_baseline": cpu}))
+    if pg is not None:
+        pg.destroy_process_group()
     return 0
 
 

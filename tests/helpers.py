@@ -121,3 +121,10 @@ def assert_distribution(counts, expected, shots, delta=0.08):
     assert set(counts) == set(expected)
     for outcome, p in expected.items():
         assert abs(counts[outcome] / shots - p) <= delta, (outcome, counts[outcome] / shots, p)
+
+
+def zz_expectation(statevector):
+    """<Z0 Z1> of a statevector: sum of |a_i|^2 with sign -1 where qubits 0 and 1 differ."""
+    p = np.abs(np.asarray(statevector)) ** 2
+    idx = np.arange(p.shape[0])
+    return float(np.dot(p, 1 - 2 * ((idx & 1) ^ ((idx >> 1) & 1))))
