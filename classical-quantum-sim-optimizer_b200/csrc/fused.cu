@@ -23,9 +23,10 @@
 // of up to five dimensions whose boxes are the tile's runs of qubits, so one
 // thread issues a tile's load and no load passes through the LSU; tiles whose
 // qubits need more dimensions fall back to 16-byte cp.async copies.
-// All tiles walk the same block sequence and share the gate images (three
-// buffers, fetched three blocks ahead by whichever group finishes its MMAs on
-// a buffer last).  Hand-offs are mbarriers (copies, MMA completion) and
+// All tiles walk the same block sequence and share the gate images: a pass of
+// up to five blocks holds all of them for the whole launch, and a longer one
+// cycles five buffers, fetched five blocks ahead by whichever group finishes
+// its MMAs on a buffer last.  Hand-offs are mbarriers (copies, MMA completion) and
 // per-group named barriers; every mbarrier wait is bounded, and a group stops
 // only by a group-wide vote, so no thread is left waiting on a named barrier.
 // On expiry the CTA records an error, waits (bounded) for its own copies and
@@ -59,7 +60,10 @@ constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part
 constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
 constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
 constexpr uint32_t kDescBytes = 320;                     // next_b[32] + next_c[128] (u16) of one block
-constexpr uint32_t kUBufs = 3;                           // gate images in flight (fetched kUBufs blocks ahead)
+// Gate-image buffers.  A pass of at most kUBufs blocks keeps every block's
+// image and tables resident for the whole launch (fetched once); a longer pass
+// cycles them as a ring fetched kUBufs blocks ahead.
+constexpr uint32_t kUBufs = 5;
 constexpr uint32_t kTBufs = kUBufs + 1;                  // block tables (also read during the readback)
 constexpr uint32_t kOffU = kGroups * kTileBytes;         // group g's operand at g*32K; then the gate images
 constexpr uint32_t kOffTabs = kOffU + kUBufs * kUBytes;  // lo_tab[64], hi_tab[64] (u64)
@@ -266,10 +270,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     // Copies of step st: its block's gate image into buffer st % kUBufs and
     // its tables into buffer st % kTBufs.
     const long long wl = fq.fault.wait_cycles;
+    const bool resident = uint32_t(nblocks) <= kUBufs;
     auto fetch = [&](uint64_t st) {
         if (st >= fq.fault.withhold) return;
         const FusedBlock* blk = blocks + int(st % uint64_t(nblocks));
-        const uint32_t ub = uint32_t(st % kUBufs), tb = uint32_t(st % kTBufs);
+        // Resident passes fetch only steps 0..nblocks-1, each into its own buffers.
+        const uint32_t ub = resident ? uint32_t(st) : uint32_t(st % kUBufs);
+        const uint32_t tb = resident ? uint32_t(st) : uint32_t(st % kTBufs);
         mbar_expect(bar(kBarUFull + ub), kUBytes);
         bulk_g2s(u0 + ub * kUBytes, upool + blk->u_off, kUBytes, bar(kBarUFull + ub));
         mbar_expect(bar(kBarTFull + tb), kDescBytes);
@@ -297,8 +304,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t i = 0; i < kNumBars; i++) mbar_init(bar(i), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         uint64_t f = 0;
+        const uint64_t first = resident ? uint64_t(nblocks) : uint64_t(kUBufs);
         if (!s_abort)
-            for (; f < kUBufs && f < steps; f++) fetch(f);
+            for (; f < first && f < steps; f++) fetch(f);
         s_fetched = f;
     }
     if (warp == 0) {
@@ -422,9 +430,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ok = false;
                 break;
             }
-            const uint32_t ub = uint32_t(st % kUBufs);
+            // Buffers of step st and the parity of their fill: resident buffers fill once.
+            const uint32_t ub = resident ? uint32_t(j) : uint32_t(st % kUBufs);
+            const uint32_t tb = resident ? uint32_t(j) : uint32_t(st % kTBufs);
+            const uint32_t u_par = resident ? 0u : uint32_t(st / kUBufs) & 1u;
+            const uint32_t t_par = resident ? 0u : uint32_t(st / kTBufs) & 1u;
             if (gt == 0) {
-                const bool uw = mbar_wait(bar(kBarUFull + ub), uint32_t(st / kUBufs) & 1u, wl);
+                const bool uw = mbar_wait(bar(kBarUFull + ub), u_par, wl);
                 if (!uw) *static_cast<volatile int*>(&s_gabort[g]) = 1;
                 if (uw) {
                     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -454,14 +466,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             // The readback's TMEM loads are warp-collective: a warp reads back only if
             // every lane saw both waits complete.
             const bool w = __all_sync(0xffffffffu, mbar_wait(bar(kBarMma + g), mma_cnt & 1u, wl) &&
-                                                       mbar_wait(bar(kBarTFull + uint32_t(st % kTBufs)),
-                                                                 uint32_t(st / kTBufs) & 1u, wl));
+                                                       mbar_wait(bar(kBarTFull + tb), t_par, wl));
             mma_cnt++;
             if (!w) {
                 *static_cast<volatile int*>(&s_gabort[g]) = 1;
                 continue;
             }
-            if (gt == 0 && st + kUBufs < steps) {
+            if (!resident && gt == 0 && st + kUBufs < steps) {
                 // The gate-image buffer is free once every tile's MMAs on it completed:
                 // the last group to get here resets the count and fetches step st + kUBufs.
                 if (atomicAdd(&s_ucnt[ub], 1u) + 1u == valid) {
@@ -471,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + uint32_t(st % kTBufs) * kDescBytes);
+            const uint16_t* nb = reinterpret_cast<const uint16_t*>(sm + kOffDesc + tb * kDescBytes);
             const uint32_t cpart = nb[32 + col];
 #pragma unroll
             for (int hh = 0; hh < kHPerWarp; hh++) {
@@ -550,10 +561,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         // (each issuing thread commits and waits for its own MMAs).
         if (g == 0) {
             const uint64_t fetched = s_fetched;
-            for (uint64_t f = fetched > kTBufs ? fetched - kTBufs : 0; f < fetched && f < fq.fault.withhold; f++) {
-                if (f + kUBufs >= fetched)
-                    mbar_wait(bar(kBarUFull + uint32_t(f % kUBufs)), uint32_t(f / kUBufs) & 1u, wl);
-                mbar_wait(bar(kBarTFull + uint32_t(f % kTBufs)), uint32_t(f / kTBufs) & 1u, wl);
+            if (resident) {
+                for (uint64_t f = 0; f < fetched && f < fq.fault.withhold; f++) {
+                    mbar_wait(bar(kBarUFull + uint32_t(f)), 0u, wl);
+                    mbar_wait(bar(kBarTFull + uint32_t(f)), 0u, wl);
+                }
+            } else {
+                for (uint64_t f = fetched > kTBufs ? fetched - kTBufs : 0; f < fetched && f < fq.fault.withhold;
+                     f++) {
+                    if (f + kUBufs >= fetched)
+                        mbar_wait(bar(kBarUFull + uint32_t(f % kUBufs)), uint32_t(f / kUBufs) & 1u, wl);
+                    mbar_wait(bar(kBarTFull + uint32_t(f % kTBufs)), uint32_t(f / kTBufs) & 1u, wl);
+                }
             }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(

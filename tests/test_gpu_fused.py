@@ -48,15 +48,22 @@ def test_fused_scattered_tile_uses_per_thread_copies():
     check(c)
 
 
-def test_fused_bounded_wait_reports_and_recovers():
+@pytest.mark.parametrize("depth, withhold, blocks", [
+    (10, 2, [7, 5, 1]),  # first pass cycles its gate images: an initial fetch withheld
+    (10, 6, [7, 5, 1]),  # ... a fetch issued when step 1's buffer frees up
+    (3, 2, [4, 1]),      # first pass holds all four gate images resident
+])
+def test_fused_bounded_wait_reports_and_recovers(depth, withhold, blocks):
     """A gate image that never arrives (its fetch withheld: a flag nothing sets)
     makes the kernel's bounded waits run out: the CTAs drain, free their tensor
     memory and set the error flag, the call raises RuntimeError, and the same
-    simulator then runs normally."""
-    c = brickwork(14, 10, seed=2, measure=False)
+    simulator then runs normally.  Covers both gate-image modes: a ring (passes
+    of more than five blocks) and resident images (five or fewer)."""
+    c = brickwork(14, depth, seed=2, measure=False)
+    assert [len(p["blocks"]) for p in _core.fused_plan_dump(c.model_dump_json())["passes"]] == blocks
     sim = fused(seed=3)
     try:
-        _core.debug_fused_fault(withhold_step=2, wait_ms=20.0)
+        _core.debug_fused_fault(withhold_step=withhold, wait_ms=20.0)
         with pytest.raises(RuntimeError, match="bounded wait"):
             sim.simulate(c)
     finally:
