@@ -49,13 +49,19 @@ namespace k {
 namespace {
 
 constexpr int kGroups = 4;                               // tiles in flight per CTA (one per group)
+// Accumulators: false = one 128-column accumulator per group, A_hi x [U_hi; U_lo]
+// (N = 128) plus A_lo x U_hi (N = 64) into its first half, the halves summed in
+// the readback; true = one 64-column accumulator per group that all three
+// products (N = 64 each) accumulate into.
+constexpr bool kOneAcc = false;
+constexpr uint32_t kAccCols = kOneAcc ? 64u : 128u;
 constexpr int kGroupWarps = 4;                           // 4 or 8: warps w and w + 4 share a TMEM lane quarter
 constexpr int kGroupThreads = 32 * kGroupWarps;
 constexpr int kThreads = kGroups * kGroupThreads;
 constexpr int kPairIters = 2048 / kGroupThreads;         // 16-byte amplitude pairs per thread and tile
 constexpr uint32_t kRowStep = uint32_t(kGroupThreads) / 32u;  // rows of 64 amplitudes between a thread's pairs
 constexpr int kHPerWarp = 16 / kGroupWarps;              // readback quarters (8 outputs each) per warp
-constexpr uint32_t kTmemCols = 512;                      // one 128-column accumulator per group
+constexpr uint32_t kTmemCols = 512;                      // tensor-memory columns the CTA allocates
 constexpr uint32_t kPartBytes = 16384;                   // one f16 operand part of a tile (4096 x 4 B)
 constexpr uint32_t kTileBytes = 32768;                   // hi + lo parts; also the FP32 stage
 constexpr uint32_t kUBytes = 16384;                      // U_hi + U_lo images of one block (f16)
@@ -63,7 +69,7 @@ constexpr uint32_t kDescBytes = 320;                     // next_b[32] + next_c[
 // Gate-image buffers.  A pass of at most kUBufs blocks keeps every block's
 // image and tables resident for the whole launch (fetched once); a longer pass
 // cycles them as a ring fetched kUBufs blocks ahead.
-constexpr uint32_t kUBufs = 5;
+constexpr uint32_t kUBufs = kGroups == 4 ? 5 : 3;
 constexpr uint32_t kTBufs = kUBufs + 1;                  // block tables (also read during the readback)
 constexpr uint32_t kOffU = kGroups * kTileBytes;         // group g's operand at g*32K; then the gate images
 constexpr uint32_t kOffTabs = kOffU + kUBufs * kUBytes;  // lo_tab[64], hi_tab[64] (u64)
@@ -88,6 +94,7 @@ constexpr uint32_t kBarDrain = kBarMma + kGroups;     // [kGroups] group g's MMA
 constexpr uint32_t kBarTile = kBarDrain + kGroups;    // [kGroups] TMA loads of group g's next tile landed (expect_tx)
 constexpr uint32_t kNumBars = kBarTile + kGroups;
 static_assert(kNumBars <= 32, "mbarrier slots");
+static_assert(kGroups * kAccCols <= kTmemCols, "accumulators fit the allocated tensor memory");
 
 // Failure-path tests: gate images of steps >= withhold are never fetched, so
 // the waits on them run out after wait_cycles (a flag that nothing sets).
@@ -327,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
     const uint32_t prow = uint32_t((2 * gt) >> 6);
     const uint32_t col = uint32_t((gw & 3) * 32 + lane);  // readback: TMEM lane = tile column
-    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + 128u * uint32_t(g);
+    const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + kAccCols * uint32_t(g);
     const int h0 = (gw >> 2) * kHPerWarp;                 // this warp's first readback quarter
     const uint64_t desc_x = make_desc_sw128(smem_addr(x));
     double scale = 1.0;
@@ -444,17 +451,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                     // Descriptors advance by (byte offset >> 4) in their start-address field.
                     // A_hi x [U_hi; U_lo] (N = 128: columns 0..63 hi*hi, 64..127 hi*lo),
                     // then A_lo x U_hi accumulated into columns 0..63.
+                    if constexpr (kOneAcc) {
+                        // Per K slice: A_hi x U_hi, A_hi x U_lo (U_lo = rows 64..127 of
+                        // the image, 8 KB on), A_lo x U_hi, all into one accumulator.
 #pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        const int ks = q & 3;
-                        const bool lo = q >= 4;
-                        const uint64_t ad = desc_x + (lo ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
-                        const uint64_t bd = desc_u + uint64_t(ks * 2);
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + 128u * g),
-                            "l"(ad), "l"(bd), "r"(lo ? kIdescN64 : kIdescN128), "r"(q > 0 ? 1u : 0u));
+                        for (int q = 0; q < 12; q++) {
+                            const int ks = q / 3, which = q % 3;
+                            const uint64_t ad =
+                                desc_x + (which == 2 ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
+                            const uint64_t bd = desc_u + (which == 1 ? uint64_t(8192 >> 4) : 0) + uint64_t(ks * 2);
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+                                    tmem + kAccCols * g),
+                                "l"(ad), "l"(bd), "r"(kIdescN64), "r"(q > 0 ? 1u : 0u));
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 8; q++) {
+                            const int ks = q & 3;
+                            const bool lo = q >= 4;
+                            const uint64_t ad = desc_x + (lo ? uint64_t(kPartBytes >> 4) : 0) + uint64_t(ks * 2);
+                            const uint64_t bd = desc_u + uint64_t(ks * 2);
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+                                    tmem + kAccCols * g),
+                                "l"(ad), "l"(bd), "r"(lo ? kIdescN64 : kIdescN128), "r"(q > 0 ? 1u : 0u));
+                        }
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                         bar(kBarMma + g))
@@ -486,7 +512,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t cpart = nb[32 + col];
 #pragma unroll
             for (int hh = 0; hh < kHPerWarp; hh++) {
-                // Outputs 8h..8h+7: columns 16h.. (hi*hi + lo*hi) plus 64 + 16h.. (hi*lo).
+                // Outputs 8h..8h+7: columns 16h.. (hi*hi + lo*hi) plus 64 + 16h.. (hi*lo),
+                // or columns 16h.. alone with one accumulator.
                 const int h = h0 + hh;
                 uint32_t r[16], q[16];
                 asm volatile(
@@ -496,13 +523,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                       "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
                       "=r"(r[15])
                     : "r"(taddr + 16u * h));
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15}, [%16];"
-                    : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
-                      "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]),
-                      "=r"(q[15])
-                    : "r"(taddr + 64u + 16u * h));
+                if constexpr (!kOneAcc)
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                        "%12, %13, %14, %15}, [%16];"
+                        : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]),
+                          "=r"(q[7]), "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]),
+                          "=r"(q[14]), "=r"(q[15])
+                        : "r"(taddr + 64u + 16u * h));
+                // Output i of the quarter as a packed (re, im) FP32 pair.
+                auto out2 = [&](int i) -> uint64_t {
+                    if constexpr (kOneAcc)
+                        return pack2(r[2 * i], r[2 * i + 1]);
+                    else
+                        return add2(pack2(r[2 * i], r[2 * i + 1]), pack2(q[2 * i], q[2 * i + 1]));
+                };
                 const uint4 nw = *reinterpret_cast<const uint4*>(nb + 8 * h);
                 const uint32_t nbw[4] = {nw.x, nw.y, nw.z, nw.w};
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
@@ -510,14 +545,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
                         const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                        put_split2(x, off, add2(pack2(r[2 * i], r[2 * i + 1]), pack2(q[2 * i], q[2 * i + 1])));
+                        put_split2(x, off, out2(i));
                     }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
                         const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                        const float re = (__uint_as_float(r[2 * i]) + __uint_as_float(q[2 * i])) * kInvScale;
-                        const float im = (__uint_as_float(r[2 * i + 1]) + __uint_as_float(q[2 * i + 1])) * kInvScale;
+                        uint32_t ur, ui;
+                        asm("mov.b64 {%0, %1}, %2;" : "=r"(ur), "=r"(ui) : "l"(out2(i)));
+                        const float re = __uint_as_float(ur) * kInvScale;
+                        const float im = __uint_as_float(ui) * kInvScale;
                         *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
                         norm_acc += double(re) * re + double(im) * im;
                     }
