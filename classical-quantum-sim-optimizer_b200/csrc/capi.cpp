@@ -880,6 +880,34 @@ int dq_tile_plan_dump(const char* json, size_t len, int tile_qubits, int fusion_
                      ",\"lowbit\":" + std::to_string(t.lowbit) + ",\"highbit\":" + std::to_string(t.highbit) +
                      ",\"mat\":" + std::to_string(t.mat) + "}";
             }
+            // The pass's register phases (complex128 swizzle), as the executor plans them.
+            s += "],\"phases\":[";
+            if (phase_supported(int(p.qubits.size()))) {
+                std::vector<TilePhase> phs;
+                std::vector<PhaseOp> pops;
+                plan_phases(p.ops, int(p.qubits.size()), false, pool, phs, pops);
+                auto arr = [](const uint32_t* v, int cnt) {
+                    std::string a = "[";
+                    for (int i = 0; i < cnt; i++) a += (i ? "," : "") + std::to_string(v[i]);
+                    return a + "]";
+                };
+                for (size_t hi = 0; hi < phs.size(); hi++) {
+                    const TilePhase& h = phs[hi];
+                    s += hi ? ",{" : "{";
+                    s += "\"rb\":" + arr(h.rb, kPhaseEntries) + ",\"prb\":" + arr(h.prb, kPhaseEntries) + ",\"sb\":" +
+                         arr(h.sb, h.nslot_bits) + ",\"psb\":" + arr(h.psb, h.nslot_bits) + ",\"ops\":[";
+                    for (int oi = 0; oi < h.nops; oi++) {
+                        const PhaseOp& po = pops[size_t(h.first_op + oi)];
+                        s += oi ? ",{" : "{";
+                        s += "\"code\":" + std::to_string(po.code) + ",\"mat\":" + std::to_string(po.mat) +
+                             ",\"mask\":" + std::to_string(po.mask) + ",\"value\":" + std::to_string(po.value) +
+                             ",\"k\":" + std::to_string(po.k) + ",\"q\":[";
+                        for (int b = 0; b < po.k; b++) s += (b ? "," : "") + std::to_string(po.q[b]);
+                        s += "]}";
+                    }
+                    s += "]}";
+                }
+            }
             s += "]}";
         }
         s += "],\"pool\":[";

@@ -518,6 +518,7 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
                 p.raw.clear();
                 p.op_begin = int(tile_ops_host_.size());
                 tile_ops_host_.insert(tile_ops_host_.end(), p.ops.begin(), p.ops.end());
+                attach_phases(p);
                 s.pass = int(passes_.size());
                 passes_.push_back(std::move(p));
             }
@@ -529,6 +530,7 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
     for (auto& p : ps) {
         p.op_begin = int(tile_ops_host_.size());
         tile_ops_host_.insert(tile_ops_host_.end(), p.ops.begin(), p.ops.end());
+        attach_phases(p);
         Step s;
         s.pass = int(passes_.size());
         s.type = Operation::Dense;
@@ -536,6 +538,15 @@ void Executor::lower_segment(const std::vector<Operation>& ops, size_t begin, si
         passes_.push_back(std::move(p));
         steps_.push_back(std::move(s));
     }
+}
+
+void Executor::attach_phases(TilePass& p) {
+    const int m = int(p.qubits.size());
+    // complex128 only: on complex64 tiles the phases measured slower than one
+    // operation per sweep (FP32 arithmetic leaves shared memory less of the time).
+    if (!cfg_.phased || cfg_.c64 || cfg_.model || !phase_supported(m) || p.ops.empty()) return;
+    p.phase_begin = int(phases_host_.size());
+    p.nphases = plan_phases(p.ops, m, cfg_.c64, pool_host_, phases_host_, phase_ops_host_);
 }
 
 void Executor::record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y) {
@@ -721,6 +732,16 @@ void Executor::upload(cudaStream_t stream) {
                                    cudaMemcpyHostToDevice, stream),
                    "upload tile operations");
     }
+    if (!phases_host_.empty()) {
+        phases_.alloc(phases_host_.size() * sizeof(TilePhase), "tile phases");
+        phase_ops_.alloc(phase_ops_host_.size() * sizeof(PhaseOp), "tile phase operations");
+        cuda_check(cudaMemcpyAsync(phases_.p, phases_host_.data(), phases_host_.size() * sizeof(TilePhase),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload tile phases");
+        cuda_check(cudaMemcpyAsync(phase_ops_.p, phase_ops_host_.data(), phase_ops_host_.size() * sizeof(PhaseOp),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload tile phase operations");
+    }
     if (!fused_blocks_host_.empty()) {
         fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
         upool_.alloc(upool_host_.size() * sizeof(uint16_t), "fused block gate images");
@@ -792,8 +813,12 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
             const TilePass& p = passes_[size_t(s.pass)];
             if (rec) rec->begin(kcTile, step_bytes(si, b));
             const int m = int(p.qubits.size());
-            k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()), pool_.as<double2>(),
-                         p);
+            if (p.nphases > 0)
+                k::tile_pass_phased(b, p, phases_.as<TilePhase>() + p.phase_begin, p.nphases,
+                                    phase_ops_.as<PhaseOp>(), pool_.as<double2>());
+            else
+                k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()),
+                             pool_.as<double2>(), p);
             if (rec) rec->end();
             if (profile) {
                 cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");

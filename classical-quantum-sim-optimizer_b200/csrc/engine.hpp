@@ -11,6 +11,7 @@
 
 #include "compile.hpp"
 #include "kernels.hpp"
+#include "phased.hpp"
 #include "tile.hpp"
 
 namespace dq {
@@ -128,6 +129,10 @@ struct ExecConfig {
     // Learned pass-cost model: picks the fused plan of least predicted time
     // from the wide portfolio (kCostFusedPasses models only).
     const CostModel* pass_model = nullptr;
+    // Tile passes run in register phases (phased.hpp).  Passes planned with a
+    // tile-op cost model keep one operation per sweep, the form that model's
+    // per-operation costs were recorded on.
+    bool phased = true;
 };
 
 // How the fused plan of a segment was chosen: the portfolio's caps, the hand
@@ -199,7 +204,9 @@ class Executor {
     std::vector<TilePass> fused_src_;  // each fused pass's tile qubits and raw operations
     std::vector<FusedBlock> fused_blocks_host_;
     std::vector<uint16_t> upool_host_;
-    DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_;
+    std::vector<TilePhase> phases_host_;
+    std::vector<PhaseOp> phase_ops_host_;
+    DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_, phases_, phase_ops_;
     bool uploaded_ = false;
     ExecConfig cfg_;
     std::vector<int> widths_;
@@ -207,6 +214,7 @@ class Executor {
     void upload(cudaStream_t stream);
     void lower(const Operation& op, std::vector<Condition>& conds);
     void lower_segment(const std::vector<Operation>& ops, size_t begin, size_t end);
+    void attach_phases(TilePass& p);
 };
 
 }  // namespace dq

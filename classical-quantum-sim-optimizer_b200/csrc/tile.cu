@@ -1314,6 +1314,22 @@ __device__ __forceinline__ uint32_t expand_ins(uint32_t j, const Ins& s) {
     return j;
 }
 
+// acc += m * v as four fused multiply-adds (the products are not rounded
+// before the sum): a third fewer FP64 instructions than a rounded product plus
+// a separate sum.
+__device__ __forceinline__ void tmac(double2& acc, double2 m, double2 v) {
+    acc.x = fma(m.x, v.x, acc.x);
+    acc.x = fma(-m.y, v.y, acc.x);
+    acc.y = fma(m.x, v.y, acc.y);
+    acc.y = fma(m.y, v.x, acc.y);
+}
+__device__ __forceinline__ void tmac(float2& acc, float2 m, float2 v) {
+    acc.x = fmaf(m.x, v.x, acc.x);
+    acc.x = fmaf(-m.y, v.y, acc.x);
+    acc.y = fmaf(m.x, v.y, acc.y);
+    acc.y = fmaf(m.y, v.x, acc.y);
+}
+
 // 1- and 2-qubit dense matrices: matrix and offsets in registers, rows fully
 // unrolled so the 4 (16) complex products of a group are independent.
 template <typename V, int K>
@@ -1334,9 +1350,9 @@ __device__ void tile_dense_small(V* __restrict__ tile, const TileOp& op, int m, 
         for (int c = 0; c < D; c++) v[c] = tile[base | off[c]];
 #pragma unroll
         for (int r = 0; r < D; r++) {
-            V acc = dev::cmul(M[r * D], v[0]);
+            V acc = dev::czero<V>();
 #pragma unroll
-            for (int c = 1; c < D; c++) acc = dev::cadd(acc, dev::cmul(M[r * D + c], v[c]));
+            for (int c = 0; c < D; c++) tmac(acc, M[r * D + c], v[c]);
             tile[base | off[r]] = acc;
         }
     }
@@ -1360,7 +1376,7 @@ __device__ void tile_dense(V* __restrict__ tile, const TileOp& op, int m, const 
         for (int r = 0; r < D; r++) {
             V acc = dev::czero<V>();
 #pragma unroll
-            for (int c = 0; c < D; c++) acc = dev::cadd(acc, dev::cmul(dev::from_d2<V>(__ldg(mat + r * D + c)), v[c]));
+            for (int c = 0; c < D; c++) tmac(acc, dev::from_d2<V>(__ldg(mat + r * D + c)), v[c]);
             tile[base | op.offs[r]] = acc;  // row offset from the (cached) descriptor: no dynamic register index
         }
     }
@@ -1389,8 +1405,13 @@ __device__ void tile_apply(V* __restrict__ tile, const TileOp& op, int m, const 
                     tile[i0] = b;
                     tile[i1] = a;
                 } else {
-                    tile[i0] = dev::cadd(dev::cmul(u00, a), dev::cmul(u01, b));
-                    tile[i1] = dev::cadd(dev::cmul(u10, a), dev::cmul(u11, b));
+                    V p = dev::czero<V>(), q = dev::czero<V>();
+                    tmac(p, u00, a);
+                    tmac(p, u01, b);
+                    tmac(q, u10, a);
+                    tmac(q, u11, b);
+                    tile[i0] = p;
+                    tile[i1] = q;
                 }
             }
             break;
