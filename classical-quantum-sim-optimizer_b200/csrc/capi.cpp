@@ -880,29 +880,62 @@ int dq_tile_plan_dump(const char* json, size_t len, int tile_qubits, int fusion_
                      ",\"lowbit\":" + std::to_string(t.lowbit) + ",\"highbit\":" + std::to_string(t.highbit) +
                      ",\"mat\":" + std::to_string(t.mat) + "}";
             }
-            // The pass's register phases (complex128 swizzle), as the executor plans them.
+            // The pass's register phases (complex128 swizzle), decoded from the
+            // block the executor plans: offsets of every register entry and slot
+            // bit, and each operation with its matrix appended to the pool.
             s += "],\"phases\":[";
             if (phase_supported(int(p.qubits.size()))) {
-                std::vector<TilePhase> phs;
-                std::vector<PhaseOp> pops;
-                plan_phases(p.ops, int(p.qubits.size()), false, pool, phs, pops);
-                auto arr = [](const uint32_t* v, int cnt) {
+                std::vector<uint4> blk;
+                const int nph = plan_phases(p.ops, int(p.qubits.size()), false, pool, blk);
+                auto arr = [](const std::vector<uint32_t>& v) {
                     std::string a = "[";
-                    for (int i = 0; i < cnt; i++) a += (i ? "," : "") + std::to_string(v[i]);
+                    for (size_t i = 0; i < v.size(); i++) a += (i ? "," : "") + std::to_string(v[i]);
                     return a + "]";
                 };
-                for (size_t hi = 0; hi < phs.size(); hi++) {
-                    const TilePhase& h = phs[hi];
+                for (int hi = 0; hi < nph; hi++) {
+                    const uint4* h = &blk[size_t(hi) * kPhaseWords];
+                    const uint32_t rp[4] = {h[1].x, h[1].y, h[1].z, h[1].w};
+                    std::vector<uint32_t> rb, prb, sb, psb;
+                    for (int v = 0; v < kPhaseEntries; v++) {
+                        uint32_t o = 0, po = 0;
+                        for (int i = 0; i < kPhaseRegBits; i++)
+                            if ((v >> i) & 1) {
+                                o |= rp[i] & 0xFFFFu;
+                                po ^= rp[i] >> 16;
+                            }
+                        rb.push_back(o);
+                        prb.push_back(po);
+                    }
+                    for (uint32_t i = 0; i < h[0].z; i++) {
+                        const uint4 w = h[2 + i / 4];
+                        const uint32_t sp = (i % 4 == 0 ? w.x : i % 4 == 1 ? w.y : i % 4 == 2 ? w.z : w.w);
+                        sb.push_back(sp & 0xFFFFu);
+                        psb.push_back(sp >> 16);
+                    }
                     s += hi ? ",{" : "{";
-                    s += "\"rb\":" + arr(h.rb, kPhaseEntries) + ",\"prb\":" + arr(h.prb, kPhaseEntries) + ",\"sb\":" +
-                         arr(h.sb, h.nslot_bits) + ",\"psb\":" + arr(h.psb, h.nslot_bits) + ",\"ops\":[";
-                    for (int oi = 0; oi < h.nops; oi++) {
-                        const PhaseOp& po = pops[size_t(h.first_op + oi)];
+                    s += "\"rb\":" + arr(rb) + ",\"prb\":" + arr(prb) + ",\"sb\":" + arr(sb) + ",\"psb\":" +
+                         arr(psb) + ",\"ops\":[";
+                    for (uint32_t oi = 0; oi < h[0].y; oi++) {
+                        const uint4 o0 = blk[h[0].x + kPhaseOpWords * oi], o1 = blk[h[0].x + kPhaseOpWords * oi + 1];
+                        const int code = int(o0.x), k = int(o1.x);
+                        int count = 0;  // matrix words of the operation
+                        if (code < kPhX || code == kPhOne + 3) count = 4;
+                        else if (code >= kPhD2 && code < kPhD3) count = 16;
+                        else if (code >= kPhD3 && code < kPhSwap) count = 64;
+                        else if (code == kPhDiagEntry) count = 1;
+                        else if (code == kPhDiagFull) count = 1 << k;
+                        const size_t mat = pool.size();
+                        for (int e = 0; e < count; e++) {
+                            double2 v;
+                            std::memcpy(&v, &blk[o0.y + uint32_t(e)], sizeof v);
+                            pool.push_back(v);
+                        }
                         s += oi ? ",{" : "{";
-                        s += "\"code\":" + std::to_string(po.code) + ",\"mat\":" + std::to_string(po.mat) +
-                             ",\"mask\":" + std::to_string(po.mask) + ",\"value\":" + std::to_string(po.value) +
-                             ",\"k\":" + std::to_string(po.k) + ",\"q\":[";
-                        for (int b = 0; b < po.k; b++) s += (b ? "," : "") + std::to_string(po.q[b]);
+                        s += "\"code\":" + std::to_string(code) + ",\"mat\":" + std::to_string(mat) +
+                             ",\"mask\":" + std::to_string(o0.z) + ",\"value\":" + std::to_string(o0.w) +
+                             ",\"k\":" + std::to_string(k) + ",\"q\":[";
+                        for (int b = 0; b < k; b++)
+                            s += (b ? "," : "") + std::to_string(((b < 4 ? o1.y : o1.z) >> (8 * (b & 3))) & 0xFFu);
                         s += "]}";
                     }
                     s += "]}";

@@ -545,8 +545,12 @@ void Executor::attach_phases(TilePass& p) {
     // complex128 only: on complex64 tiles the phases measured slower than one
     // operation per sweep (FP32 arithmetic leaves shared memory less of the time).
     if (!cfg_.phased || cfg_.c64 || cfg_.model || !phase_supported(m) || p.ops.empty()) return;
-    p.phase_begin = int(phases_host_.size());
-    p.nphases = plan_phases(p.ops, m, cfg_.c64, pool_host_, phases_host_, phase_ops_host_);
+    std::vector<uint4> block;
+    p.nphases = plan_phases(p.ops, m, cfg_.c64, pool_host_, block);
+    p.phase_block = int(phase_blocks_.size());
+    p.phase_begin = int(phase_words_host_.size());
+    phase_words_host_.insert(phase_words_host_.end(), block.begin(), block.end());
+    phase_blocks_.push_back(std::move(block));
 }
 
 void Executor::record_costs(const k::Batch& b, std::vector<float>& X, std::vector<float>& y) {
@@ -732,15 +736,11 @@ void Executor::upload(cudaStream_t stream) {
                                    cudaMemcpyHostToDevice, stream),
                    "upload tile operations");
     }
-    if (!phases_host_.empty()) {
-        phases_.alloc(phases_host_.size() * sizeof(TilePhase), "tile phases");
-        phase_ops_.alloc(phase_ops_host_.size() * sizeof(PhaseOp), "tile phase operations");
-        cuda_check(cudaMemcpyAsync(phases_.p, phases_host_.data(), phases_host_.size() * sizeof(TilePhase),
+    if (!phase_words_host_.empty()) {
+        phase_words_.alloc(phase_words_host_.size() * sizeof(uint4), "tile phases");
+        cuda_check(cudaMemcpyAsync(phase_words_.p, phase_words_host_.data(), phase_words_host_.size() * sizeof(uint4),
                                    cudaMemcpyHostToDevice, stream),
                    "upload tile phases");
-        cuda_check(cudaMemcpyAsync(phase_ops_.p, phase_ops_host_.data(), phase_ops_host_.size() * sizeof(PhaseOp),
-                                   cudaMemcpyHostToDevice, stream),
-                   "upload tile phase operations");
     }
     if (!fused_blocks_host_.empty()) {
         fused_blocks_.alloc(fused_blocks_host_.size() * sizeof(FusedBlock), "fused block descriptors");
@@ -814,8 +814,8 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
             if (rec) rec->begin(kcTile, step_bytes(si, b));
             const int m = int(p.qubits.size());
             if (p.nphases > 0)
-                k::tile_pass_phased(b, p, phases_.as<TilePhase>() + p.phase_begin, p.nphases,
-                                    phase_ops_.as<PhaseOp>(), pool_.as<double2>());
+                k::tile_pass_phased(b, p, p.nphases, phase_blocks_[size_t(p.phase_block)],
+                                    phase_words_.as<uint4>() + p.phase_begin);
             else
                 k::tile_pass(b, nullptr, m, tile_ops_.as<TileOp>() + p.op_begin, int(p.ops.size()),
                              pool_.as<double2>(), p);

@@ -204,9 +204,9 @@ class Executor {
     std::vector<TilePass> fused_src_;  // each fused pass's tile qubits and raw operations
     std::vector<FusedBlock> fused_blocks_host_;
     std::vector<uint16_t> upool_host_;
-    std::vector<TilePhase> phases_host_;
-    std::vector<PhaseOp> phase_ops_host_;
-    DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_, phases_, phase_ops_;
+    std::vector<std::vector<uint4>> phase_blocks_;  // per phased pass (host copies: launch arguments)
+    std::vector<uint4> phase_words_host_;           // the same blocks back to back (device copy)
+    DevMem pool_, tile_ops_, fused_blocks_, upool_, norm_tiles_, norm_states_, phase_words_;
     bool uploaded_ = false;
     ExecConfig cfg_;
     std::vector<int> widths_;

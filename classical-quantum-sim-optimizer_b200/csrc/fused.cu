@@ -548,16 +548,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                         put_split2(x, off, out2(i));
                     }
                 } else {
+                    // Unscaled outputs into the stage; the quarter's |re|^2 and |im|^2
+                    // summed in FP32 pairs (8 terms), then added to the thread's FP64
+                    // partial of the tile norm.
+                    const uint64_t inv2 = pack2(__float_as_uint(kInvScale), __float_as_uint(kInvScale));
+                    uint64_t nq = 0;
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
                         const uint32_t off = cpart ^ ((nbw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                        uint32_t ur, ui;
-                        asm("mov.b64 {%0, %1}, %2;" : "=r"(ur), "=r"(ui) : "l"(out2(i)));
-                        const float re = __uint_as_float(ur) * kInvScale;
-                        const float im = __uint_as_float(ui) * kInvScale;
-                        *reinterpret_cast<float2*>(x + off) = make_float2(re, im);
-                        norm_acc += double(re) * re + double(im) * im;
+                        const uint64_t v = mul2(out2(i), inv2);
+                        *reinterpret_cast<uint64_t*>(x + off) = v;
+                        asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(nq) : "l"(v));
                     }
+                    uint32_t n0, n1;
+                    asm("mov.b64 {%0, %1}, %2;" : "=r"(n0), "=r"(n1) : "l"(nq));
+                    norm_acc += double(__uint_as_float(n0)) + double(__uint_as_float(n1));
                 }
             }
         }

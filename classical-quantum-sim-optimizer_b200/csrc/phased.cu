@@ -34,7 +34,7 @@ void op_masks(const TileOp& t, uint32_t& T, uint32_t& S) {
     }
 }
 
-// Register index (0..3) of tile bit `bit` among the phase's register qubits R (ascending).
+// Register index of tile bit `bit` among the phase's register qubits R (ascending).
 int reg_of(const int R[kPhaseRegBits], int bit) {
     for (int i = 0; i < kPhaseRegBits; i++)
         if (R[i] == bit) return i;
@@ -43,17 +43,15 @@ int reg_of(const int R[kPhaseRegBits], int bit) {
 }
 
 // Dense matrix of 2 or 3 qubits re-laid out so that matrix index bit j sits on
-// the op's j-th lowest register qubit; sets the phase code, returns the pool
-// offset.
-int canonical_dense(const TileOp& t, const int R[kPhaseRegBits], const std::vector<double2>& src_pool,
-                    std::vector<double2>& pool, int& code) {
+// the op's j-th lowest register qubit; sets the phase code.
+std::vector<double2> canonical_dense(const TileOp& t, const int R[kPhaseRegBits], const std::vector<double2>& pool,
+                                     int& code) {
     const int k = t.k, D = 1 << k;
     int reg[3] = {0, 0, 0};  // register index of matrix bit (k-1-b) = op qubit q[b]
     for (int b = 0; b < k; b++) reg[b] = reg_of(R, t.q[b]);
-    // Canonical order: matrix bit j <-> the j-th smallest register index of the op.
     int sorted[3] = {reg[0], reg[1], reg[2]};
     std::sort(sorted, sorted + k);
-    // y(x): original matrix index of canonical index x.
+    // Original matrix index of canonical index x.
     auto orig = [&](int x) {
         int y = 0;
         for (int b = 0; b < k; b++) {
@@ -62,26 +60,38 @@ int canonical_dense(const TileOp& t, const int R[kPhaseRegBits], const std::vect
         }
         return y;
     };
-    if (k == 2) code = kPhD2 + phase_pair(sorted[1], sorted[0]);
-    if (k == 3) code = kPhD3 + phase_triple(sorted[2], sorted[1], sorted[0]);
-    const int off = int(pool.size());
+    code = k == 2 ? kPhD2 + phase_pair(sorted[1], sorted[0]) : kPhD3 + phase_triple(sorted[2], sorted[1], sorted[0]);
+    std::vector<double2> out;
     for (int x = 0; x < D; x++)
-        for (int xc = 0; xc < D; xc++) pool.push_back(src_pool[size_t(t.mat) + size_t(orig(x)) * D + orig(xc)]);
-    return off;
+        for (int xc = 0; xc < D; xc++) out.push_back(pool[size_t(t.mat) + size_t(orig(x)) * D + orig(xc)]);
+    return out;
 }
+
+struct PendingOp {
+    int code = 0, k = 0;
+    uint32_t mask = 0, value = 0;
+    uint8_t q[8] = {};
+    std::vector<double2> mat;
+};
+
+struct PendingPhase {
+    int R[kPhaseRegBits] = {};
+    std::vector<int> ord;  // slot bit i -> tile bit
+    std::vector<PendingOp> ops;
+};
+
+uint4 word(uint32_t x, uint32_t y, uint32_t z, uint32_t w) { return make_uint4(x, y, z, w); }
 
 }  // namespace
 
-int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, std::vector<double2>& pool,
-                std::vector<TilePhase>& phases, std::vector<PhaseOp>& phase_ops) {
+int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, const std::vector<double2>& pool,
+                std::vector<uint4>& block) {
     const int N = int(ops.size());
     const int g = c64 ? 4 : 3;
     std::vector<uint32_t> T(N), S(N);
     for (int i = 0; i < N; i++) op_masks(ops[i], T[i], S[i]);
-    // Matrices are copied out of the pool while it grows: read a snapshot.
-    const std::vector<double2> src = pool;
     std::vector<char> done(N, 0);
-    int left = N, count = 0;
+    int left = N;
     // Operations a phase with register qubits R takes: one scan in pass order;
     // an operation joins when its targets lie in R and it commutes with every
     // operation skipped before it, and a skipped operation blocks what
@@ -101,6 +111,7 @@ int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, std::vector<dou
         }
     };
     const uint32_t all = m >= 32 ? ~0u : (1u << m) - 1;
+    std::vector<PendingPhase> phases;
     while (left > 0) {
         // Candidate register sets: the targets of each operation that is ready
         // (commutes with every earlier one left), widened to kPhaseRegBits
@@ -117,16 +128,16 @@ int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, std::vector<dou
             }
         }
         std::vector<uint32_t> cands;
-        auto widen = [&](uint32_t R, uint32_t pool_bits, auto&& self) -> void {
+        auto widen = [&](uint32_t R, auto&& self) -> void {
             if (popcount32(R) >= kPhaseRegBits) {
                 cands.push_back(R);
                 return;
             }
             for (int b = 0; b < m; b++)
-                if (((pool_bits >> b) & 1) && !((R >> b) & 1)) self(R | (1u << b), pool_bits, self);
+                if (((all >> b) & 1) && !((R >> b) & 1)) self(R | (1u << b), self);
         };
         for (uint32_t x : ready)
-            if (x && popcount32(x) <= kPhaseRegBits) widen(x, all, widen);
+            if (x && popcount32(x) <= kPhaseRegBits) widen(x, widen);
         std::sort(cands.begin(), cands.end());
         cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
         if (cands.empty()) cands.push_back(0);  // only diagonal operations are ready
@@ -143,101 +154,133 @@ int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, std::vector<dou
         // Pad the register qubits with unused tile bits, highest first.
         for (int b = m - 1; b >= 0 && popcount32(R) < kPhaseRegBits; b--)
             if (!((R >> b) & 1)) R |= 1u << b;
-        int Rb[kPhaseRegBits], nr = 0;
-        for (int b = 0; b < m; b++)
-            if ((R >> b) & 1) Rb[nr++] = b;
+        PendingPhase ph;
+        for (int b = 0, nr = 0; b < m; b++)
+            if ((R >> b) & 1) ph.R[nr++] = b;
         // Slot bits: first one tile bit of each residue mod g (lowest first), so
         // the 2^g lanes of a shared-memory wavefront hit distinct bank groups;
         // then the other free bits ascending.
-        std::vector<int> ord;
         std::vector<char> used(size_t(m), 0);
         for (int cls = 0; cls < g; cls++)
             for (int b = cls; b < m; b += g)
                 if (!((R >> b) & 1)) {
-                    ord.push_back(b);
+                    ph.ord.push_back(b);
                     used[size_t(b)] = 1;
                     break;
                 }
         for (int b = 0; b < m; b++)
-            if (!((R >> b) & 1) && !used[size_t(b)]) ord.push_back(b);
-        TilePhase ph;
-        ph.first_op = int(phase_ops.size());
-        ph.nops = int(members.size());
-        ph.nslot_bits = int(ord.size());
-        for (int v = 0; v < kPhaseEntries; v++) {
-            uint32_t o = 0;
-            for (int i = 0; i < kPhaseRegBits; i++)
-                if ((v >> i) & 1) o |= 1u << Rb[i];
-            ph.rb[v] = o;
-            ph.prb[v] = phase_swizzle(o, g);
-        }
-        for (size_t i = 0; i < ord.size(); i++) {
-            ph.sb[i] = 1u << ord[i];
-            ph.psb[i] = phase_swizzle(ph.sb[i], g);
-        }
+            if (!((R >> b) & 1) && !used[size_t(b)]) ph.ord.push_back(b);
         for (int i : members) {
             const TileOp& t = ops[size_t(i)];
-            PhaseOp p;
+            PendingOp p;
+            auto copy_mat = [&](int count) {
+                for (int e = 0; e < count; e++) p.mat.push_back(pool[size_t(t.mat) + size_t(e)]);
+            };
             switch (t.type) {
                 case TileOp::kOne:
-                case TileOp::kX: {
-                    const int r = reg_of(Rb, __builtin_ctz(t.tbit));
-                    p.code = (t.type == TileOp::kOne ? kPhOne : kPhX) + r;
-                    p.mat = t.mat;
+                case TileOp::kX:
+                    p.code = (t.type == TileOp::kOne ? kPhOne : kPhX) + reg_of(ph.R, __builtin_ctz(t.tbit));
+                    if (t.type == TileOp::kOne) copy_mat(4);
                     p.mask = S[size_t(i)] & ~t.tbit;
                     p.value = t.fixed;
                     break;
-                }
-                case TileOp::kSwap: {
-                    const int lo = reg_of(Rb, __builtin_ctz(t.lowbit)), hi = reg_of(Rb, __builtin_ctz(t.highbit));
-                    p.code = kPhSwap + phase_pair(hi, lo);
+                case TileOp::kSwap:
+                    p.code = kPhSwap + phase_pair(reg_of(ph.R, __builtin_ctz(t.highbit)),
+                                                  reg_of(ph.R, __builtin_ctz(t.lowbit)));
                     p.mask = S[size_t(i)] & ~(t.lowbit | t.highbit);
                     p.value = t.fixed;
                     break;
-                }
                 case TileOp::kDiagEntry:
                     p.code = kPhDiagEntry;
-                    p.mat = t.mat;
+                    copy_mat(1);
                     p.mask = S[size_t(i)];
                     p.value = t.fixed;
                     break;
                 case TileOp::kDiagFull:
                     p.code = kPhDiagFull;
-                    p.mat = t.mat;
                     p.k = t.k;
                     for (int b = 0; b < t.k; b++) p.q[b] = uint8_t(t.q[b]);
+                    copy_mat(1 << t.k);
                     break;
                 case TileOp::kDense:
                     if (t.k == 1) {
-                        p.code = kPhOne + reg_of(Rb, t.q[0]);
-                        p.mat = t.mat;  // row-major 2x2: u00, u01, u10, u11
+                        p.code = kPhOne + reg_of(ph.R, t.q[0]);
+                        copy_mat(4);  // row-major 2x2: u00, u01, u10, u11
                     } else {
-                        p.mat = canonical_dense(t, Rb, src, pool, p.code);
+                        p.mat = canonical_dense(t, ph.R, pool, p.code);
                     }
                     break;
                 default: fail(kValueError, "tile operation without a phase form");
             }
-            phase_ops.push_back(p);
+            ph.ops.push_back(std::move(p));
             done[size_t(i)] = 1;
         }
         left -= int(members.size());
-        phases.push_back(ph);
-        count++;
+        phases.push_back(std::move(ph));
     }
-    return count;
+    // Assemble the block: phase headers, then operations, then matrices.
+    const size_t nph = phases.size();
+    size_t op_word = nph * kPhaseWords;
+    block.assign(op_word + size_t(N) * kPhaseOpWords, make_uint4(0, 0, 0, 0));
+    for (size_t pi = 0; pi < nph; pi++) {
+        const PendingPhase& ph = phases[pi];
+        uint4* h = &block[pi * kPhaseWords];
+        h[0] = word(uint32_t(op_word), uint32_t(ph.ops.size()), uint32_t(ph.ord.size()), 0);
+        uint32_t rp[4] = {0, 0, 0, 0}, sp[kPhaseMaxSlotBits] = {};
+        for (int i = 0; i < kPhaseRegBits; i++) rp[i] = (1u << ph.R[i]) | (phase_swizzle(1u << ph.R[i], g) << 16);
+        for (size_t i = 0; i < ph.ord.size(); i++)
+            sp[i] = (1u << ph.ord[i]) | (phase_swizzle(1u << ph.ord[i], g) << 16);
+        h[1] = word(rp[0], rp[1], rp[2], rp[3]);
+        for (int q4 = 0; q4 < 4; q4++) h[2 + q4] = word(sp[4 * q4], sp[4 * q4 + 1], sp[4 * q4 + 2], sp[4 * q4 + 3]);
+        for (const PendingOp& p : ph.ops) {
+            uint32_t q0 = 0, q1 = 0;
+            for (int b = 0; b < 4; b++) {
+                q0 |= uint32_t(p.q[b]) << (8 * b);
+                q1 |= uint32_t(p.q[4 + b]) << (8 * b);
+            }
+            block[op_word] = word(uint32_t(p.code), p.mat.empty() ? 0u : uint32_t(block.size()), p.mask, p.value);
+            block[op_word + 1] = word(uint32_t(p.k), q0, q1, 0);
+            op_word += kPhaseOpWords;
+            for (const double2& v : p.mat) {
+                uint4 u;
+                std::memcpy(&u, &v, sizeof u);
+                block.push_back(u);
+            }
+        }
+    }
+    return int(nph);
 }
 
 namespace k {
 namespace {
 
 constexpr int kPhaseThreads = 256;
+constexpr int E = kPhaseEntries;
 
 struct PhaseQubits {
     int m;
     int q[20];
 };
 
-constexpr int E = kPhaseEntries;
+// The block as a launch argument (constant bank).
+struct PhasedArgs {
+    uint4 q[kPhaseParamWords];
+};
+
+// Word sources: the block in device memory, or the launch argument.
+struct DevWords {
+    const uint4* __restrict__ w;
+    __device__ __forceinline__ uint4 operator()(int i) const { return __ldg(w + i); }
+};
+struct ArgWords {
+    const PhasedArgs* a;
+    __device__ __forceinline__ uint4 operator()(int i) const { return a->q[i]; }
+};
+
+template <typename V>
+__device__ __forceinline__ V mat_of(uint4 u) {
+    return dev::from_d2<V>(make_double2(__hiloint2double(int(u.y), int(u.x)), __hiloint2double(int(u.w), int(u.z))));
+}
 
 // acc += m * v as four fused multiply-adds (the products are not rounded
 // before the sum).
@@ -254,63 +297,67 @@ __device__ __forceinline__ void cmac(float2& acc, float2 m, float2 v) {
     acc.y = fmaf(m.y, v.x, acc.y);
 }
 
-template <typename V, int T>
-__device__ __forceinline__ void ph_one(V (&a)[E], const PhaseOp& op, const double2* __restrict__ pool,
-                                       uint32_t base, const TilePhase* __restrict__ P) {
-    const V u00 = dev::from_d2<V>(__ldg(pool + op.mat)), u01 = dev::from_d2<V>(__ldg(pool + op.mat + 1));
-    const V u10 = dev::from_d2<V>(__ldg(pool + op.mat + 2)), u11 = dev::from_d2<V>(__ldg(pool + op.mat + 3));
+// One operation of a phase: its first matrix word and its condition.
+struct Op {
+    int code, mat;
+    uint32_t mask, value;
+};
+
+template <typename V, int T, class W>
+__device__ __forceinline__ void ph_one(V (&a)[E], const W& w, const Op& op, uint32_t base, const uint32_t (&rb)[E]) {
+    const V u00 = mat_of<V>(w(op.mat)), u01 = mat_of<V>(w(op.mat + 1));
+    const V u10 = mat_of<V>(w(op.mat + 2)), u11 = mat_of<V>(w(op.mat + 3));
 #pragma unroll
     for (int v = 0; v < E; v++) {
         if (v & (1 << T)) continue;
-        const int w = v | (1 << T);
-        if (op.mask && ((base | __ldg(&P->rb[v])) & op.mask) != op.value) continue;
-        const V x = a[v], y = a[w];
+        const int u = v | (1 << T);
+        if (op.mask && ((base | rb[v]) & op.mask) != op.value) continue;
+        const V x = a[v], y = a[u];
         V p = dev::czero<V>(), q = dev::czero<V>();
         cmac(p, u00, x);
         cmac(p, u01, y);
         cmac(q, u10, x);
         cmac(q, u11, y);
         a[v] = p;
-        a[w] = q;
+        a[u] = q;
     }
 }
 
 template <typename V, int T>
-__device__ __forceinline__ void ph_x(V (&a)[E], const PhaseOp& op, uint32_t base, const TilePhase* __restrict__ P) {
+__device__ __forceinline__ void ph_x(V (&a)[E], const Op& op, uint32_t base, const uint32_t (&rb)[E]) {
 #pragma unroll
     for (int v = 0; v < E; v++) {
         if (v & (1 << T)) continue;
-        const int w = v | (1 << T);
-        if (op.mask && ((base | __ldg(&P->rb[v])) & op.mask) != op.value) continue;
+        const int u = v | (1 << T);
+        if (op.mask && ((base | rb[v]) & op.mask) != op.value) continue;
         const V x = a[v];
-        a[v] = a[w];
-        a[w] = x;
+        a[v] = a[u];
+        a[u] = x;
     }
 }
 
 template <typename V, int H, int L>
-__device__ __forceinline__ void ph_swap(V (&a)[E], const PhaseOp& op, uint32_t base, const TilePhase* __restrict__ P) {
+__device__ __forceinline__ void ph_swap(V (&a)[E], const Op& op, uint32_t base, const uint32_t (&rb)[E]) {
 #pragma unroll
     for (int v = 0; v < E; v++) {
         if (v & ((1 << H) | (1 << L))) continue;
         const int v01 = v | (1 << L), v10 = v | (1 << H);
-        if (op.mask && ((base | __ldg(&P->rb[v01])) & op.mask) != op.value) continue;
+        if (op.mask && ((base | rb[v01]) & op.mask) != op.value) continue;
         const V x = a[v01];
         a[v01] = a[v10];
         a[v10] = x;
     }
 }
 
-// Dense matrix of k = 2 or 3 qubits on register qubits Q[0] > ... > Q[k-1]
-// (matrix index bit k-1-b on Q[b]), applied to every group of the other
-// register qubits.  Rows are loaded one at a time; all groups' outputs are
+// Dense matrix of K = 2 or 3 qubits on register qubits Q0 > Q1 (> Q2)
+// (matrix index bit K-1-b on the b-th), applied to every group of the other
+// register qubits.  Rows are read one at a time; all groups' outputs are
 // formed before any is written back.
-template <typename V, int K, int Q0, int Q1, int Q2>
-__device__ __forceinline__ void ph_dense(V (&a)[E], const PhaseOp& op, const double2* __restrict__ pool) {
+template <typename V, int K, int Q0, int Q1, int Q2, class W>
+__device__ __forceinline__ void ph_dense(V (&a)[E], const W& w, const Op& op) {
     constexpr int D = 1 << K;
     constexpr int QM = (1 << Q0) | (1 << Q1) | (K == 3 ? (1 << Q2) : 0);
-    constexpr int G = E / D;  // groups
-    const double2* M = pool + op.mat;
+    constexpr int G = E / D;
     auto entry = [](int g0, int c) {
         return K == 3 ? (g0 | (((c >> 2) & 1) << Q0) | (((c >> 1) & 1) << Q1) | ((c & 1) << Q2))
                       : (g0 | (((c >> 1) & 1) << Q0) | ((c & 1) << Q1));
@@ -327,7 +374,7 @@ __device__ __forceinline__ void ph_dense(V (&a)[E], const PhaseOp& op, const dou
     for (int r = 0; r < D; r++) {
         V mr[D];
 #pragma unroll
-        for (int c = 0; c < D; c++) mr[c] = dev::from_d2<V>(__ldg(M + r * D + c));
+        for (int c = 0; c < D; c++) mr[c] = mat_of<V>(w(op.mat + r * D + c));
 #pragma unroll
         for (int gi = 0; gi < G; gi++) {
             V acc = dev::czero<V>();
@@ -340,61 +387,64 @@ __device__ __forceinline__ void ph_dense(V (&a)[E], const PhaseOp& op, const dou
     for (int v = 0; v < E; v++) a[v] = out[v];
 }
 
-template <typename V>
-__device__ __forceinline__ void ph_diag_entry(V (&a)[E], const PhaseOp& op, const double2* __restrict__ pool,
-                                              uint32_t base, const TilePhase* __restrict__ P) {
-    const V d = dev::from_d2<V>(__ldg(pool + op.mat));
+template <typename V, class W>
+__device__ __forceinline__ void ph_diag_entry(V (&a)[E], const W& w, const Op& op, uint32_t base,
+                                              const uint32_t (&rb)[E]) {
+    const V d = mat_of<V>(w(op.mat));
 #pragma unroll
     for (int v = 0; v < E; v++)
-        if (((base | __ldg(&P->rb[v])) & op.mask) == op.value) a[v] = dev::cmul(a[v], d);
+        if (((base | rb[v]) & op.mask) == op.value) a[v] = dev::cmul(a[v], d);
 }
 
-template <typename V>
-__device__ __forceinline__ void ph_diag_full(V (&a)[E], const PhaseOp& op, const double2* __restrict__ pool,
-                                             uint32_t base, const TilePhase* __restrict__ P) {
+// A full diagonal: `extra` = {k, table qubits 0-3 and 4-7 as bytes}.
+template <typename V, class W>
+__device__ __forceinline__ void ph_diag_full(V (&a)[E], const W& w, const Op& op, uint4 extra, uint32_t base,
+                                             const uint32_t (&rb)[E]) {
+    const int k = int(extra.x);
 #pragma unroll
     for (int v = 0; v < E; v++) {
-        const uint32_t full = base | __ldg(&P->rb[v]);
+        const uint32_t full = base | rb[v];
         uint32_t jj = 0;
 #pragma unroll
         for (int b = 0; b < 8; b++)
-            if (b < op.k) jj = (jj << 1) | ((full >> op.q[b]) & 1u);
-        a[v] = dev::cmul(a[v], dev::from_d2<V>(__ldg(pool + op.mat + jj)));
+            if (b < k) jj = (jj << 1) | ((full >> (((b < 4 ? extra.y : extra.z) >> (8 * (b & 3))) & 0xFFu)) & 1u);
+        a[v] = dev::cmul(a[v], mat_of<V>(w(op.mat + int(jj))));
     }
 }
 
-template <typename V>
-__device__ __forceinline__ void ph_apply(V (&a)[E], const PhaseOp& op, const double2* __restrict__ pool,
-                                         uint32_t base, const TilePhase* __restrict__ P) {
+template <typename V, class W>
+__device__ __forceinline__ void ph_apply(V (&a)[E], const W& w, int opw, uint32_t base, const uint32_t (&rb)[E]) {
+    const uint4 h = w(opw);
+    const Op op{int(h.x), int(h.y), h.z, h.w};
     switch (op.code) {
-        case kPhOne + 0: ph_one<V, 0>(a, op, pool, base, P); break;
-        case kPhOne + 1: ph_one<V, 1>(a, op, pool, base, P); break;
-        case kPhOne + 2: ph_one<V, 2>(a, op, pool, base, P); break;
-        case kPhX + 0: ph_x<V, 0>(a, op, base, P); break;
-        case kPhX + 1: ph_x<V, 1>(a, op, base, P); break;
-        case kPhX + 2: ph_x<V, 2>(a, op, base, P); break;
-        case kPhD2 + phase_pair(1, 0): ph_dense<V, 2, 1, 0, 0>(a, op, pool); break;
-        case kPhD2 + phase_pair(2, 0): ph_dense<V, 2, 2, 0, 0>(a, op, pool); break;
-        case kPhD2 + phase_pair(2, 1): ph_dense<V, 2, 2, 1, 0>(a, op, pool); break;
-        case kPhD3 + phase_triple(2, 1, 0): ph_dense<V, 3, 2, 1, 0>(a, op, pool); break;
-        case kPhSwap + phase_pair(1, 0): ph_swap<V, 1, 0>(a, op, base, P); break;
-        case kPhSwap + phase_pair(2, 0): ph_swap<V, 2, 0>(a, op, base, P); break;
-        case kPhSwap + phase_pair(2, 1): ph_swap<V, 2, 1>(a, op, base, P); break;
+        case kPhOne + 0: ph_one<V, 0>(a, w, op, base, rb); break;
+        case kPhOne + 1: ph_one<V, 1>(a, w, op, base, rb); break;
+        case kPhOne + 2: ph_one<V, 2>(a, w, op, base, rb); break;
+        case kPhX + 0: ph_x<V, 0>(a, op, base, rb); break;
+        case kPhX + 1: ph_x<V, 1>(a, op, base, rb); break;
+        case kPhX + 2: ph_x<V, 2>(a, op, base, rb); break;
+        case kPhD2 + phase_pair(1, 0): ph_dense<V, 2, 1, 0, 0>(a, w, op); break;
+        case kPhD2 + phase_pair(2, 0): ph_dense<V, 2, 2, 0, 0>(a, w, op); break;
+        case kPhD2 + phase_pair(2, 1): ph_dense<V, 2, 2, 1, 0>(a, w, op); break;
+        case kPhD3 + phase_triple(2, 1, 0): ph_dense<V, 3, 2, 1, 0>(a, w, op); break;
+        case kPhSwap + phase_pair(1, 0): ph_swap<V, 1, 0>(a, op, base, rb); break;
+        case kPhSwap + phase_pair(2, 0): ph_swap<V, 2, 0>(a, op, base, rb); break;
+        case kPhSwap + phase_pair(2, 1): ph_swap<V, 2, 1>(a, op, base, rb); break;
 #if DQ_PHASE_REG_BITS == 4
-        case kPhOne + 3: ph_one<V, 3>(a, op, pool, base, P); break;
-        case kPhX + 3: ph_x<V, 3>(a, op, base, P); break;
-        case kPhD2 + phase_pair(3, 0): ph_dense<V, 2, 3, 0, 0>(a, op, pool); break;
-        case kPhD2 + phase_pair(3, 1): ph_dense<V, 2, 3, 1, 0>(a, op, pool); break;
-        case kPhD2 + phase_pair(3, 2): ph_dense<V, 2, 3, 2, 0>(a, op, pool); break;
-        case kPhD3 + phase_triple(3, 1, 0): ph_dense<V, 3, 3, 1, 0>(a, op, pool); break;
-        case kPhD3 + phase_triple(3, 2, 0): ph_dense<V, 3, 3, 2, 0>(a, op, pool); break;
-        case kPhD3 + phase_triple(3, 2, 1): ph_dense<V, 3, 3, 2, 1>(a, op, pool); break;
-        case kPhSwap + phase_pair(3, 0): ph_swap<V, 3, 0>(a, op, base, P); break;
-        case kPhSwap + phase_pair(3, 1): ph_swap<V, 3, 1>(a, op, base, P); break;
-        case kPhSwap + phase_pair(3, 2): ph_swap<V, 3, 2>(a, op, base, P); break;
+        case kPhOne + 3: ph_one<V, 3>(a, w, op, base, rb); break;
+        case kPhX + 3: ph_x<V, 3>(a, op, base, rb); break;
+        case kPhD2 + phase_pair(3, 0): ph_dense<V, 2, 3, 0, 0>(a, w, op); break;
+        case kPhD2 + phase_pair(3, 1): ph_dense<V, 2, 3, 1, 0>(a, w, op); break;
+        case kPhD2 + phase_pair(3, 2): ph_dense<V, 2, 3, 2, 0>(a, w, op); break;
+        case kPhD3 + phase_triple(3, 1, 0): ph_dense<V, 3, 3, 1, 0>(a, w, op); break;
+        case kPhD3 + phase_triple(3, 2, 0): ph_dense<V, 3, 3, 2, 0>(a, w, op); break;
+        case kPhD3 + phase_triple(3, 2, 1): ph_dense<V, 3, 3, 2, 1>(a, w, op); break;
+        case kPhSwap + phase_pair(3, 0): ph_swap<V, 3, 0>(a, op, base, rb); break;
+        case kPhSwap + phase_pair(3, 1): ph_swap<V, 3, 1>(a, op, base, rb); break;
+        case kPhSwap + phase_pair(3, 2): ph_swap<V, 3, 2>(a, op, base, rb); break;
 #endif
-        case kPhDiagEntry: ph_diag_entry<V>(a, op, pool, base, P); break;
-        case kPhDiagFull: ph_diag_full<V>(a, op, pool, base, P); break;
+        case kPhDiagEntry: ph_diag_entry<V>(a, w, op, base, rb); break;
+        case kPhDiagFull: ph_diag_full<V>(a, w, op, w(opw + 1), base, rb); break;
         default: break;
     }
 }
@@ -408,10 +458,11 @@ __device__ __forceinline__ uint32_t swz(uint32_t e) {
     return e ^ (f & ((1u << g) - 1));
 }
 
-template <typename V>
-__global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V) == 8 ? 2 : 1)
-    k_tile_phased(V* __restrict__ s, int n, int m, PhaseQubits tq, const TilePhase* __restrict__ phases, int nphases,
-                  const PhaseOp* __restrict__ ops, const double2* __restrict__ pool, uint64_t total_tiles) {
+// The persistent pass: each CTA loads a tile into (swizzled) shared memory,
+// runs the phases and writes the tile back.
+template <typename V, class W>
+__device__ __forceinline__ void phased_body(V* __restrict__ s, int n, int m, const PhaseQubits& tq, int nphases,
+                                            uint64_t total_tiles, const W& w) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
     const int lb = m < 6 ? m : 6;
@@ -457,30 +508,64 @@ __global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V)
         }
         __syncthreads();
         for (int p = 0; p < nphases; p++) {
-            const TilePhase* __restrict__ P = phases + p;
-            const int nsb = __ldg(&P->nslot_bits), first = __ldg(&P->first_op), nops = __ldg(&P->nops);
+            const uint4 h0 = w(kPhaseWords * p), h1 = w(kPhaseWords * p + 1);
+            const int first = int(h0.x), nops = int(h0.y), nsb = int(h0.z);
+            const uint32_t rp[4] = {h1.x, h1.y, h1.z, h1.w};
+            // Register entry v: tile offset and swizzled offset (ORs / XORs of
+            // its register qubits' bits).
+            uint32_t rb[E], prb[E];
+#pragma unroll
+            for (int v = 0; v < E; v++) {
+                uint32_t o = 0, po = 0;
+#pragma unroll
+                for (int i = 0; i < kPhaseRegBits; i++)
+                    if ((v >> i) & 1) {
+                        o |= rp[i] & 0xFFFFu;
+                        po ^= rp[i] >> 16;
+                    }
+                rb[v] = o;
+                prb[v] = po;
+            }
             for (uint32_t sl = threadIdx.x; sl < slots; sl += blockDim.x) {
                 uint32_t base = 0, pbase = 0;
-                for (int i = 0; i < nsb; i++)
-                    if ((sl >> i) & 1u) {
-                        base |= __ldg(&P->sb[i]);
-                        pbase ^= __ldg(&P->psb[i]);
-                    }
+#pragma unroll
+                for (int q4 = 0; q4 < kPhaseMaxSlotBits / 4; q4++) {
+                    if (4 * q4 >= nsb) break;
+                    const uint4 sw = w(kPhaseWords * p + 2 + q4);
+                    const uint32_t spk[4] = {sw.x, sw.y, sw.z, sw.w};
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        if (4 * q4 + j < nsb && ((sl >> (4 * q4 + j)) & 1u)) {
+                            base |= spk[j] & 0xFFFFu;
+                            pbase ^= spk[j] >> 16;
+                        }
+                }
                 V a[E];
 #pragma unroll
-                for (int v = 0; v < E; v++) a[v] = tile[pbase ^ __ldg(&P->prb[v])];
-                for (int o = 0; o < nops; o++) {
-                    const PhaseOp op = ops[first + o];
-                    ph_apply<V>(a, op, pool, base, P);
-                }
+                for (int v = 0; v < E; v++) a[v] = tile[pbase ^ prb[v]];
+                for (int o = 0; o < nops; o++) ph_apply<V>(a, w, first + kPhaseOpWords * o, base, rb);
 #pragma unroll
-                for (int v = 0; v < E; v++) tile[pbase ^ __ldg(&P->prb[v])] = a[v];
+                for (int v = 0; v < E; v++) tile[pbase ^ prb[v]] = a[v];
             }
             __syncthreads();
         }
         for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) gp[lo_tab[e & lmask] | hi_tab[e >> lb]] = tile[swz<V>(e)];
         __syncthreads();
     }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V) == 8 ? 2 : 1)
+    k_tile_phased_dev(V* __restrict__ s, int n, int m, PhaseQubits tq, int nphases, uint64_t total_tiles,
+                      const uint4* __restrict__ block) {
+    phased_body<V>(s, n, m, tq, nphases, total_tiles, DevWords{block});
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V) == 8 ? 2 : 1)
+    k_tile_phased_arg(V* __restrict__ s, int n, int m, PhaseQubits tq, int nphases, uint64_t total_tiles,
+                      const __grid_constant__ PhasedArgs args) {
+    phased_body<V>(s, n, m, tq, nphases, total_tiles, ArgWords{&args});
 }
 
 int sm_count() {
@@ -494,42 +579,56 @@ int sm_count() {
     return c;
 }
 
+template <typename Kernel>
+uint64_t configure(Kernel kernel, size_t smem, size_t& configured, uint64_t total) {
+    if (smem > configured) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxShared));
+        configured = smem;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPhaseThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    return std::min<uint64_t>(total, uint64_t(sm_count()) * per_sm);
+}
+
 template <typename V>
-void launch_phased(const Batch& b, const TilePass& hp, const TilePhase* phases, int nphases, const PhaseOp* ops,
-                   const double2* pool) {
+void launch_phased(const Batch& b, const TilePass& hp, int nphases, const std::vector<uint4>& block,
+                   const uint4* block_dev) {
     const int m = int(hp.qubits.size());
     if (!phase_supported(m)) fail(kValueError, "tile pass too small or too large for register phases");
     PhaseQubits tq{};
     tq.m = m;
     for (int i = 0; i < m; i++) tq.q[i] = hp.qubits[size_t(i)];
     const size_t smem = tile_smem_bytes(m, sizeof(V) == 8);
-    static size_t configured[2] = {0, 0};
-    size_t& conf = configured[sizeof(V) == 8 ? 1 : 0];
-    if (smem > conf) {
-        cudaFuncSetAttribute(k_tile_phased<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        cudaFuncSetAttribute(k_tile_phased<V>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             int(cudaSharedmemCarveoutMaxShared));
-        conf = smem;
-    }
     const uint64_t total = b.W << (b.n - m);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_phased<V>, kPhaseThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    const uint64_t grid = std::min<uint64_t>(total, uint64_t(sm_count()) * per_sm);
-    k_tile_phased<V><<<unsigned(grid), kPhaseThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq, phases,
-                                                                         nphases, ops, pool, total);
+    if (block.size() <= size_t(kPhaseParamWords)) {
+        static size_t configured = 0;
+        const uint64_t grid = configure(k_tile_phased_arg<V>, smem, configured, total);
+        static thread_local PhasedArgs args;
+        std::memcpy(args.q, block.data(), block.size() * sizeof(uint4));
+        k_tile_phased_arg<V><<<unsigned(grid), kPhaseThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq,
+                                                                                 nphases, total, args);
+    } else {
+        if (!block_dev) fail(kValueError, "phased tile pass without its device block");
+        static size_t configured = 0;
+        const uint64_t grid = configure(k_tile_phased_dev<V>, smem, configured, total);
+        k_tile_phased_dev<V><<<unsigned(grid), kPhaseThreads, smem, b.stream>>>(static_cast<V*>(b.amps), b.n, m, tq,
+                                                                                 nphases, total, block_dev);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(kCudaError, std::string("phased tile pass: ") + cudaGetErrorString(e));
 }
 
 }  // namespace
 
-void tile_pass_phased(const Batch& b, const TilePass& host_pass, const TilePhase* phases_dev, int nphases,
-                      const PhaseOp* ops_dev, const double2* pool_dev) {
+void tile_pass_phased(const Batch& b, const TilePass& host_pass, int nphases, const std::vector<uint4>& block,
+                      const uint4* block_dev) {
     if (b.c64)
-        launch_phased<float2>(b, host_pass, phases_dev, nphases, ops_dev, pool_dev);
+        launch_phased<float2>(b, host_pass, nphases, block, block_dev);
     else
-        launch_phased<double2>(b, host_pass, phases_dev, nphases, ops_dev, pool_dev);
+        launch_phased<double2>(b, host_pass, nphases, block, block_dev);
 }
 
 }  // namespace k

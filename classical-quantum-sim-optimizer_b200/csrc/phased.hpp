@@ -18,6 +18,12 @@
 // operations have no targets; controls and diagonal patterns are read off
 // each amplitude's tile index.  Within a phase the operations keep their
 // pass order.
+//
+// A pass's phases, operations and matrices form one block of 16-byte words.
+// A block that fits the kernel-parameter space travels as a launch argument:
+// every thread reads the same word at the same time, which the constant cache
+// serves without the load/store pipe the amplitudes need.  Larger blocks are
+// read from device memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -38,34 +44,24 @@ static_assert(kPhaseRegBits == 3 || kPhaseRegBits == 4, "three or four register 
 constexpr int kPhaseEntries = 1 << kPhaseRegBits;  // amplitudes per thread and slot
 constexpr int kPhaseMaxSlotBits = 16;
 
-// Device descriptor of one phase.  Register entry v (bit i of v = register
-// qubit i) of slot s sits at tile index base(s) | rb[v], where base(s) ORs
-// sb[i] over the set bits i of s; prb / psb are the same offsets after the
-// shared-memory swizzle, which is linear, so entry addresses are XORs.
-struct TilePhase {
-    int first_op = 0, nops = 0;
-    int nslot_bits = 0, pad = 0;
-    uint32_t rb[kPhaseEntries] = {}, prb[kPhaseEntries] = {};
-    uint32_t sb[kPhaseMaxSlotBits] = {}, psb[kPhaseMaxSlotBits] = {};
-};
+// Block layout (uint4 words, indices relative to the block):
+//   phase p at 6p: w0 = {first op word, op count, slot bits, 0};
+//     w1 = register qubit i as (1 << q) | (swizzled (1 << q)) << 16, i < 4;
+//     w2..w5 = slot bit i likewise, i < 16;
+//   operation at 2 words: {code, first matrix word, condition mask, value},
+//     {k, diagonal qubits 0-3 and 4-7 as bytes, 0};
+//   matrices: one double2 per word.
+constexpr int kPhaseWords = 6;
+constexpr int kPhaseOpWords = 2;
+constexpr int kPhaseParamWords = 2040;  // largest block passed as a kernel argument (32,640 bytes)
 
-// One operation of a phase.  code: 0-3 one-qubit matrix on register qubit
-// 0-3; 4-7 X; 8-13 two-qubit dense on register qubits (1,0), (2,0), (2,1),
-// (3,0), (3,1), (3,2) (matrix index bit 1 on the higher one); 14-17
-// three-qubit dense on (2,1,0), (3,1,0), (3,2,0), (3,2,1) (matrix index bit 2
-// on the highest); 18-23 swap of the pairs in the two-qubit order; 24 one
-// diagonal entry; 25 a full diagonal over k tile qubits (q[0] the MSB of the
-// table index).  Operations with a condition act where (tile index & mask) ==
-// value.
-struct PhaseOp {
-    int code = 0;
-    int mat = 0;  // offset into the pass's double2 pool
-    uint32_t mask = 0, value = 0;
-    int k = 0;
-    uint8_t q[8] = {};
-    int pad = 0;
-};
-
+// Operation codes: 0-3 one-qubit matrix on register qubit 0-3; 4-7 X; 8-13
+// two-qubit dense on register qubits (1,0), (2,0), (2,1), (3,0), (3,1), (3,2)
+// (matrix index bit 1 on the higher one); 14-17 three-qubit dense on (2,1,0),
+// (3,1,0), (3,2,0), (3,2,1) (matrix index bit 2 on the highest); 18-23 swap of
+// the pairs in the two-qubit order; 24 one diagonal entry; 25 a full diagonal
+// over k tile qubits (the first the MSB of the table index).  Operations with
+// a condition act where (tile index & mask) == value.
 enum PhaseCode : int { kPhOne = 0, kPhX = 4, kPhD2 = 8, kPhD3 = 14, kPhSwap = 18, kPhDiagEntry = 24, kPhDiagFull = 25 };
 
 // Index of register-qubit pair (h > l) in the two-qubit order above, and of
@@ -86,18 +82,18 @@ inline uint32_t phase_swizzle(uint32_t e, int g) {
 // True when a pass of m tile qubits can run in phases.
 inline bool phase_supported(int m) { return m >= kPhaseRegBits + 2 && m - kPhaseRegBits <= kPhaseMaxSlotBits; }
 
-// Groups `ops` (one pass, m tile qubits) into phases, appending descriptors and
-// operations; dense matrices are re-laid out for their register qubits and
-// appended to `pool`.  Returns the number of phases.
-int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, std::vector<double2>& pool,
-                std::vector<TilePhase>& phases, std::vector<PhaseOp>& phase_ops);
+// Groups `ops` (one pass, m tile qubits, matrices in `pool`) into phases and
+// writes the pass's block.  Returns the number of phases.
+int plan_phases(const std::vector<TileOp>& ops, int m, bool c64, const std::vector<double2>& pool,
+                std::vector<uint4>& block);
 
 namespace k {
 
-// One tile pass in phases: phases_dev[0 .. nphases) of this pass, whose
-// operations index ops_dev and pool_dev.
-void tile_pass_phased(const Batch& b, const TilePass& host_pass, const TilePhase* phases_dev, int nphases,
-                      const PhaseOp* ops_dev, const double2* pool_dev);
+// One tile pass in phases.  `block` is the host copy of the pass's block and
+// `block_dev` the same words on the device (read when the block is larger
+// than the kernel-parameter space).
+void tile_pass_phased(const Batch& b, const TilePass& host_pass, int nphases, const std::vector<uint4>& block,
+                      const uint4* block_dev);
 
 }  // namespace k
 }  // namespace dq

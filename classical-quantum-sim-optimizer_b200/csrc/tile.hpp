@@ -41,8 +41,10 @@ struct TilePass {
     std::vector<int> qubits;  // ascending global positions of the m tile qubits
     std::vector<TileOp> ops;
     int op_begin = 0;         // index into the device op array
-    int phase_begin = 0;      // register phases of the pass (phased.hpp): first index and count,
-    int nphases = 0;          // 0 when the pass runs one operation per sweep
+    // Register phases of the pass (phased.hpp): its block (index into the
+    // executor's blocks, and first word in their device copy) and phase count;
+    // nphases 0 when the pass runs one operation per sweep.
+    int phase_block = -1, phase_begin = 0, nphases = 0;
     int raw_ops = 0;          // unfused operations covered (for statistics)
     std::vector<Operation> raw;  // filled when TilePlanOptions::keep_raw
     std::vector<size_t> op_index;  // the pass's operations: indices into the planned list, ascending
