@@ -85,3 +85,30 @@ def test_c64_sampling_and_queries():
     assert abs(sum(probs.values()) - 1.0) < 1e-5
     ref = oracle_sv(qft(10, seed=2))
     assert r.fidelity(ref) >= 1 - 1e-6
+
+
+def phase_block_words(p):
+    """16-byte words of a pass's phase block: 6 per phase, 2 per operation and one per matrix entry."""
+    words = 6 * len(p["phases"])
+    for ph in p["phases"]:
+        for op in ph["ops"]:
+            c, k = op["code"], op["k"]
+            entries = (4 if c < 4 else 0 if c < 8 else 16 if c < 14 else 64 if c < 18 else 0 if c < 24
+                       else 1 if c == 24 else 1 << k)
+            words += 2 + entries
+    return words
+
+
+def test_phase_blocks_as_launch_arguments_and_in_device_memory():
+    """complex128 tile passes take their phase block as a launch argument when it
+    fits 2,040 words and read it from device memory otherwise: both reproduce the
+    oracle."""
+    from dqsim import _core
+
+    small = brickwork(16, 12, seed=2, measure=False)
+    large = brickwork(12, 40, seed=1, measure=False)  # one pass holds every operation
+    sizes_small = [phase_block_words(p) for p in _core.tile_plan_dump(small.model_dump_json(), 12, 2)["passes"]]
+    sizes_large = [phase_block_words(p) for p in _core.tile_plan_dump(large.model_dump_json(), 12, 2)["passes"]]
+    assert max(sizes_small) <= 2040 < min(sizes_large)
+    for c in (small, large):
+        assert np.max(np.abs(run(c, execution="tiled", tile_qubits=12, fusion_width=2) - oracle_sv(c))) <= 1e-12
