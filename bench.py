@@ -407,7 +407,8 @@ def main():
             fp64 = dqsim._core.device_fp64_tflops(local)
             ach = fl / (tile["ms"] * 1e-3) / 1e12
             out_forms["complex128_tiled"]["fp64_roofline"] = {
-                "kernel": "k_tile<double2>", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                "kernel": "k_tile_phased_arg<double2> (register phases)", "bound": "fp64", "achieved": ach,
+                "peak": fp64, "unit": "TFLOP/s",
                 "frac": ach / fp64, "peak_kind": "measured (dq_device_fp64_tflops)", "flops": fl,
                 "launches": tile["launches"]}
         del plant, simt

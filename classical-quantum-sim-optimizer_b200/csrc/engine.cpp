@@ -260,17 +260,22 @@ void StateBatch::allocate(int n_, uint64_t W_, uint64_t ncb_, bool c64_, cudaStr
     ncb = ncb_;
     c64 = c64_;
     cwords = int(std::max<uint64_t>(1, (ncb + 63) / 64));
-    if (pool_stream)
-        amps.alloc_on((size_t(W) << n) * (c64 ? 8 : 16), pool_stream, "the statevector");
-    else
-        amps.alloc((size_t(W) << n) * (c64 ? 8 : 16), "the statevector");
-    cbits.alloc(size_t(W) * cwords * 8, "classical bits");
-    seeds.alloc(size_t(W) * 8, "rng seeds");
-    draws.alloc(size_t(W) * 8, "rng counters");
-    outcome.alloc(size_t(W) * 4, "measurement outcomes");
-    scale.alloc(size_t(W) * 8, "measurement scales");
-    partial.alloc(size_t(W) * k::kMaxChunks * 2 * 8, "measurement partial sums");
-    err.alloc(16, "error flag");
+    // With a stream, every buffer comes from the engine's pool: freeing them
+    // is stream-ordered and never waits for the device.
+    auto get = [&](DevMem& m, size_t bytes, const char* what) {
+        if (pool_stream)
+            m.alloc_on(bytes, pool_stream, what);
+        else
+            m.alloc(bytes, what);
+    };
+    get(amps, (size_t(W) << n) * (c64 ? 8 : 16), "the statevector");
+    get(cbits, size_t(W) * cwords * 8, "classical bits");
+    get(seeds, size_t(W) * 8, "rng seeds");
+    get(draws, size_t(W) * 8, "rng counters");
+    get(outcome, size_t(W) * 4, "measurement outcomes");
+    get(scale, size_t(W) * 8, "measurement scales");
+    get(partial, size_t(W) * k::kMaxChunks * 2 * 8, "measurement partial sums");
+    get(err, 16, "error flag");
 }
 
 k::Batch StateBatch::view(cudaStream_t s, uint64_t W_active) const {

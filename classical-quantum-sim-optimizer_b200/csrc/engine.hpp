@@ -41,6 +41,9 @@ struct DevMem {
     void ensure(size_t b, const char* what) {
         if (b > bytes) alloc(b, what);
     }
+    void ensure_on(size_t b, cudaStream_t s, const char* what) {
+        if (b > bytes) alloc_on(b, s, what);
+    }
     void release();
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };

@@ -103,7 +103,7 @@ void probs_to(const k::Batch& b, const std::vector<uint64_t>& qubits, double* ou
 // returns the total, the last entry of the full running sums.
 double build_sums(const k::Batch& b, const std::vector<uint64_t>& qubits, double* cdf, uint64_t len, DevMem& tmp) {
     cudaStream_t s = b.stream;
-    tmp.ensure(k::scan_tmp_size(len) * 8, "scan scratch");
+    tmp.ensure_on(k::scan_tmp_size(len) * 8, s, "scan scratch");
     if (is_full_descending(qubits, uint64_t(b.n))) {
         k::scan_probs(b, cdf, tmp.as<double>(), false);
     } else {
@@ -300,7 +300,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
                 phase(kPhSums);
                 st.amps.release();  // the state is no longer needed (shots.rs:150)
-                idx.alloc(shots * 8, "sampled outcomes");
+                idx.alloc_on(shots * 8, s, "sampled outcomes");
                 k::sample_sums(s, cdf.as<double>(), tmp.as<double>(), clen, nullptr, total, false, seed, shots, true,
                                idx.as<uint64_t>());
                 std::vector<uint64_t> h(shots);
