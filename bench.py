@@ -573,7 +573,7 @@ def run_batch(args):
     loop_ms = max_over_ranks(pg, local, loop_ms)
     zz_err = max_over_ranks(pg, local, zz_err)
     cpu = None
-    if world == 1:
+    if world == 1 and not args.no_cpu:
         # CPU restatement on a bounded sample: whole simulate_shots calls on circuits taken in a seeded order
         # until the budget is spent, scaled to the batch by amplitude-operations (2^n x gates per circuit).
         rng = np.random.default_rng(args.seed)
