@@ -24,7 +24,7 @@
 // distinct pass of the candidate plans of recorded circuits, and seeded
 // random passes), it chooses which of the candidate fused plans to run in
 // place of the hand-fitted pass and spread constants; the hand rule's plan is
-// the fallback and the judge.
+// the fallback, and every learned plan is timed against it.
 #pragma once
 
 #include <cuda_runtime.h>
