@@ -452,19 +452,25 @@ def main():
     if not args.no_e2e:
         api = dqsim.StatevectorSimulator(seed=args.seed, max_memory_mb=1 << 20, precision="complex64",
                                          device=local)
+        warm_runs, warm_phases = [], []
         for _ in range(max(1, args.warmup)):
+            t0 = time.perf_counter()
             api.simulate_shots(circuit, shots=args.shots)
+            warm_runs.append(time.perf_counter() - t0)
+            warm_phases.append({**{k: round(v * 1e3, 3) for k, v in dqsim._core.last_call_phases(api).items()},
+                                "free_gb": round(dqsim._core.device_memory(local)["free"] / 1e9, 2)})
         e2e_runs, e2e_phases = [], []
         for _ in range(5):
             t0 = time.perf_counter()
             counts = api.simulate_shots(circuit, shots=args.shots)
             e2e_runs.append(time.perf_counter() - t0)
-            e2e_phases.append({k: round(v * 1e3, 3) for k, v in dqsim._core.last_call_phases(api).items()})
+            e2e_phases.append({**{k: round(v * 1e3, 3) for k, v in dqsim._core.last_call_phases(api).items()},
+                               "free_gb": round(dqsim._core.device_memory(local)["free"] / 1e9, 2)})
             assert sum(counts.values()) == args.shots
         e2e = {"value": statistics.median(e2e_runs), "unit": "s",
                "h2d_bytes_per_step": len(circuit.model_dump_json()), "d2h_bytes_per_step": 8 * args.shots,
                "runs_s": e2e_runs, "mean_s": statistics.mean(e2e_runs), "max_s": max(e2e_runs),
-               "phases_ms": e2e_phases}
+               "phases_ms": e2e_phases, "warmup_runs_s": warm_runs, "warmup_phases_ms": warm_phases}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -162,6 +162,14 @@ Simulator::Simulator(const Options& o) : opt_(o) {
     budget_ = o.max_memory_mb * 1024 * 1024;
 }
 
+Simulator::~Simulator() {
+    if (ws_ && dev_) {
+        std::lock_guard<std::mutex> lk(dev_->mu);
+        cudaSetDevice(dev_->ordinal);
+        ws_.reset();
+    }
+}
+
 uint64_t Simulator::next_seed() {
     if (opt_.has_seed) return opt_.seed;
     std::random_device rd;
@@ -275,12 +283,24 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 mark = now;
             };
             {
-                StateBatch st;
-                st.allocate(int(n), 1, ncb, c64, s);
+                // The workspace of the previous call is reused where its sizes match.
+                if (!ws_) ws_ = std::make_unique<SamplingWorkspace>();
+                StateBatch& st = ws_->st;
+                if (!st.amps.p || st.n != int(n) || st.W != 1 || st.ncb != ncb || st.c64 != c64)
+                    st.allocate(int(n), 1, ncb, c64, s);
                 k::Batch b = st.view(s, 1);
                 k::init_basis(b);
                 reset_bookkeeping(st, 1, {kept_seed}, s);
                 phase(kPhState);
+                DevMem& cdf = ws_->table;
+                DevMem& tmp = ws_->scratch;
+                DevMem& idx = ws_->outcomes;
+                const uint64_t clen = uint64_t(1) << kq;
+                if (cdf.bytes != clen * 8) cdf.alloc_on(clen * 8, s, "the sampling table");
+                const uint64_t tmp_bytes = std::max<uint64_t>(k::scan_tmp_size(clen) * 8, 16);
+                if (tmp.bytes != tmp_bytes) tmp.alloc_on(tmp_bytes, s, "scan scratch");
+                if (idx.bytes != shots * 8) idx.alloc_on(shots * 8, s, "sampled outcomes");
+                phase(kPhTable);
                 // The prefix's executor: kept with the circuit's cached plan (the
                 // device lock above serialises its use), or built for this call.
                 std::unique_ptr<Executor> own;
@@ -291,16 +311,25 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                     if (shot_plan) shot_plan->prefix = std::move(own);
                 }
                 phase(kPhPlan);
+                // Device time of the prefix, read once the sums below have synchronised.
+                cudaEvent_t ev[2] = {nullptr, nullptr};
+                for (cudaEvent_t& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+                struct EventPair {
+                    cudaEvent_t* e;
+                    ~EventPair() {
+                        for (int i = 0; i < 2; i++) cudaEventDestroy(e[i]);
+                    }
+                } ev_guard{ev};
+                cuda_check(cudaEventRecord(ev[0], s), "cudaEventRecord");
                 ex->run(b, nullptr);
+                cuda_check(cudaEventRecord(ev[1], s), "cudaEventRecord");
                 phase(kPhRun);
-                DevMem cdf, tmp, idx;
-                const uint64_t clen = uint64_t(1) << kq;
-                cdf.alloc_on(clen * 8, s, "the sampling table");
                 double total = build_sums(b, qubits, cdf.as<double>(), clen, tmp);
                 if (!std::isfinite(total) || total <= 0.0) fail(kMemoryError, "Invalid state normalization when sampling");
                 phase(kPhSums);
-                st.amps.release();  // the state is no longer needed (shots.rs:150)
-                idx.alloc_on(shots * 8, s, "sampled outcomes");
+                float prefix_ms = 0.f;
+                if (cudaEventElapsedTime(&prefix_ms, ev[0], ev[1]) == cudaSuccess)
+                    set_phase(kPhPrefixDevice, double(prefix_ms) * 1e-3);
                 k::sample_sums(s, cdf.as<double>(), tmp.as<double>(), clen, nullptr, total, false, seed, shots, true,
                                idx.as<uint64_t>());
                 std::vector<uint64_t> h(shots);

@@ -66,6 +66,8 @@ enum CallPhase : int {
     kPhKeys,        // sorting outcomes into distinct count keys
     kPhRelease,     // freeing the call's device buffers
     kPhTotal,
+    kPhTable,         // allocating the sampling table and its scan scratch (before the prefix)
+    kPhPrefixDevice,  // device time of the unitary prefix (CUDA events on the simulator's stream)
     kNumCallPhases
 };
 
@@ -107,9 +109,22 @@ struct ShotPlan {
     std::unique_ptr<Executor> prefix;
 };
 
+// Device buffers of terminal sampling, kept by a simulator between calls:
+// the statevector with its bookkeeping, the sampling table, the scan scratch
+// and the drawn outcomes.  A call whose sizes match the previous one's
+// allocates nothing.  Allocating them per call from the stream-ordered pool
+// cost 50 ms to over 1 s of host time per 8 GiB buffer at 30 qubits: small
+// bookkeeping blocks carved from the freed large ones left no whole free
+// block, and the pool mapped the memory again.
+struct SamplingWorkspace {
+    StateBatch st;
+    DevMem table, scratch, outcomes;
+};
+
 class Simulator {
   public:
     explicit Simulator(const Options& o);
+    ~Simulator();
     ShotOutput simulate_shots(const char* json, size_t len, uint64_t shots, bool profile, double* preprocessing,
                               double* fusion);
     std::unique_ptr<Result> simulate(const char* json, size_t len);
@@ -156,6 +171,8 @@ class Simulator {
     // Most recently used first; at most kShotPlans entries.
     static constexpr size_t kShotPlans = 4;
     std::vector<std::shared_ptr<ShotPlan>> plans_;
+    // Used under dev_->mu; released (on the device's stream) before dev_.
+    std::unique_ptr<SamplingWorkspace> ws_;
     void set_phase(int i, double v) {
         std::lock_guard<std::mutex> lk(mu_);
         phases_[i] = v;

@@ -762,7 +762,8 @@ def planner_log(simulator):
         _string_free(ctypes.cast(out, ctypes.c_void_p))
 
 
-CALL_PHASES = ("parse", "compile", "state", "plan", "run", "sums", "sample", "keys", "release", "total")
+CALL_PHASES = ("parse", "compile", "state", "plan", "run", "sums", "sample", "keys", "release", "total", "table",
+               "prefix_device")
 
 
 def last_call_phases(simulator):

@@ -301,9 +301,11 @@ DQ_API int dq_device_fp64_tflops(int device, double* tflops);
  * [3] pass planning and gate images, [4] launching the unitary prefix,
  * [5] probability running sums (waits for the prefix to finish), [6] shot
  * draws and their copy to the host, [7] count keys, [8] freeing the call's
- * device buffers, [9] the whole call.  Terminal sampling fills every phase;
- * trajectories fill 0, 1 and 9. */
-#define DQ_CALL_PHASES 10
+ * device buffers, [9] the whole call, [10] allocating the sampling table
+ * (host time, before the prefix is launched) and [11] the device time of the unitary
+ * prefix (CUDA events around its launches).  Terminal sampling fills every
+ * phase; trajectories fill 0, 1 and 9. */
+#define DQ_CALL_PHASES 12
 DQ_API int dq_sim_last_call_phases(dq_sim* sim, double* out, uint64_t n);
 
 /* Measure without allocating.  No counterpart in the reference: it serves
