@@ -32,6 +32,11 @@ if not _LIB_PATH.exists():
 
 _lib = ctypes.CDLL(str(_LIB_PATH))
 
+try:  # count dictionaries built in C (dqsim/_counts.c); the same dictionaries otherwise
+    from . import _counts
+except ImportError:
+    _counts = None
+
 _u64 = ctypes.c_uint64
 _P = ctypes.c_void_p
 
@@ -149,6 +154,8 @@ def _take_counts(handle):
         keys = ctypes.create_string_buffer(max(1, n * w))
         counts = np.zeros(max(1, n), dtype=np.uint64)
         _check(_counts_copy(handle, keys, counts.ctypes.data))
+        if _counts is not None:
+            return _counts.build(keys.raw[:n * w], w, counts[:n].tobytes())
         text = keys.raw[:n * w].decode("ascii")
         return dict(zip([text[i:i + w] for i in range(0, n * w, w)] if w else [""] * n, counts[:n].tolist()))
     finally:
