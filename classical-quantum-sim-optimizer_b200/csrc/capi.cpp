@@ -1009,7 +1009,9 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
             for (int bi = 0; bi < fp.nblocks; bi++) {
                 const FusedBlock& b = blocks[size_t(fp.first_block + bi)];
                 s += bi ? ",{" : "{";
-                s += "\"u_off\":" + std::to_string(b.u_off) + ",\"last\":" + std::to_string(b.last) + ",\"next_b\":[";
+                s += "\"u_off\":" + std::to_string(b.u_off) + ",\"last\":" + std::to_string(b.last) + ",\"mask\":" +
+                     std::to_string(size_t(bi) < fp.block_masks.size() ? fp.block_masks[size_t(bi)] : 0u) +
+                     ",\"next_b\":[";
                 for (int i = 0; i < 32; i++) s += (i ? "," : "") + std::to_string(b.next_b[i]);
                 s += "],\"next_c\":[";
                 for (int i = 0; i < kFusedCols; i++) s += (i ? "," : "") + std::to_string(b.next_c[i]);

@@ -760,7 +760,7 @@ void Executor::upload(cudaStream_t stream) {
     uploaded_ = true;
 }
 
-void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
+void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec, bool normalize) {
     upload(b.stream);
     std::vector<uint64_t> host_cbits;
     bool norm_pending = false;  // a fused pass left a norm the next fused pass divides out
@@ -796,17 +796,20 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec) {
                           norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>());
             if (rec) rec->end();
             const bool last_fused = si + 1 == steps_.size() || steps_[si + 1].fused < 0;
-            // Tile norms read (8 B per tile); the final rescale reads and writes the state.
-            if (rec)
-                rec->begin(kcNorm, double(tiles) * 8.0 + (last_fused ? 2.0 * double(size_t(b.W) << b.n) * 8.0 : 0.0),
-                           last_fused ? 2 : 1);
-            k::fused_state_norm(b, norm_tiles_.as<double>(), norm_states_.as<double>());
-            norm_pending = true;
-            if (last_fused) {
-                k::fused_renormalize(b, norm_states_.as<double>());
-                norm_pending = false;
+            if (normalize || si + 1 != steps_.size()) {
+                // Tile norms read (8 B per tile); the final rescale reads and writes the state.
+                if (rec)
+                    rec->begin(kcNorm,
+                               double(tiles) * 8.0 + (last_fused ? 2.0 * double(size_t(b.W) << b.n) * 8.0 : 0.0),
+                               last_fused ? 2 : 1);
+                k::fused_state_norm(b, norm_tiles_.as<double>(), norm_states_.as<double>());
+                norm_pending = true;
+                if (last_fused) {
+                    k::fused_renormalize(b, norm_states_.as<double>());
+                    norm_pending = false;
+                }
+                if (rec) rec->end();
             }
-            if (rec) rec->end();
             if (profile) {
                 cuda_check(cudaStreamSynchronize(b.stream), "stream synchronize");
                 profile->nq_calls++;

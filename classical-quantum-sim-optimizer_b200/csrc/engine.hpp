@@ -156,7 +156,11 @@ class Executor {
   public:
     Executor(const std::vector<Operation>& ops, size_t begin, size_t end, const ExecConfig& cfg = ExecConfig());
     // Launch every step on the batch (asynchronously unless `profile`).
-    void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr);
+    // `normalize` false: when the last step is a fused tensor-core pass, its
+    // FP64 norm and rescale are left out (the state keeps the pass's rounding
+    // of the norm, ~1e-7); for callers that only sample, which divides by the
+    // total probability anyway.
+    void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr, bool normalize = true);
     // Uploads the matrix pools and sizes the scratch a run over batches like
     // `b` needs, so that later runs allocate nothing and copy nothing from the
     // host (they can then be captured into a CUDA graph).

@@ -566,17 +566,21 @@ __global__ void __launch_bounds__(256) k_dot(const V* __restrict__ a, const doub
 template <typename VA, typename VB>
 __global__ void __launch_bounds__(256) k_compare(const VA* __restrict__ a, const VB* __restrict__ b, uint64_t len,
                                                 double* __restrict__ partial) {
-    double re = 0.0, im = 0.0, mx = 0.0;
+    double re = 0.0, im = 0.0, mx = 0.0, na = 0.0, nb = 0.0;
     for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < len; g += uint64_t(gridDim.x) * blockDim.x) {
         VA x = a[g];
         VB y = b[g];
         double xr = x.x, xi = x.y, yr = y.x, yi = y.y;
         re += xr * yr + xi * yi;
         im += xr * yi - xi * yr;
+        na += xr * xr + xi * xi;
+        nb += yr * yr + yi * yi;
         double dr = xr - yr, di = xi - yi;
         mx = fmax(mx, sqrt(dr * dr + di * di));
     }
     block_sum2(re, im);
+    __syncthreads();  // block_sum2's shared partials are reused below
+    block_sum2(na, nb);
     __shared__ double smx[32];
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
     if ((threadIdx.x & 31) == 0) smx[threadIdx.x >> 5] = mx;
@@ -584,9 +588,11 @@ __global__ void __launch_bounds__(256) k_compare(const VA* __restrict__ a, const
     if (threadIdx.x == 0) {
         double m = 0.0;
         for (int w = 0; w < int(blockDim.x >> 5); w++) m = fmax(m, smx[w]);
-        partial[blockIdx.x * 3] = re;
-        partial[blockIdx.x * 3 + 1] = im;
-        partial[blockIdx.x * 3 + 2] = m;
+        partial[blockIdx.x * 5] = re;
+        partial[blockIdx.x * 5 + 1] = im;
+        partial[blockIdx.x * 5 + 2] = m;
+        partial[blockIdx.x * 5 + 3] = na;
+        partial[blockIdx.x * 5 + 4] = nb;
     }
 }
 

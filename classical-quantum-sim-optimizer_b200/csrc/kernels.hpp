@@ -121,6 +121,8 @@ void gather(const Batch& b, const uint64_t* idx, uint64_t count, double2* out);
 int pauli_partials(const Batch& b, uint64_t x, uint64_t z, double2* partial);
 // Per-block partials of <a|b> and max |a_i - b_i| for two states of `len`
 // amplitudes, each c128 or c64; partial holds kDotBlocks * 3 doubles.
+// Per-block partials (kDotBlocks x 5): Re and Im of <a|b>, max |a_i - b_i|,
+// <a|a> and <b|b>.
 void compare(cudaStream_t s, const void* a, bool a64, const void* b, bool b64, uint64_t len, double* partial);
 
 }  // namespace k

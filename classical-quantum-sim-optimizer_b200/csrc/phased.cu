@@ -554,15 +554,25 @@ __device__ __forceinline__ void phased_body(V* __restrict__ s, int n, int m, con
     }
 }
 
+// Resident CTAs per SM the register allocation is bounded for: complex128 tiles
+// (64 KB of shared memory each at 12 tile qubits) take DQ_PHASE_CTAS_C128.
+#ifndef DQ_PHASE_CTAS_C128
+#define DQ_PHASE_CTAS_C128 2
+#endif
 template <typename V>
-__global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V) == 8 ? 2 : 1)
+constexpr int phase_min_ctas() {
+    return sizeof(V) == 16 ? (kPhaseRegBits == 3 ? DQ_PHASE_CTAS_C128 : 1) : 2;
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kPhaseThreads, phase_min_ctas<V>())
     k_tile_phased_dev(V* __restrict__ s, int n, int m, PhaseQubits tq, int nphases, uint64_t total_tiles,
                       const uint4* __restrict__ block) {
     phased_body<V>(s, n, m, tq, nphases, total_tiles, DevWords{block});
 }
 
 template <typename V>
-__global__ void __launch_bounds__(kPhaseThreads, kPhaseRegBits == 3 || sizeof(V) == 8 ? 2 : 1)
+__global__ void __launch_bounds__(kPhaseThreads, phase_min_ctas<V>())
     k_tile_phased_arg(V* __restrict__ s, int n, int m, PhaseQubits tq, int nphases, uint64_t total_tiles,
                       const __grid_constant__ PhasedArgs args) {
     phased_body<V>(s, n, m, tq, nphases, total_tiles, ArgWords{&args});

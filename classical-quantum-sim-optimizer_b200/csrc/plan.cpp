@@ -120,7 +120,7 @@ double Plan::run(bool record) {
     cuda_check(cudaMemsetAsync(st_.draws.p, 0, 8, s), "clear draws");
     cuda_check(cudaMemsetAsync(st_.err.p, 0, 16, s), "clear error flag");
     cuda_check(cudaMemcpyAsync(st_.seeds.p, &seed_, 8, cudaMemcpyHostToDevice, s), "seed");
-    ex_->run(bt, nullptr, record ? &rec : nullptr);
+    ex_->run(bt, nullptr, record ? &rec : nullptr, /*normalize=*/cdf_.p == nullptr);
     if (cdf_.p) {
         const uint64_t clen = uint64_t(1) << sample_qubits_.size();
         bool full = sample_qubits_.size() == n_;
@@ -187,19 +187,23 @@ void Plan::compare(const Plan& other, double* fidelity, double* max_abs_err) con
     dev_->activate();
     cuda_check(cudaStreamSynchronize(other.dev_->stream), "stream synchronize");
     DevMem part;
-    part.alloc(size_t(k::kDotBlocks) * 3 * 8, "comparison partial sums");
+    part.alloc(size_t(k::kDotBlocks) * 5 * 8, "comparison partial sums");
     k::compare(dev_->stream, st_.amps.p, st_.c64, other.st_.amps.p, other.st_.c64, uint64_t(1) << n_,
                part.as<double>());
-    std::vector<double> h(size_t(k::kDotBlocks) * 3);
+    std::vector<double> h(size_t(k::kDotBlocks) * 5);
     cuda_check(cudaMemcpyAsync(h.data(), part.p, h.size() * 8, cudaMemcpyDeviceToHost, dev_->stream), "read");
     dev_->sync();
-    double re = 0, im = 0, mx = 0;
+    double re = 0, im = 0, mx = 0, na = 0, nb = 0;
     for (int i = 0; i < k::kDotBlocks; i++) {
-        re += h[i * 3];
-        im += h[i * 3 + 1];
-        mx = std::max(mx, h[i * 3 + 2]);
+        re += h[i * 5];
+        im += h[i * 5 + 1];
+        mx = std::max(mx, h[i * 5 + 2]);
+        na += h[i * 5 + 3];
+        nb += h[i * 5 + 4];
     }
-    *fidelity = re * re + im * im;
+    // |<a|b>|^2 / (<a|a> <b|b>): a sampling run leaves the fused form's last
+    // pass unrescaled (sampling divides by the total), so norms are divided out.
+    *fidelity = (re * re + im * im) / (na * nb);
     *max_abs_err = mx;
 }
 

@@ -321,7 +321,7 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                     }
                 } ev_guard{ev};
                 cuda_check(cudaEventRecord(ev[0], s), "cudaEventRecord");
-                ex->run(b, nullptr);
+                ex->run(b, nullptr, nullptr, /*normalize=*/false);  // the sampler divides by the total
                 cuda_check(cudaEventRecord(ev[1], s), "cudaEventRecord");
                 phase(kPhRun);
                 double total = build_sums(b, qubits, cdf.as<double>(), clen, tmp);
