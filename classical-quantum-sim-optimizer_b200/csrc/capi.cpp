@@ -991,6 +991,12 @@ int dq_fused_plan_dump(const char* json, size_t len, char** out_text) {
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_lo[i]);
             s += "],\"out_hi\":[";
             for (int i = 0; i < 64; i++) s += (i ? "," : "") + std::to_string(fp.out_hi[i]);
+            s += "],\"split_pos\":[";
+            for (int i = 0; i < 8; i++) s += (i ? "," : "") + std::to_string(fp.split_pos[i]);
+            s += "],\"split_q\":[";
+            for (int i = 0; i < 16; i++) s += (i ? "," : "") + std::to_string(fp.split_q[i]);
+            s += "],\"split_qoff\":[";
+            for (int i = 0; i < 16; i++) s += (i ? "," : "") + std::to_string(fp.split_qoff[i]);
             const FusedTma t = fused_tma_plan(fp.qubits, int(n), 1);
             s += "],\"tma\":{\"ok\":" + std::to_string(t.ok) + ",\"dims\":" + std::to_string(t.dims) +
                  ",\"copies\":" + std::to_string(t.copies) + ",\"copy_bytes\":" + std::to_string(t.copy_bytes);

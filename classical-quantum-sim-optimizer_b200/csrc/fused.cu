@@ -85,6 +85,7 @@ static_assert(kOffU % 1024 == 0 && kOffBar % 8 == 0 && kOffWsum % 8 == 0, "opera
 static_assert(offsetof(FusedBlock, next_b) == 16 && sizeof(FusedBlock) % 16 == 0, "block table layout");
 static_assert(kUBytes == kFusedUHalves * 2, "gate image size");
 static_assert(kGroupWarps == 4 || kGroupWarps == 8, "a group's warps cover the four TMEM lane quarters evenly");
+static_assert(kGroupThreads == 128 && kPairIters == 16, "the split's thread mapping covers 2 * 128 x 16 amplitudes");
 
 // mbarrier slots (8 bytes each) from kOffBar, all with one arrival per phase
 constexpr uint32_t kBarUFull = 0;                     // [kUBufs] gate image of buffer b landed (expect_tx)
@@ -106,6 +107,9 @@ struct FusedFault {
 struct FusedQubits {
     int q[kFusedM];
     uint16_t io[4][64];  // in_lo, in_hi, out_lo, out_hi
+    uint8_t split_pos[8];      // the split's thread mapping (FusedPass::split_pos)
+    uint16_t split_q[16];      // ... its per-iteration amplitude bits
+    uint16_t split_qoff[16];   // ... and their operand offsets
     FusedTma tma;        // tile loads by TMA when tma.ok
     FusedFault fault;
 };
@@ -331,7 +335,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     unsigned char* x = sm + uint32_t(g) * kTileBytes;
     const uint64_t pair_lo = lo_tab[(2 * gt) & 63];       // load and store: pairs (e, e+1), e = 2*gt + 256k
     const uint32_t pair_out = io[128 + ((2 * gt) & 63)];
-    const uint32_t pair_even = io[(2 * gt) & 63], pair_odd = io[((2 * gt) & 63) + 1];
+    uint32_t split_p = 0;  // the split's amplitude bits of this thread (FusedPass::split_pos)
+#pragma unroll
+    for (int b = 1; b < 8; b++)
+        if (((2 * gt) >> b) & 1) split_p |= 1u << fq.split_pos[b];
+    const uint32_t split_off = uint32_t(io[split_p & 63]) ^ uint32_t(io[64 + (split_p >> 6)]);
+    const uint32_t split_odd = io[1];  // operand offset of local bit 0
     const uint32_t prow = uint32_t((2 * gt) >> 6);
     const uint32_t col = uint32_t((gw & 3) * 32 + lane);  // readback: TMEM lane = tile column
     const uint32_t taddr = tmem + ((uint32_t(gw & 3) * 32u) << 16) + kAccCols * uint32_t(g);
@@ -411,18 +420,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             group_sync(g);  // the group's copies of this tile have landed
         }
         {
+            // Pairs (e, e + 1), e = split_p | split_q[k]: 16-byte reads of the raw tile
+            // (natural order), 4-byte hi/lo stores into block 0's operand.
             float4 v[kPairIters];
 #pragma unroll
             for (int k = 0; k < kPairIters; k++)
-                v[k] = *reinterpret_cast<const float4*>(x + (2u * gt + 2u * kGroupThreads * k) * 8u);
+                v[k] = *reinterpret_cast<const float4*>(x + (split_p | uint32_t(fq.split_q[k])) * 8u);
             group_sync(g);  // raw tile read: the split may overwrite it
 #pragma unroll
             for (int k = 0; k < kPairIters; k++) {
-                const uint32_t hi_part = io[64 + prow + kRowStep * k];
-                put_split2(x, pair_even ^ hi_part,
-                           mul2(pack2(__float_as_uint(v[k].x), __float_as_uint(v[k].y)), fs2));
-                put_split2(x, pair_odd ^ hi_part,
-                           mul2(pack2(__float_as_uint(v[k].z), __float_as_uint(v[k].w)), fs2));
+                const uint32_t off = split_off ^ uint32_t(fq.split_qoff[k]);
+                put_split2(x, off, mul2(pack2(__float_as_uint(v[k].x), __float_as_uint(v[k].y)), fs2));
+                put_split2(x, off ^ split_odd, mul2(pack2(__float_as_uint(v[k].z), __float_as_uint(v[k].w)), fs2));
             }
         }
         double norm_acc = 0.0;
@@ -575,9 +584,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         float2* __restrict__ gp = s + base;
 #pragma unroll 8
-        for (int k = 0; k < kPairIters; k++)  // 16-byte pairs: adjacent stage slots, adjacent in HBM
-            *reinterpret_cast<float4*>(gp + (pair_lo | hi_tab[prow + kRowStep * k])) =
-                *reinterpret_cast<const float4*>(x + (pair_out ^ io[192 + prow + kRowStep * k]));
+        for (int k = 0; k < kPairIters; k++) {
+            // 16-byte pairs: the stage slots of amplitudes e and e + 1 are the two
+            // halves of one 16-byte pair (swapped when bit 3 of e's offset is set),
+            // adjacent in HBM.
+            const uint32_t so = pair_out ^ io[192 + prow + kRowStep * k];
+            float4 v = *reinterpret_cast<const float4*>(x + (so & ~15u));
+            if (so & 8u) v = make_float4(v.z, v.w, v.x, v.y);
+            *reinterpret_cast<float4*>(gp + (pair_lo | hi_tab[prow + kRowStep * k])) = v;
+        }
         // Per-tile FP64 norm, fixed-order reduction (deterministic).
         for (int o = 16; o > 0; o >>= 1) norm_acc += __shfl_down_sync(0xffffffffu, norm_acc, o);
         if (lane == 0) wsum[g * kGroupWarps + gw] = norm_acc;
@@ -778,6 +793,11 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     if (p.qubits[0] != 0 || p.qubits[1] != 1) fail(kValueError, "fused passes hold global qubits 0 and 1");
     FusedQubits fq;
     for (int i = 0; i < kFusedM; i++) fq.q[i] = p.qubits[i];
+    for (int b = 0; b < 8; b++) fq.split_pos[b] = p.split_pos[b];
+    for (int k = 0; k < 16; k++) {
+        fq.split_q[k] = p.split_q[k];
+        fq.split_qoff[k] = p.split_qoff[k];
+    }
     for (int e = 0; e < 64; e++) {
         fq.io[0][e] = p.in_lo[e];
         fq.io[1][e] = p.in_hi[e];

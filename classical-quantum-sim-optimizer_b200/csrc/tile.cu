@@ -461,6 +461,59 @@ inline size_t sw128_half(int row, int k) {
 
 }  // namespace
 
+namespace {
+
+// Rank over GF(2) of up to 32-bit vectors.
+int gf2_rank(std::vector<uint32_t> v) {
+    int r = 0;
+    for (int bit = 31; bit >= 0; bit--) {
+        size_t piv = v.size();
+        for (size_t i = size_t(r); i < v.size(); i++)
+            if ((v[i] >> bit) & 1u) {
+                piv = i;
+                break;
+            }
+        if (piv == v.size()) continue;
+        std::swap(v[size_t(r)], v[piv]);
+        for (size_t i = 0; i < v.size(); i++)
+            if (i != size_t(r) && ((v[i] >> bit) & 1u)) v[i] ^= v[size_t(r)];
+        r++;
+    }
+    return r;
+}
+
+// The split's thread mapping (FusedPass::split_pos): lane bits 3 and 4 of a
+// warp go to the first pair of local bits (4..11) whose banks in block 0's
+// operand layout, with those of local bits 1..3, are independent.
+void set_split_map(FusedPass& fp) {
+    auto off = [&](uint32_t l) { return uint32_t(fp.in_lo[l & 63u] ^ fp.in_hi[l >> 6]); };
+    auto bank = [&](int q) { return (off(1u << q) >> 2) & 31u; };
+    int x = 4, y = 5;
+    if (gf2_rank({bank(1), bank(2), bank(3), bank(4), bank(5)}) < 5) {
+        bool found = false;
+        for (int a = 4; a < kFusedM && !found; a++)
+            for (int b = a + 1; b < kFusedM && !found; b++)
+                if (gf2_rank({bank(1), bank(2), bank(3), bank(a), bank(b)}) == 5) {
+                    x = a;
+                    y = b;
+                    found = true;
+                }
+    }
+    int pos[kFusedM] = {0, 1, 2, 3, x, y};
+    for (int q = 4, i = 6; q < kFusedM; q++)
+        if (q != x && q != y) pos[i++] = q;
+    for (int b = 0; b < 8; b++) fp.split_pos[b] = uint8_t(pos[b]);
+    for (int k = 0; k < 16; k++) {
+        uint32_t e = 0;
+        for (int b = 0; b < 4; b++)
+            if ((k >> b) & 1) e |= 1u << pos[8 + b];
+        fp.split_q[k] = uint16_t(e);
+        fp.split_qoff[k] = uint16_t(off(e));
+    }
+}
+
+}  // namespace
+
 FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::vector<int>& tile_qubits,
                            std::vector<FusedBlock>& blocks, std::vector<uint16_t>& upool) {
     FusedPass fp;
@@ -616,14 +669,15 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
     // Stage after the last block: natural index l lives at slot s(l) = l ^ h(l),
     // h copying lane qubits above bit 3 onto the bank bits 0..3 that the last
     // block's lanes leave constant (s is linear and invertible; a warp reading
-    // consecutive l still covers every bank).
+    // consecutive l still covers every bank).  The sources are bits 4 and up,
+    // so the slots of l and l ^ 1 stay the two halves of one 16-byte pair; when
+    // bit 0 is a destination they may sit swapped, and the store phase reads
+    // the pair at its 16-byte boundary and swaps it back.
     uint32_t hsrc[4] = {0, 0, 0, 0}, hdst[4] = {0, 0, 0, 0};
     int hn = 0;
     {
         std::vector<uint32_t> free_bits, high;
-        // Bit 0 is never a destination: slots of l and l ^ 1 stay adjacent, so
-        // the store phase reads 16-byte pairs.
-        for (uint32_t b = 1; b < 4; b++)
+        for (uint32_t b = 0; b < 4; b++)
             if (!((lanes >> b) & 1u)) free_bits.push_back(b);
         for (uint32_t b = 4; b < 12; b++)
             if ((lanes >> b) & 1u) high.push_back(b);
@@ -648,6 +702,7 @@ FusedPass build_fused_pass(const std::vector<Operation>& pass_ops, const std::ve
         fp.out_lo[e] = stage_off(uint32_t(e));
         fp.out_hi[e] = stage_off(uint32_t(e) << 6);
     }
+    set_split_map(fp);
     for (size_t j = 0; j < blk.size(); j++) {
         FusedBlock d;
         std::memset(&d, 0, sizeof d);

@@ -154,6 +154,16 @@ struct FusedPass {
     int first_block = 0, nblocks = 0;
     uint16_t in_lo[64], in_hi[64];    // natural local index l -> operand offset of block 0 (lo ^ hi)
     uint16_t out_lo[64], out_hi[64];  // natural local index l -> stage offset (lo ^ hi)
+    // The split of a loaded tile into block 0's operand: thread gt of a group
+    // takes the amplitude pairs e = P(gt) | split_q[k], k = 0..15, where P
+    // deposits bit b of 2*gt (b = 1..7) at local bit split_pos[b]; split_qoff[k]
+    // is the operand offset of split_q[k].  Local bits 1..3 follow lane bits
+    // 0..2 (16-byte reads of a quarter-warp stay in one 128-byte row); lane
+    // bits 3 and 4 take the two local bits that give the warp's 4-byte stores
+    // 32 distinct banks in block 0's layout, where two such bits exist.
+    uint8_t split_pos[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    uint16_t split_q[16] = {};
+    uint16_t split_qoff[16] = {};
     int raw_ops = 0;
     std::vector<int> block_gates;        // gates fused into each block
     std::vector<uint32_t> block_masks;   // each block's local qubits

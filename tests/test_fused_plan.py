@@ -66,6 +66,31 @@ def random_circuit_n(n, gates, seed):
     return Circuit(n, ins)
 
 
+def split_tile(p, tiles):
+    """The kernel's split of loaded tiles into block 0's operand: thread gt takes the
+    pairs (e, e + 1), e = P(gt) | split_q[k], P depositing bits 1..7 of 2 * gt at
+    split_pos, and stores them at split_off(gt) ^ split_qoff[k] (and ^ in_lo[1])."""
+    in_lo, in_hi = np.asarray(p["in_lo"]), np.asarray(p["in_hi"])
+    pos, q, qoff = p["split_pos"], np.asarray(p["split_q"]), np.asarray(p["split_qoff"])
+    gt = np.arange(128)
+    P = np.zeros(128, dtype=np.int64)
+    for b in range(1, 8):
+        P |= (((2 * gt) >> b) & 1) << pos[b]
+    split_off = in_lo[P & 63] ^ in_hi[P >> 6]
+    slots = np.zeros_like(tiles)
+    seen = np.zeros(4096, dtype=np.int64)
+    for k in range(16):
+        e = P | q[k]
+        off = split_off ^ qoff[k]
+        assert np.array_equal(off, in_lo[e & 63] ^ in_hi[e >> 6])  # the per-iteration offsets are the layout's
+        slots[:, off // 4] = tiles[:, e]
+        slots[:, (off ^ in_lo[1]) // 4] = tiles[:, e + 1]
+        seen[e] += 1
+        seen[e + 1] += 1
+    assert np.all(seen == 1)  # every amplitude of the tile exactly once
+    return slots
+
+
 def emulate(plan):
     n = plan["n"]
     upool = np.asarray(plan["upool"], dtype=np.uint16).view(np.float16)
@@ -78,9 +103,7 @@ def emulate(plan):
         idx = deposit(np.arange(1 << (n - 12)), other)[:, None] | deposit(local, T)[None, :]
         tiles = state[idx]
         # tables hold byte offsets combined by XOR: 4-byte operand entries, 8-byte stage entries
-        off = np.asarray(p["in_lo"])[local & 63] ^ np.asarray(p["in_hi"])[local >> 6]
-        slots = np.zeros_like(tiles)
-        slots[:, off // 4] = tiles
+        slots = split_tile(p, tiles)
         for blk in p["blocks"]:
             X = slots[:, SLOT_OF_PACKED].reshape(-1, 128, 32)
             U = block_matrix(upool, blk["u_off"])
@@ -269,3 +292,39 @@ def test_planning_in_a_forked_child():
     child.join(120)
     assert child.exitcode == 0
     assert queue.get(timeout=5) == expect
+
+
+def warp_wavefronts(offsets, entry_bytes):
+    """Shared-memory wavefronts of one warp store (one per 128 bytes, more on bank conflicts)."""
+    banks = (np.asarray(offsets) // 4) % 32
+    if entry_bytes == 4:
+        return int(np.bincount(banks, minlength=32).max())
+    # 8-byte entries go out a half-warp (128 bytes) at a time
+    return sum(int(np.bincount(banks[h * 16:(h + 1) * 16] // 2, minlength=16).max()) for h in range(2))
+
+
+@pytest.mark.parametrize("maker", [lambda: brickwork(30, 40, seed=0, measure=False), lambda: qft(30, seed=0),
+                                   lambda: hea(26, 20, seed=0), lambda: random_circuit_n(20, 400, 5)])
+def test_split_and_stage_stores_avoid_bank_conflicts(maker):
+    plan = _core.fused_plan_dump(maker().model_dump_json())
+    split_extra = 0
+    for p in plan["passes"]:
+        in_lo, in_hi = np.asarray(p["in_lo"]), np.asarray(p["in_hi"])
+        pos, qoff = p["split_pos"], np.asarray(p["split_qoff"])
+        # split: a warp (lanes = bits 0..4 of gt) stores one 4-byte entry per lane
+        for w in range(4):
+            gt = np.arange(32) + 32 * w
+            P = np.zeros(32, dtype=np.int64)
+            for b in range(1, 8):
+                P |= (((2 * gt) >> b) & 1) << pos[b]
+            off = (in_lo[P & 63] ^ in_hi[P >> 6]) ^ qoff[3]
+            split_extra += warp_wavefronts(off, 4) - 1
+        # stage: the last block's readback, lanes = its TMEM lanes (tile columns)
+        nc = np.asarray(p["blocks"][-1]["next_c"])
+        for w in range(4):
+            assert warp_wavefronts(nc[32 * w:32 * w + 32], 8) == 2
+        # the stage keeps the amplitudes e and e ^ 1 in one 16-byte pair
+        out = np.asarray(p["out_lo"])[np.arange(4096) & 63] ^ np.asarray(p["out_hi"])[np.arange(4096) >> 6]
+        assert np.all((out[0::2] ^ out[1::2]) == 8)
+    # at most one conflicting warp store in ten, across the plan
+    assert split_extra <= 0.1 * 4 * len(plan["passes"]), split_extra
