@@ -135,3 +135,26 @@ def test_repeated_calls_reuse_the_compiled_plan():
             seed=5, precision="complex64").simulate_shots(other, 500)
     assert sim.simulate_shots(c, 4000) == first
     assert _core.last_call_phases(sim)["parse"] > 0  # evicted, so planned again
+
+
+@pytest.mark.parametrize("precision", ["complex128", "complex64"])
+def test_sampling_workspace_follows_changing_sizes(precision):
+    """A simulator keeps its terminal-sampling buffers (statevector, table, scratch, outcomes) between calls
+    and reallocates them when a call needs other sizes: calls of changing qubit count, measured register and
+    shot count on one simulator give the counts fresh simulators give, and only the first call of a size
+    allocates."""
+    def measured(n, qubits, seed):
+        ins = brickwork(n, 5, seed=seed, measure=False).data["instructions"]
+        return Circuit(n, ins + [inst("measure", qubit=q, cbit=c) for c, q in enumerate(qubits)], len(qubits))
+
+    calls = [(measured(14, range(14), 1), 3000), (measured(16, range(16), 2), 3000),
+             (measured(14, range(14), 1), 3000), (measured(14, [3, 9, 12], 4), 700),
+             (measured(18, [0, 17, 5, 5], 6), 5000), (measured(14, range(14), 1), 3000)]
+    sim = dqsim.StatevectorSimulator(seed=9, precision=precision)
+    for i, (c, shots) in enumerate(calls):
+        got = sim.simulate_shots(c, shots)
+        assert got == dqsim.StatevectorSimulator(seed=9, precision=precision).simulate_shots(c, shots), i
+        assert sum(got.values()) == shots
+    again = sim.simulate_shots(calls[-1][0], calls[-1][1])
+    assert _core.last_call_phases(sim)["table"] < 0.05  # same sizes as the call before: nothing allocated
+    assert again == dqsim.StatevectorSimulator(seed=9, precision=precision).simulate_shots(*calls[-1])
