@@ -25,7 +25,11 @@ static PyObject* build(PyObject* self, PyObject* args) {
         PyErr_SetString(PyExc_ValueError, "counts buffers do not match");
         goto done;
     }
+#if PY_VERSION_HEX >= 0x030D0000
+    out = PyDict_New();  /* the presizing helper is private from 3.13 on */
+#else
     out = _PyDict_NewPresized(n);
+#endif
     if (!out) goto done;
     const char* k = (const char*)keys.buf;
     const unsigned char* c = (const unsigned char*)counts.buf;
