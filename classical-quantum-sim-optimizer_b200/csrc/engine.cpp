@@ -760,7 +760,7 @@ void Executor::upload(cudaStream_t stream) {
     uploaded_ = true;
 }
 
-void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec, bool normalize) {
+void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec, bool normalize, bool from_basis) {
     upload(b.stream);
     std::vector<uint64_t> host_cbits;
     bool norm_pending = false;  // a fused pass left a norm the next fused pass divides out
@@ -793,7 +793,8 @@ void Executor::run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec, b
             norm_states_.ensure(size_t(b.W) * size_t(k::fused_norm_parts(b.n)) * 8, "fused state norms");
             if (rec) rec->begin(kcFused, step_bytes(si, b));
             k::fused_pass(b, p, fused_blocks_.as<FusedBlock>(), upool_.as<uint16_t>(), b.err,
-                          norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>());
+                          norm_pending ? norm_states_.as<double>() : nullptr, norm_tiles_.as<double>(),
+                          from_basis && si == 0);
             if (rec) rec->end();
             const bool last_fused = si + 1 == steps_.size() || steps_[si + 1].fused < 0;
             if (normalize || si + 1 != steps_.size()) {

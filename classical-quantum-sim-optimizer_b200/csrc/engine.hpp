@@ -160,7 +160,12 @@ class Executor {
     // FP64 norm and rescale are left out (the state keeps the pass's rounding
     // of the norm, ~1e-7); for callers that only sample, which divides by the
     // total probability anyway.
-    void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr, bool normalize = true);
+    // `from_basis`: every state of the batch is |0...0> on entry; a first step
+    // that is a fused pass then builds its input tiles itself (the caller
+    // need not write the state first: starts_with_fused_pass()).
+    void run(const k::Batch& b, ProfileAcc* profile, EventRecorder* rec = nullptr, bool normalize = true,
+             bool from_basis = false);
+    bool starts_with_fused_pass() const { return !steps_.empty() && steps_[0].fused >= 0; }
     // Uploads the matrix pools and sizes the scratch a run over batches like
     // `b` needs, so that later runs allocate nothing and copy nothing from the
     // host (they can then be captured into a CUDA graph).

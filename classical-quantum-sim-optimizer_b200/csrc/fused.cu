@@ -112,6 +112,7 @@ struct FusedQubits {
     uint16_t split_qoff[16];   // ... and their operand offsets
     FusedTma tma;        // tile loads by TMA when tma.ok
     FusedFault fault;
+    int basis;           // 1: the input is |0...0> in every state, built here and not loaded
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -359,6 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const bool use_tma = fq.tma.ok != 0;
     uint32_t tiles_loaded = 0, tiles_landed = 0;
     auto prefetch = [&](uint64_t tt) {
+        if (fq.basis) return;  // the input tiles are built in place
         if (use_tma) {
             tiles_loaded++;
             if (gt != 0) return;
@@ -407,7 +409,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const float fs = float(scale * double(kScale));
         const uint64_t fs2 = pack2(__float_as_uint(fs), __float_as_uint(fs));
-        if (use_tma) {
+        if (fq.basis) {
+            // nothing loaded
+        } else if (use_tma) {
             // Every thread observes the tile's mbarrier phase (bounded), then votes.
             const bool landed = mbar_wait(bar(kBarTile + uint32_t(g)), tiles_landed & 1u, wl);
             tiles_landed++;
@@ -423,9 +427,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             // Pairs (e, e + 1), e = split_p | split_q[k]: 16-byte reads of the raw tile
             // (natural order), 4-byte hi/lo stores into block 0's operand.
             float4 v[kPairIters];
+            // |0...0> (basis): amplitude 1 at the state's index 0 (local index 0 of
+            // its first tile: thread split_p == 0, k = 0), 0 elsewhere.
+            const bool one = fq.basis && split_p == 0 && (base & ((uint64_t(1) << n) - 1)) == 0;
 #pragma unroll
-            for (int k = 0; k < kPairIters; k++)
+            for (int k = 0; k < kPairIters; k++) {
                 v[k] = *reinterpret_cast<const float4*>(x + (split_p | uint32_t(fq.split_q[k])) * 8u);
+                if (fq.basis) v[k] = make_float4(k == 0 && one ? 1.f : 0.f, 0.f, 0.f, 0.f);
+            }
             group_sync(g);  // raw tile read: the split may overwrite it
 #pragma unroll
             for (int k = 0; k < kPairIters; k++) {
@@ -786,7 +795,7 @@ void fused_configure() {
 }
 
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev, int* err,
-                const double* in_norm, double* tile_norm) {
+                const double* in_norm, double* tile_norm, bool basis) {
     if (!b.c64) fail(kValueError, "fused tensor-core passes run on complex64 states");
     if (b.n < kFusedM || int(p.qubits.size()) != kFusedM) fail(kValueError, "fused passes need 12 tile qubits");
     if (p.nblocks < 1) fail(kValueError, "fused pass without blocks");
@@ -808,6 +817,7 @@ void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev
     std::memset(&tile_map, 0, sizeof tile_map);
     fq.tma = fused_tma_plan(p.qubits, b.n, b.W);
     fq.fault = g_fault;
+    fq.basis = basis ? 1 : 0;
     if (fq.tma.ok && !encode_tile_map(fq.tma, b.amps, b.W << b.n, &tile_map)) fq.tma.ok = 0;
     fused_configure();
     // One CTA per SM, persistent over groups of kGroups tiles.

@@ -115,12 +115,14 @@ double Plan::run(bool record) {
     cuda_check(cudaEventCreate(&b), "cudaEventCreate");
     cuda_check(cudaEventRecord(a, s), "cudaEventRecord");
     k::Batch bt = st_.view(s, 1);
-    k::init_basis(bt);
+    // |0...0>: written here, or built by a first fused pass in its tiles.
+    const bool built = ex_->starts_with_fused_pass();
+    if (!built) k::init_basis(bt);
     cuda_check(cudaMemsetAsync(st_.cbits.p, 0, size_t(st_.cwords) * 8, s), "clear cbits");
     cuda_check(cudaMemsetAsync(st_.draws.p, 0, 8, s), "clear draws");
     cuda_check(cudaMemsetAsync(st_.err.p, 0, 16, s), "clear error flag");
     cuda_check(cudaMemcpyAsync(st_.seeds.p, &seed_, 8, cudaMemcpyHostToDevice, s), "seed");
-    ex_->run(bt, nullptr, record ? &rec : nullptr, /*normalize=*/cdf_.p == nullptr);
+    ex_->run(bt, nullptr, record ? &rec : nullptr, /*normalize=*/cdf_.p == nullptr, /*from_basis=*/built);
     if (cdf_.p) {
         const uint64_t clen = uint64_t(1) << sample_qubits_.size();
         bool full = sample_qubits_.size() == n_;

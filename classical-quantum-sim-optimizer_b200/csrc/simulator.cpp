@@ -289,7 +289,6 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                 if (!st.amps.p || st.n != int(n) || st.W != 1 || st.ncb != ncb || st.c64 != c64)
                     st.allocate(int(n), 1, ncb, c64, s);
                 k::Batch b = st.view(s, 1);
-                k::init_basis(b);
                 reset_bookkeeping(st, 1, {kept_seed}, s);
                 phase(kPhState);
                 DevMem& cdf = ws_->table;
@@ -321,7 +320,10 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                     }
                 } ev_guard{ev};
                 cuda_check(cudaEventRecord(ev[0], s), "cudaEventRecord");
-                ex->run(b, nullptr, nullptr, /*normalize=*/false);  // the sampler divides by the total
+                // |0...0>: written here, or built by a first fused pass in its tiles.
+                const bool built = ex->starts_with_fused_pass();
+                if (!built) k::init_basis(b);
+                ex->run(b, nullptr, nullptr, /*normalize=*/false, /*from_basis=*/built);  // the sampler divides by the total
                 cuda_check(cudaEventRecord(ev[1], s), "cudaEventRecord");
                 phase(kPhRun);
                 double total = build_sums(b, qubits, cdf.as<double>(), clen, tmp);

@@ -259,9 +259,11 @@ namespace k {
 // flag set to 3 when a bounded wait on an mbarrier runs out.
 // in_norm (nullable): the previous fused pass's partial norm sums
 // (fused_state_norm's output), divided out on load; tile_norm (W * 2^(n-12)
-// doubles) receives each output tile's FP64 squared norm.
+// doubles) receives each output tile's FP64 squared norm.  basis: every state
+// is |0...0> on entry; the pass builds its input tiles itself and reads
+// nothing of the state (which may hold anything).
 void fused_pass(const Batch& b, const FusedPass& p, const FusedBlock* blocks_dev, const uint16_t* upool_dev,
-                int* err_dev, const double* in_norm, double* tile_norm);
+                int* err_dev, const double* in_norm, double* tile_norm, bool basis = false);
 // Partial sums of each state's tile norms, fused_norm_parts(n) per state in
 // a fixed order (state st's norm is the in-order sum of norm[st*parts ..]).
 int fused_norm_parts(int n);

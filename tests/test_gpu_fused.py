@@ -158,3 +158,18 @@ def test_sampling_workspace_follows_changing_sizes(precision):
     again = sim.simulate_shots(calls[-1][0], calls[-1][1])
     assert _core.last_call_phases(sim)["table"] < 0.05  # same sizes as the call before: nothing allocated
     assert again == dqsim.StatevectorSimulator(seed=9, precision=precision).simulate_shots(*calls[-1])
+
+
+def test_terminal_sampling_from_a_state_built_by_the_first_fused_pass():
+    """Terminal sampling starts the unitary prefix from |0...0>; when its first step is a fused pass, that pass
+    builds the input tiles itself (no state write, no load).  Counts follow the oracle's (same ChaCha8 streams;
+    complex64 probabilities differ by ~1e-7, so almost every shot agrees), on one state and on a second call
+    that reuses the workspace the first one left behind."""
+    for seed, n in ((5, 14), (6, 16)):
+        c = brickwork(n, 6, seed=seed, measure=True)
+        sim = fused(seed=3)
+        for _ in range(2):
+            counts = sim.simulate_shots(c, 6000)
+            want = o.OracleSimulator(seed=3).simulate_shots(c, 6000)
+            tvd = sum(abs(counts.get(k, 0) - want.get(k, 0)) for k in set(counts) | set(want)) / 2 / 6000
+            assert tvd < 0.01, tvd
