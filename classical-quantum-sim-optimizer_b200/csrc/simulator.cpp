@@ -5,6 +5,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -372,10 +373,21 @@ ShotOutput Simulator::run_shots(const std::vector<Operation>& ops, uint64_t n, u
                     out.key_width = ncb;
                     out.flat_keys.assign(distinct * ncb, '0');
                     out.flat_counts.resize(distinct);
+                    // cbit 0 is the rightmost character; whole bytes of the value through
+                    // a table of their eight characters (most significant bit first).
+                    static const std::array<std::array<char, 8>, 256> byte_chars = [] {
+                        std::array<std::array<char, 8>, 256> t{};
+                        for (int v = 0; v < 256; v++)
+                            for (int b = 0; b < 8; b++) t[size_t(v)][size_t(7 - b)] = char('0' + ((v >> b) & 1));
+                        return t;
+                    }();
                     char* key = &out.flat_keys[0];
                     for (size_t i = 0; i < distinct; i++, key += ncb) {
-                        for (uint64_t c = 0; c < ncb; c++)  // cbit 0 is the rightmost character
-                            key[ncb - 1 - c] = char('0' + ((kc[i].first >> c) & 1));
+                        const uint64_t v = kc[i].first;
+                        uint64_t c = 0;
+                        for (; c + 8 <= ncb; c += 8)  // cbits c..c+7 end at character ncb - 1 - c
+                            std::memcpy(key + (ncb - 8 - c), byte_chars[size_t((v >> c) & 0xFFu)].data(), 8);
+                        for (; c < ncb; c++) key[ncb - 1 - c] = char('0' + ((v >> c) & 1));
                         out.flat_counts[i] = kc[i].second;
                     }
                 } else {
