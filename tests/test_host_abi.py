@@ -40,6 +40,13 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
 
 
+def test_call_phase_count_matches_the_header():
+    text = (ROOT / "include" / "dqsim_sv.h").read_text()
+    declared = int(re.search(r"#define DQ_CALL_PHASES (\d+)", text).group(1))
+    assert declared == len(_core.CALL_PHASES) == 12
+    assert _core.CALL_PHASES[-2:] == ("table", "prefix_device")
+
+
 def _bits(x):
     return "%016x" % struct.unpack("<Q", struct.pack("<d", x))[0]
 
