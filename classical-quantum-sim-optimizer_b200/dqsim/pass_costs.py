@@ -24,7 +24,7 @@ import numpy as np
 from . import _core, workloads
 
 # Seeded random passes per state size (the bulk of the training set).
-RANDOM_PASSES = {24: 9000, 26: 9000, 28: 9000, 30: 7000, 31: 3000, 32: 2000}
+RANDOM_PASSES = {24: 11000, 26: 11000, 28: 11000, 30: 9000, 31: 4000, 32: 3000}
 # Circuits whose candidate plans' passes join the training set: depth-40 brickwork and QFT, 24-30 qubits.
 TRAIN_CIRCUITS = ([("brickwork", n, 100 + 10 * n + s) for n in (24, 26, 28, 30) for s in range(2)]
                   + [("qft", n, 200 + n) for n in (24, 26, 28, 30)])
