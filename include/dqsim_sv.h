@@ -168,7 +168,11 @@ typedef enum dq_kernel_class {
 } dq_kernel_class;
 DQ_API int dq_plan_create(dq_sim* sim, const char* json, size_t json_len, uint64_t shots, dq_plan** out);
 /* One run; *device_ms is the CUDA-event time on the engine stream.  With
- * record != 0 every launch is bracketed by events for dq_plan_stats. */
+ * record != 0 every launch is bracketed by events for dq_plan_stats.  A plan
+ * created with shots > 0 samples at the end of each run; its complex64 fused
+ * form then skips the FP64 rescale after the last fused pass (sampling
+ * divides by the total), so its final state keeps that pass's rounding of
+ * the norm (~1e-7). */
 DQ_API int dq_plan_run(dq_plan* p, int record, double* device_ms);
 /* Per kernel class of the last recorded run: milliseconds, kernel launches and
  * algorithmic bytes (arrays of DQ_K_NUM_CLASSES entries). */
@@ -176,8 +180,9 @@ DQ_API int dq_plan_stats(const dq_plan* p, double* ms, uint64_t* launches, doubl
 DQ_API int dq_plan_info(const dq_plan* p, uint64_t* num_qubits, uint64_t* num_ops, double* state_bytes);
 DQ_API int dq_plan_statevector(const dq_plan* p, double* out, uint64_t out_len);
 DQ_API int dq_plan_samples(const dq_plan* p, uint64_t* out, uint64_t out_len);
-/* State fidelity |<a|b>|^2 and max amplitude error of two plans' final states
- * (same qubit count, any precisions), computed on the device. */
+/* State fidelity |<a|b>|^2 / (<a|a> <b|b>) and max amplitude error of two
+ * plans' final states (same qubit count, any precisions), computed on the
+ * device. */
 DQ_API int dq_plan_compare(const dq_plan* a, const dq_plan* b, double* fidelity, double* max_abs_err);
 DQ_API void dq_plan_free(dq_plan* p);
 
