@@ -502,7 +502,7 @@ class PreparedCircuit:
         return {"passes": p.value, "tile_ops": t.value, "fused_blocks": f.value}
 
     def compare(self, other):
-        """(fidelity |<self|other>|^2, max amplitude error) of the two final states."""
+        """(fidelity |<self|other>|^2 / (<self|self> <other|other>), max amplitude error) of the two final states."""
         f, e = ctypes.c_double(), ctypes.c_double()
         _check(_plan_compare(self._h, other._h, ctypes.byref(f), ctypes.byref(e)))
         return f.value, e.value
