@@ -22,7 +22,10 @@
 // Tiles arrive by TMA (cp.async.bulk.tensor): the state is viewed as a tensor
 // of up to five dimensions whose boxes are the tile's runs of qubits, so one
 // thread issues a tile's load and no load passes through the LSU; tiles whose
-// qubits need more dimensions fall back to 16-byte cp.async copies.
+// qubits need more dimensions fall back to 16-byte cp.async copies.  The split
+// into block 0's operand follows a per-pass thread mapping chosen on the host
+// so that its stores hit 32 distinct banks; the first pass of a circuit from
+// |0...0> builds its input tiles instead of loading them.
 // All tiles walk the same block sequence and share the gate images: a pass of
 // up to five blocks holds all of them for the whole launch, and a longer one
 // cycles five buffers, fetched five blocks ahead by whichever group finishes
